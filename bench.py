@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Benchmark of the exact 2-NN matching path (one JSON line on rank 0).
+
+Workload: 10,000 queries against a 1,000,000 x 128 uint8 base from the seeded
+generator (matching_sift_b200.datagen; stand-in for ANN_SIFT1M), exact
+2-NN with the Lowe ratio test at 0.8.
+
+  value : queries/s with inputs resident in HBM, one step = one full
+          sift2nn_match call (row norms, fused tensor-core search, merge)
+  e2e   : queries/s through the reference-named C ABI call cublas_2nn_sift
+          with host uint8 buffers in and a host match array out; the copies
+          are inside the timed region
+  roofline : the fused search kernel, timed with CUDA events on its own
+          stream; 2 * Q * N * 128 integer ops per launch
+  cpu_baseline : the reference's own host_brute (compiled from its sources)
+          on all host cores over a bounded query sample
+
+Multi-GPU: the path shards by queries with the base replicated, so every rank
+matches its own 10,000 queries (weak scaling, no data-path collective).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+Q_N, R_N, DIM = 10_000, 1_000_000, 128
+THRESHOLD = 0.8
+METRIC = "2-NN queries/s on a 1M×128 base: exact u8 vs FP16 vs learned hash at recall@1≥0.8"
+WORKLOAD = "exact 2-NN, 10,000 x 128 u8 queries vs 1,000,000 x 128 u8 base, ratio test 0.8"
+L2_BYTES = 126 * 1024 * 1024
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p, "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+        self._t = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            if self._t is not None:
+                self._t.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def _profile_traffic():
+    """DRAM bytes per launch of the search kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "exact2nn_u8_10000x1M.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+# ------------------------------------------------------------ CPU baselines --
+
+def _host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_reference_rate(q, r, target_s: float):
+    """(queries/s, sample description, threads, kind) of the reference host_brute on a bounded sample."""
+    import oracle
+
+    threads = _host_threads()
+    rf = np.ascontiguousarray(r, dtype=np.float32)
+    kind = "reference"
+    if oracle.ref_available():
+        def run(n):
+            return oracle.ref_host_brute(q[:n].astype(np.float32), rf, nthreads=threads)
+    else:
+        kind = "port"
+
+        def run(n):
+            return oracle.brute_2nn_u8(q[:n], r, nthreads=threads)
+    n = threads
+    t0 = time.perf_counter()
+    run(n)
+    dt = time.perf_counter() - t0
+    per_q = dt / n
+    n2 = int(max(threads, min(q.shape[0], target_s / max(per_q, 1e-9))))
+    n2 = max(threads, (n2 // threads) * threads)
+    t0 = time.perf_counter()
+    run(n2)
+    dt = time.perf_counter() - t0
+    return n2 / dt, f"{n2} queries x {r.shape[0]} base rows ({dt:.1f} s)", threads, kind
+
+
+# ----------------------------------------------------------------- main ----
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = _env_int("WORLD_SIZE", 1)
+    rank = _env_int("RANK", 0)
+    local_rank = _env_int("LOCAL_RANK", 0)
+
+    if args.impl == "reference":
+        return reference_arm(args, world, rank)
+
+    import torch
+    import torch.distributed as dist
+
+    import matching_sift_b200 as ms
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
+
+    from matching_sift_b200 import datagen
+
+    base = datagen.make_base(R_N, seed=0)
+    queries = datagen.make_queries(Q_N, base, seed=rank)
+    lib = ms.lib()
+
+    qd = torch.from_numpy(queries).to(dev)
+    rd = torch.from_numpy(base).to(dev)
+    matches = torch.empty(Q_N, dtype=torch.int32, device=dev)
+    nn_idx = torch.empty((Q_N, 2), dtype=torch.int32, device=dev)
+    nn_dist = torch.empty((Q_N, 2), dtype=torch.float32, device=dev)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        rc = lib.sift2nn_match(qd.data_ptr(), rd.data_ptr(), ms.U8_DEVICE, Q_N, R_N, ms.METRIC_L2, THRESHOLD,
+                               matches.data_ptr(), None, nn_idx.data_ptr(), nn_dist.data_ptr(), stream.cuda_stream)
+        if rc != 0:
+            raise ms.SiftError(rc, "sift2nn_match")
+
+    # ---- device-resident throughput
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if ms.stream_status(stream.cuda_stream) != 0:
+        raise RuntimeError("device status after warm-up")
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.sift_launch_count()
+    lib.sift_profile_enable(1)
+    with ClockSampler(local_rank) as clocks:
+        for k in range(args.steps):
+            flush.fill_(k)  # evict the base from L2 between steps (outside the timed events)
+            ev[k][0].record(stream)
+            step()
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+    lib.sift_profile_enable(0)
+    launches = lib.sift_launch_count() - launches0
+    import ctypes
+    kt, kn = ctypes.c_double(0.0), ctypes.c_int(0)
+    lib.sift_profile_collect(ctypes.byref(kt), ctypes.byref(kn))
+    if ms.stream_status(stream.cuda_stream) != 0:
+        raise RuntimeError("device status after timed steps")
+    step_ms = float(sum(a.elapsed_time(b) for a, b in ev))
+    kernel_ms = kt.value / max(kn.value, 1)
+
+    # ---- end to end through the C ABI with host buffers
+    qh = torch.from_numpy(queries).pin_memory()
+    rh = torch.from_numpy(base).pin_memory()
+    mh = torch.empty(Q_N, dtype=torch.int32).pin_memory()
+
+    def e2e_step():
+        rc = lib.cublas_2nn_sift(qh.data_ptr(), rh.data_ptr(), ms.U8_HOST, Q_N, R_N, mh.data_ptr(), THRESHOLD,
+                                 None, 1, 0, 17)
+        if rc != 0:
+            raise ms.SiftError(rc, "cublas_2nn_sift")
+
+    for _ in range(args.warmup):
+        e2e_step()
+    e2e_ms = 0.0
+    legacy = torch.cuda.default_stream(dev)
+    for k in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(legacy)
+        e2e_step()
+        b.record(legacy)
+        b.synchronize()
+        e2e_ms += a.elapsed_time(b)
+    np.testing.assert_array_equal(mh.numpy(), matches.cpu().numpy())
+
+    # ---- max over ranks
+    t = torch.tensor([step_ms, e2e_ms, kernel_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    step_ms, e2e_ms, kernel_ms = t.tolist()
+
+    if rank == 0:
+        peaks, peak_src = _peaks()
+        ops = 2.0 * Q_N * R_N * DIM
+        achieved = ops / (kernel_ms * 1e-3) / 1e12
+        peak_int8 = 2.0 * peaks["bf16_tflops"]
+        qps = world * Q_N * args.steps / (step_ms * 1e-3)
+        e2e_qps = world * Q_N * args.steps / (e2e_ms * 1e-3)
+        line = {
+            "metric": METRIC,
+            "value": round(qps, 1),
+            "unit": "queries/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(step_ms / args.steps, 4),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "u8",
+            "data": "synthetic (seeded generator standing in for ANN_SIFT1M; base seed 0, queries seed = rank)",
+            "config": {"workload": WORKLOAD, "queries_per_gpu": Q_N, "base_rows": R_N, "dim": DIM,
+                       "ratio": THRESHOLD, "l2_between_steps": "flushed (256 MiB write outside the timed events)",
+                       "parallelism": f"query-sharded x{world}, base replicated"},
+            "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s",
+                    "h2d_bytes_per_step": (Q_N + R_N) * DIM, "d2h_bytes_per_step": Q_N * 4,
+                    "call": "cublas_2nn_sift(type=SIFT_U8_HOST) with pinned host buffers"},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "tensor", "kernel": "exact2nn_u8_kernel", "achieved": round(achieved, 1),
+                         "peak": round(peak_int8, 1), "unit": "TFLOP/s", "frac": round(achieved / peak_int8, 4),
+                         "traffic": _profile_traffic(),
+                         "ops_per_launch": ops, "kernel_ms": round(kernel_ms, 4),
+                         "peak_note": f"dense int8 peak taken as 2 x {peak_src} bf16 burst "
+                                      f"({peaks['bf16_tflops']} TFLOP/s); nominal 4500"},
+            "clocks": clocks.summary(),
+        }
+        if not args.no_cpu_baseline:
+            rate, sample, threads, kind = cpu_reference_rate(queries, base, 15.0)
+            line["cpu_baseline"] = {"value": round(rate, 2), "unit": "queries/s", "cores": threads, "kind": kind,
+                                    "sample": sample}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def reference_arm(args, world, rank):
+    """The reference's own CPU implementation (host_brute) on all host threads, bounded samples."""
+    if rank != 0:
+        return
+    import oracle
+    from matching_sift_b200 import datagen
+
+    base = datagen.make_base(R_N, seed=0)
+    queries = datagen.make_queries(Q_N, base, seed=0)
+    threads = _host_threads()
+    kind = "reference" if oracle.ref_available() else "port"
+    rf = np.ascontiguousarray(base, dtype=np.float32)
+
+    def run(n, off):
+        qs = queries[off:off + n]
+        if kind == "reference":
+            return oracle.ref_host_brute(qs.astype(np.float32), rf, nthreads=threads)
+        return oracle.brute_2nn_u8(qs, base, nthreads=threads)
+
+    # size one step to about 3 s of work
+    t0 = time.perf_counter()
+    run(threads, 0)
+    per_q = (time.perf_counter() - t0) / threads
+    n = max(threads, int(3.0 / max(per_q, 1e-9)) // threads * threads)
+    n = min(n, Q_N)
+    for k in range(args.warmup):
+        run(n, (k * n) % (Q_N - n + 1))
+    total = 0.0
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        run(n, (k * n) % (Q_N - n + 1))
+        total += time.perf_counter() - t0
+    qps = n * args.steps / total
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": round(qps, 2),
+        "unit": "queries/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(1e3 * total / args.steps, 2),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded generator standing in for ANN_SIFT1M)",
+        "config": {"workload": WORKLOAD, "queries_per_step": n, "base_rows": R_N, "dim": DIM},
+        "cpu_baseline": {"value": round(qps, 2), "unit": "queries/s", "cores": threads, "kind": kind,
+                         "sample": f"{n} queries x {R_N} base rows per step"},
+        "e2e": {"value": round(qps, 2), "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

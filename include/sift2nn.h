@@ -1,0 +1,158 @@
+/*
+ * sift2nn.h - C ABI of the B200-native 2-NN SIFT descriptor matcher.
+ *
+ * Part 1 keeps the reference's entry points, with the reference's names and
+ * argument lists, so existing callers (C via this header, cgo, ctypes, or C++
+ * through the mangled forwarders also exported by libsift2nn.so) switch by
+ * relinking. Part 2 is the native interface: u8 descriptors, explicit
+ * streams, all four outputs.
+ *
+ * Conventions shared by every entry point
+ *  - Descriptors are row-major [n][128] (des_t_f = float[128] in the
+ *    reference, include/knn_brute.h:5; des_t_h2 = __half2[64], :6).
+ *  - Distances are squared Euclidean unless stated otherwise; nearest and
+ *    second-nearest are taken in lexicographic (distance, index) order, so a
+ *    tie goes to the lower base index (the order of the reference host_brute,
+ *    src/knn_brute.cu:816-831).
+ *  - The Lowe ratio test passes when sqrtf(d1) / sqrtf(d2) < threshold in
+ *    single precision. For unit-norm inputs this is the reference's
+ *    sqrt(d + 2) form of src/knn_brute.cu:430-442, whose d = -2 q.r.
+ *  - Results are exact for integer-valued descriptors in [0, 255] (computed
+ *    on the tensor cores as u8 x u8 -> s32).
+ *  - The library allocates nothing per call after warm-up: scratch lives in a
+ *    per-device arena that grows on demand and is reused.
+ *  - int-returning functions return SIFT_OK (0) or a negative SIFT_ERR_*;
+ *    void compatibility functions record their status for sift_last_status().
+ *  - Nothing here falls back to the CPU: without a usable CUDA device every
+ *    call returns SIFT_ERR_NO_DEVICE.
+ */
+#ifndef SIFT2NN_H_
+#define SIFT2NN_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SIFT_API __attribute__((visibility("default")))
+#else
+#define SIFT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Input memory types: 0..2 as in the reference (src/knn_brute.cu:15-19,
+   src/lsh_h.cu:710-714); 3 and 4 are extensions for u8 descriptors. */
+enum sift_mem_type {
+    SIFT_FLOAT_HOST = 0,   /* float[n][128] in mapped pinned host memory (read zero-copy) */
+    SIFT_FLOAT_DEVICE = 1, /* float[n][128] in device memory */
+    SIFT_HALF_DEVICE = 2,  /* __half[n][128] in device memory */
+    SIFT_U8_DEVICE = 3,    /* uint8[n][128] in device memory (16-byte aligned) */
+    SIFT_U8_HOST = 4       /* uint8[n][128] in host memory (pinned is fastest) */
+};
+
+/* Metrics of the native interface. */
+enum sift_metric {
+    SIFT_METRIC_L2 = 0, /* squared Euclidean distance */
+    SIFT_METRIC_DOT = 1 /* -2 q.r, the ranking of the reference cublas_2nn_f (src/knn_brute.cu:579-592) */
+};
+
+#define SIFT_OK 0
+#define SIFT_ERR_INVALID_ARG (-1)
+#define SIFT_ERR_CUDA (-2)
+#define SIFT_ERR_NOT_INTEGER (-3)
+#define SIFT_ERR_DEVICE_TIMEOUT (-4)
+#define SIFT_ERR_NO_DEVICE (-5)
+#define SIFT_ERR_UNSUPPORTED (-6)
+#define SIFT_ERR_ALLOC (-7)
+
+typedef struct cublasContext* cublasHandle_t; /* accepted and ignored: no cuBLAS inside */
+typedef float des_t_f[128];
+typedef struct {
+    float x, y, z, w;
+} sift_float4; /* layout of CUDA float4: {d1, d2, i1, i2} */
+
+/* ---------------------------------------------------------------------
+ * Part 1: reference entry points (same names and arguments)
+ * ------------------------------------------------------------------- */
+
+/* Exact 2-NN + Lowe ratio test. Replaces cublas_2nn_sift,
+   include/knn_brute.h:22 / src/knn_brute.cu:24. matches[q] = index of the
+   nearest base row if the ratio test passes, else UINT32_MAX. `matches` may be
+   device, managed or host memory. handle, stream_n, use and warps (the
+   reference's cuBLAS handle, stream count, batch byte budget and scan block
+   size) are accepted and ignored: the fused kernel needs no distance batches.
+   Synchronises before returning (the reference's trailing cudaFree did). */
+SIFT_API int cublas_2nn_sift(void* q_points, void* r_points, int type, uint32_t q_n, uint32_t r_n, uint32_t* matches,
+                    float threshold, cublasHandle_t handle, int stream_n, size_t use, int warps);
+
+/* FP32-interface 2-NN ranked by -2 q.r. Replaces cublas_2nn_f,
+   include/knn_brute.h:18 / src/knn_brute.cu:523. sorted[q] = {d1, d2, i1, i2}
+   with d = -2 q.r as the reference computes it (norms are not added).
+   q/r/sorted: device or managed memory. Synchronises. */
+SIFT_API void cublas_2nn_f(des_t_f* q_points, des_t_f* r_points, int q_n, int r_n, sift_float4* sorted,
+                  cublasHandle_t handle);
+
+/* Exact 2-NN with full squared distances. Replaces device_brute,
+   include/knn_brute.h:14 / src/knn_brute.cu:619. sorted[q] = {d1, d2, i1, i2};
+   absent neighbours are FLT_MAX. q/r/sorted: device or managed memory.
+   Synchronises. */
+SIFT_API void device_brute(des_t_f* q_points, des_t_f* r_points, int q_n, int r_n, sift_float4* sorted);
+
+/* Same contract as device_brute for host arrays. Replaces host_brute,
+   include/knn_brute.h:29 / src/knn_brute.cu:801; the search runs on the GPU
+   (there is no CPU path in this library). */
+SIFT_API void host_brute(des_t_f* q_points, des_t_f* r_points, int q_points_size, int r_points_size, sift_float4* sorted);
+
+/* Status of the last void call above on this thread (SIFT_OK or SIFT_ERR_*). */
+SIFT_API int sift_last_status(void);
+
+/* ---------------------------------------------------------------------
+ * Part 2: native interface
+ * ------------------------------------------------------------------- */
+
+/* Exact 2-NN of q against r. q, r: descriptors of memory type `type` (the same
+   for both). Outputs (device, managed or host memory; any may be NULL):
+     matches[q_n]    nearest index if the ratio test passes, else UINT32_MAX
+     sorted[q_n]     {d1, d2, i1, i2} as floats, FLT_MAX where absent
+     nn_idx[2*q_n]   int32 nearest / second indices, -1 where absent
+     nn_dist[2*q_n]  float distances under `metric`, FLT_MAX where absent
+   stream: a cudaStream_t (NULL = legacy default stream). With device inputs
+   and device outputs the call is asynchronous on `stream`; device-side
+   problems are then reported by sift_stream_status(stream). Any host input or
+   host output makes the call synchronous. */
+SIFT_API int sift2nn_match(const void* q, const void* r, int type, uint32_t q_n, uint32_t r_n, int metric, float threshold,
+                  uint32_t* matches, sift_float4* sorted, int32_t* nn_idx, float* nn_dist, void* stream);
+
+/* Synchronises `stream` and returns the device status of the calls issued on
+   the current device since the last check (SIFT_OK, SIFT_ERR_DEVICE_TIMEOUT
+   when a bounded wait inside a kernel expired, SIFT_ERR_CUDA). */
+SIFT_API int sift_stream_status(void* stream);
+
+/* Human-readable name of a status code. */
+SIFT_API const char* sift_status_string(int status);
+
+/* Library version string. */
+SIFT_API const char* sift_version(void);
+
+/* ---------------------------------------------------------------------
+ * Part 3: instrumentation (used by the benchmark)
+ * ------------------------------------------------------------------- */
+
+/* Number of kernels this library has launched in the process so far. */
+SIFT_API long long sift_launch_count(void);
+
+/* When enabled, the search kernel of every exact call is bracketed by CUDA
+   events recorded on the stream it is launched on. */
+SIFT_API void sift_profile_enable(int on);
+
+/* Synchronises the recorded events and returns (and clears) the summed search
+   kernel time in milliseconds and the number of timed launches. */
+SIFT_API int sift_profile_collect(double* total_ms, int* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SIFT2NN_H_ */

@@ -1,0 +1,113 @@
+"""B200-native 2-NN SIFT descriptor matching.
+
+Host-side mirror of the reference's matching interface (src/knn_brute.cu,
+src/lsh_h.cu): the functions below keep the reference's names and argument
+order and call the CUDA library ``libsift2nn.so`` through its C ABI
+(``include/sift2nn.h``). Pointers may be given as integers, torch tensors or
+numpy arrays. Unlike the reference, failures are reported: int-returning
+functions return the status, void ones raise :class:`SiftError`.
+
+``match`` is the native convenience call on torch tensors.
+"""
+from __future__ import annotations
+
+import ctypes
+
+from ._native import (FLOAT_DEVICE, FLOAT_HOST, HALF_DEVICE, METRIC_DOT, METRIC_L2, SIFT_ERR_ALLOC,
+                      SIFT_ERR_CUDA, SIFT_ERR_DEVICE_TIMEOUT, SIFT_ERR_INVALID_ARG, SIFT_ERR_NO_DEVICE,
+                      SIFT_ERR_NOT_INTEGER, SIFT_ERR_UNSUPPORTED, SIFT_OK, U8_DEVICE, U8_HOST, LIB_PATH,
+                      SiftError, check, lib, status_string)
+
+__all__ = [
+    "cublas_2nn_sift", "cublas_2nn_f", "device_brute", "host_brute", "match", "stream_status", "version",
+    "SiftError", "FLOAT_HOST", "FLOAT_DEVICE", "HALF_DEVICE", "U8_DEVICE", "U8_HOST", "METRIC_L2", "METRIC_DOT",
+]
+
+
+def _ptr(x):
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if hasattr(x, "ctypes"):
+        return x.ctypes.data
+    if isinstance(x, ctypes.c_void_p):
+        return x.value
+    raise TypeError(f"cannot take the address of {type(x)!r}")
+
+
+def version() -> str:
+    return lib().sift_version().decode()
+
+
+# ----------------------------------------------------- reference interface --
+
+def cublas_2nn_sift(q_points, r_points, type, q_n, r_n, matches, threshold, handle=None, stream_n=1, use=0,
+                    warps=17) -> int:
+    """Exact 2-NN + ratio test (reference src/knn_brute.cu:24). Returns the status code."""
+    return lib().cublas_2nn_sift(_ptr(q_points), _ptr(r_points), type, q_n, r_n, _ptr(matches), threshold,
+                                 _ptr(handle), stream_n, use, warps)
+
+
+def cublas_2nn_f(q_points, r_points, q_n, r_n, sorted, handle=None) -> None:
+    """2-NN ranked by -2 q.r into float4 {d1, d2, i1, i2} (reference src/knn_brute.cu:523)."""
+    lib().cublas_2nn_f(_ptr(q_points), _ptr(r_points), q_n, r_n, _ptr(sorted), _ptr(handle))
+    check(lib().sift_last_status(), "cublas_2nn_f")
+
+
+def device_brute(q_points, r_points, q_n, r_n, sorted) -> None:
+    """Exact squared-L2 2-NN into float4 {d1, d2, i1, i2} (reference src/knn_brute.cu:619)."""
+    lib().device_brute(_ptr(q_points), _ptr(r_points), q_n, r_n, _ptr(sorted))
+    check(lib().sift_last_status(), "device_brute")
+
+
+def host_brute(q_points, r_points, q_points_size, r_points_size, sorted) -> None:
+    """host_brute contract (reference src/knn_brute.cu:801) computed on the GPU for host arrays."""
+    lib().host_brute(_ptr(q_points), _ptr(r_points), q_points_size, r_points_size, _ptr(sorted))
+    check(lib().sift_last_status(), "host_brute")
+
+
+def stream_status(stream=None) -> int:
+    return lib().sift_stream_status(_ptr(stream) if stream is not None else None)
+
+
+# -------------------------------------------------------- native interface --
+
+def match(q, r, threshold: float = 0.8, metric: int = METRIC_L2, stream=None, outputs=("matches", "nn_idx", "nn_dist")):
+    """Exact 2-NN of torch uint8 CUDA tensors q [n, 128] and r [m, 128].
+
+    Returns a dict with the requested outputs as CUDA tensors: ``matches``
+    (int64 view of uint32; UINT32_MAX where the ratio test fails), ``nn_idx``
+    [n, 2] int32 (-1 absent), ``nn_dist`` [n, 2] float32, ``sorted`` [n, 4].
+    Asynchronous on ``stream`` (a torch.cuda.Stream or None for the current one).
+    """
+    import torch
+
+    if q.dtype != torch.uint8 or r.dtype != torch.uint8 or not q.is_cuda or not r.is_cuda:
+        raise TypeError("match() expects uint8 CUDA tensors")
+    if q.dim() != 2 or q.shape[1] != 128 or r.dim() != 2 or r.shape[1] != 128:
+        raise ValueError("descriptors must be [n, 128]")
+    q = q.contiguous()
+    r = r.contiguous()
+    n = q.shape[0]
+    dev = q.device
+    out = {}
+    if "matches" in outputs:
+        out["matches"] = torch.empty(n, dtype=torch.int32, device=dev)
+    if "nn_idx" in outputs:
+        out["nn_idx"] = torch.empty((n, 2), dtype=torch.int32, device=dev)
+    if "nn_dist" in outputs:
+        out["nn_dist"] = torch.empty((n, 2), dtype=torch.float32, device=dev)
+    if "sorted" in outputs:
+        out["sorted"] = torch.empty((n, 4), dtype=torch.float32, device=dev)
+    s = stream if stream is not None else torch.cuda.current_stream(dev)
+    with torch.cuda.device(dev):
+        rc = lib().sift2nn_match(q.data_ptr(), r.data_ptr(), U8_DEVICE, n, r.shape[0], metric, threshold,
+                                 _ptr(out.get("matches")), _ptr(out.get("sorted")), _ptr(out.get("nn_idx")),
+                                 _ptr(out.get("nn_dist")), s.cuda_stream)
+    check(rc, "sift2nn_match")
+    if "matches" in out:
+        out["matches"] = out["matches"].view(torch.uint32) if hasattr(torch, "uint32") else out["matches"]
+    return out

@@ -1,0 +1,76 @@
+"""Loader for libsift2nn.so, the CUDA product library (sm_100a).
+
+There is no CPU path: if the library is missing this module raises, and every
+compute call on a machine without a usable B200 returns SIFT_ERR_NO_DEVICE.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsift2nn.so")
+
+SIFT_OK = 0
+SIFT_ERR_INVALID_ARG = -1
+SIFT_ERR_CUDA = -2
+SIFT_ERR_NOT_INTEGER = -3
+SIFT_ERR_DEVICE_TIMEOUT = -4
+SIFT_ERR_NO_DEVICE = -5
+SIFT_ERR_UNSUPPORTED = -6
+SIFT_ERR_ALLOC = -7
+
+FLOAT_HOST, FLOAT_DEVICE, HALF_DEVICE, U8_DEVICE, U8_HOST = 0, 1, 2, 3, 4
+METRIC_L2, METRIC_DOT = 0, 1
+
+_vp = ctypes.c_void_p
+_PROTOS = {
+    "cublas_2nn_sift": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, _vp,
+                                       ctypes.c_float, _vp, ctypes.c_int, ctypes.c_size_t, ctypes.c_int]),
+    "cublas_2nn_f": (None, [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "device_brute": (None, [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
+    "host_brute": (None, [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
+    "sift_last_status": (ctypes.c_int, []),
+    "sift2nn_match": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
+                                     ctypes.c_float, _vp, _vp, _vp, _vp, _vp]),
+    "sift_stream_status": (ctypes.c_int, [_vp]),
+    "sift_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "sift_version": (ctypes.c_char_p, []),
+    "sift_launch_count": (ctypes.c_longlong, []),
+    "sift_profile_enable": (None, [ctypes.c_int]),
+    "sift_profile_collect": (ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]),
+}
+
+_lib = None
+
+
+class SiftError(RuntimeError):
+    def __init__(self, status: int, where: str = ""):
+        self.status = status
+        msg = status_string(status) if _lib is not None else str(status)
+        super().__init__(f"{where}: {msg} ({status})" if where else f"{msg} ({status})")
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded product library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `make -C matching_sift_b200` "
+                              "(or __graft_entry__.build()); there is no CPU fallback")
+        so = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _PROTOS.items():
+            f = getattr(so, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = so
+    return _lib
+
+
+def status_string(status: int) -> str:
+    return lib().sift_status_string(status).decode()
+
+
+def check(status: int, where: str = "") -> None:
+    if status != SIFT_OK:
+        raise SiftError(status, where)

@@ -1,0 +1,444 @@
+// C ABI of the matcher (include/sift2nn.h): per-device context, scratch arena,
+// input staging, TMA descriptor construction and the launch sequence
+//   [pack f32/f16 -> u8] -> row norms -> exact2nn (tcgen05) -> merge.
+#include <cfloat>
+#include <cstdio>
+#include <cstring>
+#include <atomic>
+#include <mutex>
+#include <vector>
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+#include "sift2nn.h"
+#include "api_internal.h"
+#include "exact2nn.cuh"
+#include "pack.cuh"
+
+namespace sift {
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+
+struct DeviceCtx {
+    std::mutex mu;
+    bool ready = false;
+    int num_sms = 0;
+    char* arena = nullptr;
+    size_t arena_bytes = 0;
+    int* d_status = nullptr;  // [0] device error code, [1] pack flag
+    int* h_status = nullptr;  // pinned mirror of d_status
+};
+
+DeviceCtx g_ctx[kMaxDevices];
+std::mutex g_init_mu;
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+thread_local int t_last_status = SIFT_OK;
+std::atomic<long long> g_launches{0};
+std::atomic<bool> g_profile{false};
+std::mutex g_prof_mu;
+std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_prof_events;
+
+// 256-byte aligned bump layout over the arena.
+struct Layout {
+    size_t off = 0;
+    size_t take(size_t bytes) {
+        off = (off + 255) & ~static_cast<size_t>(255);
+        const size_t o = off;
+        off += bytes;
+        return o;
+    }
+};
+
+int ensure_ready(DeviceCtx*& out, int& dev) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        return SIFT_ERR_NO_DEVICE;
+    }
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return SIFT_ERR_NO_DEVICE;
+    DeviceCtx& c = g_ctx[dev];
+    {
+        std::lock_guard<std::mutex> lk(g_init_mu);
+        if (!g_encode) {
+            void* fn = nullptr;
+            cudaDriverEntryPointQueryResult q{};
+            if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) !=
+                    cudaSuccess ||
+                q != cudaDriverEntryPointSuccess || !fn)
+                return SIFT_ERR_CUDA;
+            g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+        }
+        if (!c.ready) {
+            cudaDeviceProp prop{};
+            if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return SIFT_ERR_CUDA;
+            if (prop.major != 10) return SIFT_ERR_UNSUPPORTED;  // sm_100a code only
+            c.num_sms = prop.multiProcessorCount;
+            if (cudaMalloc(&c.d_status, 4 * sizeof(int)) != cudaSuccess) return SIFT_ERR_ALLOC;
+            if (cudaMemset(c.d_status, 0, 4 * sizeof(int)) != cudaSuccess) return SIFT_ERR_CUDA;
+            if (cudaMallocHost(&c.h_status, 4 * sizeof(int)) != cudaSuccess) return SIFT_ERR_ALLOC;
+            if (cudaDeviceSynchronize() != cudaSuccess) return SIFT_ERR_CUDA;
+            c.ready = true;
+        }
+    }
+    out = &c;
+    return SIFT_OK;
+}
+
+int ensure_arena(DeviceCtx& c, size_t bytes) {
+    if (bytes <= c.arena_bytes) return SIFT_OK;
+    if (c.arena) {
+        cudaDeviceSynchronize();
+        cudaFree(c.arena);
+        c.arena = nullptr;
+        c.arena_bytes = 0;
+    }
+    size_t cap = bytes + bytes / 8 + (1 << 20);
+    if (cudaMalloc(&c.arena, cap) != cudaSuccess) {
+        cudaGetLastError();
+        return SIFT_ERR_ALLOC;
+    }
+    c.arena_bytes = cap;
+    return SIFT_OK;
+}
+
+bool is_device_accessible(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+int encode_u8_rows(CUtensorMap* m, const void* base, uint64_t rows, uint32_t box_rows) {
+    cuuint64_t dims[2] = {static_cast<cuuint64_t>(kDim), static_cast<cuuint64_t>(rows)};
+    cuuint64_t strides[1] = {static_cast<cuuint64_t>(kDim)};
+    cuuint32_t box[2] = {static_cast<cuuint32_t>(kDim), box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? SIFT_OK : SIFT_ERR_CUDA;
+}
+
+int map_cuda(cudaError_t e) {
+    if (e == cudaSuccess) return SIFT_OK;
+    if (e == cudaErrorMemoryAllocation) return SIFT_ERR_ALLOC;
+    return SIFT_ERR_CUDA;
+}
+
+#define SIFT_TRY(expr)                 \
+    do {                               \
+        int _rc = (expr);              \
+        if (_rc != SIFT_OK) return _rc; \
+    } while (0)
+#define SIFT_CUDA(expr) SIFT_TRY(map_cuda(expr))
+
+// Reads and clears the device status words. Caller has synchronised `st`.
+int collect_device_status(DeviceCtx& c, cudaStream_t st) {
+    SIFT_CUDA(cudaMemcpyAsync(c.h_status, c.d_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    SIFT_CUDA(cudaStreamSynchronize(st));
+    const int code = c.h_status[0];
+    if (code != 0) {
+        SIFT_CUDA(cudaMemsetAsync(c.d_status, 0, sizeof(int), st));
+        SIFT_CUDA(cudaStreamSynchronize(st));
+        return SIFT_ERR_DEVICE_TIMEOUT;
+    }
+    return SIFT_OK;
+}
+
+}  // namespace
+
+// Core of every exact entry point.
+int exact_match(const MatchArgs& a) {
+    if (a.q_n > 0 && !a.q) return SIFT_ERR_INVALID_ARG;
+    if (a.r_n > 0 && !a.r) return SIFT_ERR_INVALID_ARG;
+    if (a.type < SIFT_FLOAT_HOST || a.type > SIFT_U8_HOST) return SIFT_ERR_INVALID_ARG;
+    if (a.metric != SIFT_METRIC_L2 && a.metric != SIFT_METRIC_DOT) return SIFT_ERR_INVALID_ARG;
+    if (a.q_n > 0x7fffffffu - 256 || a.r_n > 0x7fffffffu - 256) return SIFT_ERR_INVALID_ARG;
+    DeviceCtx* cp = nullptr;
+    int dev = 0;
+    SIFT_TRY(ensure_ready(cp, dev));
+    DeviceCtx& c = *cp;
+    std::lock_guard<std::mutex> lk(c.mu);
+    cudaStream_t st = static_cast<cudaStream_t>(a.stream);
+    const int q_n = static_cast<int>(a.q_n), r_n = static_cast<int>(a.r_n);
+    if (q_n == 0) return SIFT_OK;
+
+    const ExactPlan plan = make_exact_plan(q_n, r_n, c.num_sms);
+
+    // Output placement: direct when the device can write the pointer, else staged.
+    const bool m_dev = !a.matches || is_device_accessible(a.matches);
+    const bool s_dev = !a.sorted || is_device_accessible(a.sorted);
+    const bool i_dev = !a.nn_idx || is_device_accessible(a.nn_idx);
+    const bool d_dev = !a.nn_dist || is_device_accessible(a.nn_dist);
+    const bool host_out = !(m_dev && s_dev && i_dev && d_dev);
+
+    // Input placement.
+    const uint8_t* qd = nullptr;
+    const uint8_t* rd = nullptr;
+    const void* q_src = a.q;
+    const void* r_src = a.r;
+    bool need_pack = a.type != SIFT_U8_DEVICE && a.type != SIFT_U8_HOST;
+    bool stage_u8 = a.type == SIFT_U8_HOST;
+    bool stage_f32 = false;
+    if (a.type == SIFT_U8_DEVICE) {
+        // TMA needs 16-byte aligned rows; unaligned device input is copied.
+        stage_u8 = (reinterpret_cast<uintptr_t>(a.q) & 15) || (reinterpret_cast<uintptr_t>(a.r) & 15);
+    }
+    if (a.type == SIFT_FLOAT_HOST) {
+        // Zero-copy like the reference (src/knn_brute.cu:58, :223) when the
+        // memory is mapped pinned memory; otherwise stage it.
+        void* qm = nullptr;
+        void* rm = nullptr;
+        if (cudaHostGetDevicePointer(&qm, const_cast<void*>(a.q), 0) == cudaSuccess &&
+            (r_n == 0 || cudaHostGetDevicePointer(&rm, const_cast<void*>(a.r), 0) == cudaSuccess) &&
+            !(reinterpret_cast<uintptr_t>(qm) & 15) && !(reinterpret_cast<uintptr_t>(rm) & 15)) {
+            q_src = qm;
+            r_src = rm;
+        } else {
+            cudaGetLastError();
+            stage_f32 = true;
+        }
+    }
+    if ((a.type == SIFT_FLOAT_DEVICE || a.type == SIFT_HALF_DEVICE) &&
+        ((reinterpret_cast<uintptr_t>(a.q) & 15) || (reinterpret_cast<uintptr_t>(a.r) & 15)))
+        return SIFT_ERR_INVALID_ARG;
+
+    Layout L;
+    const size_t o_qu8 = (need_pack || stage_u8) ? L.take(static_cast<size_t>(q_n) * kDim) : 0;
+    const size_t o_ru8 = (need_pack || stage_u8) ? L.take(static_cast<size_t>(r_n) * kDim + 16) : 0;
+    const size_t o_qf = stage_f32 ? L.take(static_cast<size_t>(q_n) * kDim * 4) : 0;
+    const size_t o_rf = stage_f32 ? L.take(static_cast<size_t>(r_n) * kDim * 4 + 16) : 0;
+    const size_t o_bnorm = L.take(static_cast<size_t>(plan.r_pad) * 4 + 16);
+    const size_t o_bgmin = L.take(static_cast<size_t>(plan.r_pad / 32) * 4 + 16);
+    const size_t o_qnorm = L.take(static_cast<size_t>(plan.q_pad) * 4);
+    const size_t o_part = L.take(static_cast<size_t>(plan.max_splits) * 2 * plan.q_pad * sizeof(int4));
+    const size_t o_m = (a.matches && !m_dev) ? L.take(static_cast<size_t>(q_n) * 4) : 0;
+    const size_t o_s = (a.sorted && !s_dev) ? L.take(static_cast<size_t>(q_n) * 16) : 0;
+    const size_t o_i = (a.nn_idx && !i_dev) ? L.take(static_cast<size_t>(q_n) * 8) : 0;
+    const size_t o_d = (a.nn_dist && !d_dev) ? L.take(static_cast<size_t>(q_n) * 8) : 0;
+    SIFT_TRY(ensure_arena(c, L.off));
+    char* A = c.arena;
+
+    // ---- inputs
+    if (a.type == SIFT_U8_DEVICE && !stage_u8) {
+        qd = static_cast<const uint8_t*>(a.q);
+        rd = static_cast<const uint8_t*>(a.r);
+    } else if (stage_u8) {
+        const cudaMemcpyKind k = a.type == SIFT_U8_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+        SIFT_CUDA(cudaMemcpyAsync(A + o_qu8, a.q, static_cast<size_t>(q_n) * kDim, k, st));
+        if (r_n) SIFT_CUDA(cudaMemcpyAsync(A + o_ru8, a.r, static_cast<size_t>(r_n) * kDim, k, st));
+        qd = reinterpret_cast<uint8_t*>(A + o_qu8);
+        rd = reinterpret_cast<uint8_t*>(A + o_ru8);
+    } else {
+        if (stage_f32) {
+            SIFT_CUDA(cudaMemcpyAsync(A + o_qf, a.q, static_cast<size_t>(q_n) * kDim * 4, cudaMemcpyHostToDevice, st));
+            if (r_n)
+                SIFT_CUDA(
+                    cudaMemcpyAsync(A + o_rf, a.r, static_cast<size_t>(r_n) * kDim * 4, cudaMemcpyHostToDevice, st));
+            q_src = A + o_qf;
+            r_src = A + o_rf;
+        }
+        SIFT_CUDA(cudaMemsetAsync(c.d_status + 1, 0, sizeof(int), st));
+        uint8_t* qo = reinterpret_cast<uint8_t*>(A + o_qu8);
+        uint8_t* ro = reinterpret_cast<uint8_t*>(A + o_ru8);
+        g_launches += r_n > 0 ? 2 : 1;
+        if (a.type == SIFT_HALF_DEVICE) {
+            SIFT_CUDA(launch_pack_f16_u8(q_src, q_n, qo, c.d_status + 1, c.num_sms, st));
+            SIFT_CUDA(launch_pack_f16_u8(r_src, r_n, ro, c.d_status + 1, c.num_sms, st));
+        } else {
+            SIFT_CUDA(launch_pack_f32_u8(static_cast<const float*>(q_src), q_n, qo, c.d_status + 1, c.num_sms, st));
+            SIFT_CUDA(launch_pack_f32_u8(static_cast<const float*>(r_src), r_n, ro, c.d_status + 1, c.num_sms, st));
+        }
+        SIFT_CUDA(cudaMemcpyAsync(c.h_status + 1, c.d_status + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+        SIFT_CUDA(cudaStreamSynchronize(st));
+        if (c.h_status[1] != 0) return SIFT_ERR_NOT_INTEGER;
+        qd = qo;
+        rd = ro;
+    }
+
+    // ---- norms
+    int32_t* bnorm = reinterpret_cast<int32_t*>(A + o_bnorm);
+    int32_t* bgmin = reinterpret_cast<int32_t*>(A + o_bgmin);
+    int32_t* qnorm = reinterpret_cast<int32_t*>(A + o_qnorm);
+    SIFT_CUDA(launch_row_norms_u8(rd, r_n, plan.r_pad, a.metric, bnorm, bgmin, st));
+    SIFT_CUDA(launch_row_norms_u8(qd, q_n, plan.q_pad, kMetricL2, qnorm, nullptr, st));
+    g_launches += (plan.r_pad > 0 ? 1 : 0) + 1;
+
+    // ---- fused GEMM + top-2
+    int4* partial = reinterpret_cast<int4*>(A + o_part);
+    if (r_n > 0) {
+        CUtensorMap qmap, bmap;
+        SIFT_TRY(encode_u8_rows(&qmap, qd, q_n, kBM));
+        SIFT_TRY(encode_u8_rows(&bmap, rd, r_n, kBN));
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        const bool prof = g_profile.load();
+        if (prof) {
+            SIFT_CUDA(cudaEventCreate(&e0));
+            SIFT_CUDA(cudaEventCreate(&e1));
+            SIFT_CUDA(cudaEventRecord(e0, st));
+        }
+        SIFT_CUDA(launch_exact2nn_u8(qmap, bmap, bnorm, bgmin, plan, partial, c.d_status, st));
+        ++g_launches;
+        if (prof) {
+            SIFT_CUDA(cudaEventRecord(e1, st));
+            std::lock_guard<std::mutex> pl(g_prof_mu);
+            g_prof_events.emplace_back(e0, e1);
+        }
+    }
+
+    // ---- merge + outputs
+    uint32_t* m_out = (a.matches && !m_dev) ? reinterpret_cast<uint32_t*>(A + o_m) : a.matches;
+    float4* s_out = (a.sorted && !s_dev) ? reinterpret_cast<float4*>(A + o_s) : reinterpret_cast<float4*>(a.sorted);
+    int32_t* i_out = (a.nn_idx && !i_dev) ? reinterpret_cast<int32_t*>(A + o_i) : a.nn_idx;
+    float* d_out = (a.nn_dist && !d_dev) ? reinterpret_cast<float*>(A + o_d) : a.nn_dist;
+    SIFT_CUDA(launch_merge2nn(partial, plan, qnorm, a.metric, a.threshold, m_out, s_out, i_out, d_out, st));
+    ++g_launches;
+    if (a.matches && !m_dev)
+        SIFT_CUDA(cudaMemcpyAsync(a.matches, m_out, static_cast<size_t>(q_n) * 4, cudaMemcpyDeviceToHost, st));
+    if (a.sorted && !s_dev)
+        SIFT_CUDA(cudaMemcpyAsync(a.sorted, s_out, static_cast<size_t>(q_n) * 16, cudaMemcpyDeviceToHost, st));
+    if (a.nn_idx && !i_dev)
+        SIFT_CUDA(cudaMemcpyAsync(a.nn_idx, i_out, static_cast<size_t>(q_n) * 8, cudaMemcpyDeviceToHost, st));
+    if (a.nn_dist && !d_dev)
+        SIFT_CUDA(cudaMemcpyAsync(a.nn_dist, d_out, static_cast<size_t>(q_n) * 8, cudaMemcpyDeviceToHost, st));
+
+    const bool host_in = a.type == SIFT_U8_HOST || a.type == SIFT_FLOAT_HOST;
+    if (a.sync || host_out || host_in) {
+        SIFT_CUDA(cudaStreamSynchronize(st));
+        return collect_device_status(c, st);
+    }
+    return SIFT_OK;
+}
+
+int stream_status(void* stream) {
+    DeviceCtx* cp = nullptr;
+    int dev = 0;
+    SIFT_TRY(ensure_ready(cp, dev));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    SIFT_CUDA(cudaStreamSynchronize(st));
+    std::lock_guard<std::mutex> lk(cp->mu);
+    return collect_device_status(*cp, st);
+}
+
+int profile_collect(double* total_ms, int* launches) {
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+    {
+        std::lock_guard<std::mutex> pl(g_prof_mu);
+        ev.swap(g_prof_events);
+    }
+    double tot = 0.0;
+    int rc = SIFT_OK;
+    for (auto& p : ev) {
+        float ms = 0.f;
+        if (cudaEventSynchronize(p.second) != cudaSuccess || cudaEventElapsedTime(&ms, p.first, p.second) != cudaSuccess)
+            rc = SIFT_ERR_CUDA;
+        tot += ms;
+        cudaEventDestroy(p.first);
+        cudaEventDestroy(p.second);
+    }
+    if (total_ms) *total_ms = tot;
+    if (launches) *launches = static_cast<int>(ev.size());
+    return rc;
+}
+
+long long launch_count() { return g_launches.load(); }
+void profile_enable(bool on) { g_profile.store(on); }
+
+void set_last_status(int s) { t_last_status = s; }
+int last_status() { return t_last_status; }
+
+}  // namespace sift
+
+// ------------------------------------------------------------------ C ABI --
+using sift::MatchArgs;
+
+extern "C" {
+
+int sift_impl_cublas_2nn_sift(void* q_points, void* r_points, int type, uint32_t q_n, uint32_t r_n,
+                              uint32_t* matches, float threshold) {
+    if (!matches && q_n) return SIFT_ERR_INVALID_ARG;
+    MatchArgs a{};
+    a.q = q_points; a.r = r_points; a.type = type; a.q_n = q_n; a.r_n = r_n;
+    a.metric = SIFT_METRIC_L2; a.threshold = threshold; a.matches = matches; a.sync = true;
+    return sift::exact_match(a);
+}
+
+void sift_impl_cublas_2nn_f(void* q_points, void* r_points, int q_n, int r_n, void* sorted) {
+    if (q_n < 0 || r_n < 0 || (q_n && !sorted)) { sift::set_last_status(SIFT_ERR_INVALID_ARG); return; }
+    MatchArgs a{};
+    a.q = q_points; a.r = r_points; a.type = SIFT_FLOAT_DEVICE; a.q_n = q_n; a.r_n = r_n;
+    a.metric = SIFT_METRIC_DOT; a.threshold = 0.8f; a.sorted = static_cast<sift_float4*>(sorted); a.sync = true;
+    sift::set_last_status(sift::exact_match(a));
+}
+
+void sift_impl_device_brute(void* q_points, void* r_points, int q_n, int r_n, void* sorted) {
+    if (q_n < 0 || r_n < 0 || (q_n && !sorted)) { sift::set_last_status(SIFT_ERR_INVALID_ARG); return; }
+    MatchArgs a{};
+    a.q = q_points; a.r = r_points; a.type = SIFT_FLOAT_DEVICE; a.q_n = q_n; a.r_n = r_n;
+    a.metric = SIFT_METRIC_L2; a.threshold = 0.8f; a.sorted = static_cast<sift_float4*>(sorted); a.sync = true;
+    sift::set_last_status(sift::exact_match(a));
+}
+
+void sift_impl_host_brute(void* q_points, void* r_points, int q_n, int r_n, void* sorted) {
+    if (q_n < 0 || r_n < 0 || (q_n && !sorted)) { sift::set_last_status(SIFT_ERR_INVALID_ARG); return; }
+    MatchArgs a{};
+    a.q = q_points; a.r = r_points; a.type = SIFT_FLOAT_HOST; a.q_n = q_n; a.r_n = r_n;
+    a.metric = SIFT_METRIC_L2; a.threshold = 0.8f; a.sorted = static_cast<sift_float4*>(sorted); a.sync = true;
+    sift::set_last_status(sift::exact_match(a));
+}
+
+int cublas_2nn_sift(void* q_points, void* r_points, int type, uint32_t q_n, uint32_t r_n, uint32_t* matches,
+                    float threshold, cublasHandle_t, int, size_t, int) {
+    return sift_impl_cublas_2nn_sift(q_points, r_points, type, q_n, r_n, matches, threshold);
+}
+
+void cublas_2nn_f(des_t_f* q_points, des_t_f* r_points, int q_n, int r_n, sift_float4* sorted, cublasHandle_t) {
+    sift_impl_cublas_2nn_f(q_points, r_points, q_n, r_n, sorted);
+}
+
+void device_brute(des_t_f* q_points, des_t_f* r_points, int q_n, int r_n, sift_float4* sorted) {
+    sift_impl_device_brute(q_points, r_points, q_n, r_n, sorted);
+}
+
+void host_brute(des_t_f* q_points, des_t_f* r_points, int q_points_size, int r_points_size, sift_float4* sorted) {
+    sift_impl_host_brute(q_points, r_points, q_points_size, r_points_size, sorted);
+}
+
+int sift_last_status(void) { return sift::last_status(); }
+
+int sift2nn_match(const void* q, const void* r, int type, uint32_t q_n, uint32_t r_n, int metric, float threshold,
+                  uint32_t* matches, sift_float4* sorted, int32_t* nn_idx, float* nn_dist, void* stream) {
+    MatchArgs a{};
+    a.q = q; a.r = r; a.type = type; a.q_n = q_n; a.r_n = r_n; a.metric = metric; a.threshold = threshold;
+    a.matches = matches; a.sorted = sorted; a.nn_idx = nn_idx; a.nn_dist = nn_dist; a.stream = stream;
+    a.sync = false;
+    return sift::exact_match(a);
+}
+
+int sift_stream_status(void* stream) { return sift::stream_status(stream); }
+
+const char* sift_status_string(int s) {
+    switch (s) {
+        case SIFT_OK: return "ok";
+        case SIFT_ERR_INVALID_ARG: return "invalid argument";
+        case SIFT_ERR_CUDA: return "CUDA error";
+        case SIFT_ERR_NOT_INTEGER: return "descriptor values are not integers in [0, 255]";
+        case SIFT_ERR_DEVICE_TIMEOUT: return "a bounded wait inside a kernel expired";
+        case SIFT_ERR_NO_DEVICE: return "no usable CUDA device";
+        case SIFT_ERR_UNSUPPORTED: return "unsupported device or input";
+        case SIFT_ERR_ALLOC: return "device allocation failed";
+        default: return "unknown status";
+    }
+}
+
+const char* sift_version(void) { return "sift2nn-b200 0.1.0 (sm_100a)"; }
+
+long long sift_launch_count(void) { return sift::launch_count(); }
+void sift_profile_enable(int on) { sift::profile_enable(on != 0); }
+int sift_profile_collect(double* total_ms, int* launches) { return sift::profile_collect(total_ms, launches); }
+
+}  // extern "C"

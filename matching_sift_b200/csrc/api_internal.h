@@ -1,0 +1,40 @@
+// Internal interface between the C ABI entry points and the implementation.
+#pragma once
+#include <cstdint>
+#include "sift2nn.h"
+
+namespace sift {
+
+struct MatchArgs {
+    const void* q = nullptr;
+    const void* r = nullptr;
+    int type = SIFT_U8_DEVICE;
+    uint32_t q_n = 0, r_n = 0;
+    int metric = SIFT_METRIC_L2;
+    float threshold = 0.8f;
+    uint32_t* matches = nullptr;
+    sift_float4* sorted = nullptr;
+    int32_t* nn_idx = nullptr;
+    float* nn_dist = nullptr;
+    void* stream = nullptr;
+    bool sync = false;  // synchronise and collect the device status before returning
+};
+
+int exact_match(const MatchArgs& a);
+int stream_status(void* stream);
+void set_last_status(int s);
+int profile_collect(double* total_ms, int* launches);
+long long launch_count();
+void profile_enable(bool on);
+int last_status();
+
+}  // namespace sift
+
+// C-linkage implementations used by the mangled C++ forwarders (compat_cxx.cpp).
+extern "C" {
+int sift_impl_cublas_2nn_sift(void* q_points, void* r_points, int type, uint32_t q_n, uint32_t r_n,
+                              uint32_t* matches, float threshold);
+void sift_impl_cublas_2nn_f(void* q_points, void* r_points, int q_n, int r_n, void* sorted);
+void sift_impl_device_brute(void* q_points, void* r_points, int q_n, int r_n, void* sorted);
+void sift_impl_host_brute(void* q_points, void* r_points, int q_n, int r_n, void* sorted);
+}

@@ -1,0 +1,488 @@
+// Exact 2-NN of u8 SIFT descriptors on sm_100a: one persistent, warp-
+// specialised kernel computes q.b on the 5th-generation tensor cores
+// (tcgen05.mma kind::i8, u8 x u8 -> s32, accumulators in TMEM, operands
+// staged by TMA) and reduces every accumulator tile to a per-query top-2 in
+// the epilogue, so the queries x base distance matrix never reaches HBM.
+//
+// Replaces the reference's GEMM + scan pairs:
+//   cublasHgemm / cublasGemmEx   src/knn_brute.cu:244, :592   (dist = -2 q.r to HBM)
+//   find_matches / min_dist_f    src/knn_brute.cu:340-448, :726-796 (scan of dist)
+//   sqrEuclidianDist             src/knn_brute.cu:671-691     (full squared L2)
+//
+// Ranking key. For query q and base row b the kernel ranks by
+//     key(b) = norm(b) - 2 q.b        (norm(b) = |b|^2 for kMetricL2, 0 for kMetricDot)
+// which orders candidates exactly like |q - b|^2 = |q|^2 + key (resp. -2 q.b).
+// All values are exact integers: |key| <= 2 * 128 * 255^2 < 2^25.
+// Ties are broken by the lower base index (lexicographic (key, index) order),
+// which is the order of the reference's host_brute (src/knn_brute.cu:816-831).
+//
+// Warp roles (kThreads = 320):
+//   warp 0      TMA producer: query tiles (resident per query group) and a
+//               kStages ring of base tiles
+//   warp 1      TMEM allocator + single-thread MMA issuer
+//   warps 2..9  epilogue: warp w reads TMEM lane quarter (w % 4), half
+//               (w - 2) / 4 of the 256 columns of every accumulator slot
+//
+// Epilogue filter. Per group of 32 base rows the epilogue takes the largest
+// dot product m of its query row and the smallest norm n_min of the group
+// (precomputed): if n_min - 2 m >= key2 (the query's current second-best key)
+// no row of the group can enter the top-2 and the group costs ~1 instruction
+// per element. Otherwise (rare once the top-2 has settled) the exact keys of
+// the 32 rows are formed and merged in index order.
+#include <cfloat>
+#include <climits>
+#include <algorithm>
+#include "exact2nn.cuh"
+#include "ptx.cuh"
+
+namespace sift {
+
+namespace {
+
+constexpr int kQTileBytes = kBM * kDim;  // 16 KB: one query tile (u8)
+constexpr int kBTileBytes = kBN * kDim;  // 32 KB: one base tile (u8)
+
+struct __align__(8) SmemCtl {
+    uint64_t full[kStages];
+    uint64_t empty[kStages];
+    uint64_t qfull, qempty;
+    uint64_t tfull[2], tempty[2];
+    uint64_t drain;
+    uint32_t tmem_base;
+    int abort_flag;
+};
+
+constexpr size_t kSmemBytes = 1024 + kQT * kQTileBytes + kStages * kBTileBytes + sizeof(SmemCtl);
+
+__device__ __forceinline__ int max32(const uint32_t (&v)[32]) {
+    int m[11];
+    #pragma unroll
+    for (int i = 0; i < 10; ++i)
+        m[i] = __vimax3_s32(static_cast<int>(v[3 * i]), static_cast<int>(v[3 * i + 1]), static_cast<int>(v[3 * i + 2]));
+    m[10] = max(static_cast<int>(v[30]), static_cast<int>(v[31]));
+    int a = __vimax3_s32(m[0], m[1], m[2]);
+    int b = __vimax3_s32(m[3], m[4], m[5]);
+    int c = __vimax3_s32(m[6], m[7], m[8]);
+    int d = max(m[9], m[10]);
+    return max(__vimax3_s32(a, b, c), d);
+}
+
+__device__ __forceinline__ void top2_update(int key, int idx, int& k1, int& i1, int& k2, int& i2) {
+    if (key < k2) {
+        if (key < k1) {
+            k2 = k1; i2 = i1;
+            k1 = key; i1 = idx;
+        } else {
+            k2 = key; i2 = idx;
+        }
+    }
+}
+
+// One group of 32 consecutive base rows [row0, row0 + 32) for this thread's
+// query row; v[c] = q.b(row0 + c).
+__device__ __forceinline__ void scan_group(const uint32_t (&v)[32], int row0, int gmin,
+                                           const int32_t* __restrict__ bnorm, int& k1, int& i1, int& k2, int& i2) {
+    const int mx = max32(v);
+    const bool pass = (gmin - 2 * mx) < k2;
+    if (__any_sync(0xffffffffu, pass)) {
+        if (pass) {
+            const int4* nb4 = reinterpret_cast<const int4*>(bnorm + row0);
+            #pragma unroll
+            for (int c4 = 0; c4 < 8; ++c4) {
+                const int4 nb = __ldg(nb4 + c4);
+                top2_update(nb.x - 2 * static_cast<int>(v[4 * c4 + 0]), row0 + 4 * c4 + 0, k1, i1, k2, i2);
+                top2_update(nb.y - 2 * static_cast<int>(v[4 * c4 + 1]), row0 + 4 * c4 + 1, k1, i1, k2, i2);
+                top2_update(nb.z - 2 * static_cast<int>(v[4 * c4 + 2]), row0 + 4 * c4 + 2, k1, i1, k2, i2);
+                top2_update(nb.w - 2 * static_cast<int>(v[4 * c4 + 3]), row0 + 4 * c4 + 3, k1, i1, k2, i2);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) row_norms_u8_kernel(const uint8_t* __restrict__ x, int n, int n_pad,
+                                                           int metric, int32_t* __restrict__ norm,
+                                                           int32_t* __restrict__ gmin) {
+    // 32 rows per block, 8 threads per row, 16 bytes per thread.
+    const int row = blockIdx.x * 32 + (threadIdx.x >> 3);
+    const int sub = threadIdx.x & 7;
+    uint32_t s = 0;
+    if (row < n) {
+        const uint4 w = reinterpret_cast<const uint4*>(x + static_cast<size_t>(row) * kDim)[sub];
+        s = __dp4a(w.x, w.x, 0u);
+        s = __dp4a(w.y, w.y, s);
+        s = __dp4a(w.z, w.z, s);
+        s = __dp4a(w.w, w.w, s);
+    }
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    s += __shfl_xor_sync(0xffffffffu, s, 4);
+    const int32_t v = row < n ? (metric == kMetricL2 ? static_cast<int32_t>(s) : 0) : kKeyPad;
+    if (sub == 0 && row < n_pad && norm) norm[row] = v;
+    int m = v;
+    m = min(m, __shfl_xor_sync(0xffffffffu, m, 8));
+    m = min(m, __shfl_xor_sync(0xffffffffu, m, 16));
+    __shared__ int wmin[8];
+    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0 && gmin) {
+        int mm = wmin[0];
+        #pragma unroll
+        for (int i = 1; i < 8; ++i) mm = min(mm, wmin[i]);
+        gmin[blockIdx.x] = mm;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    exact2nn_u8_kernel(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap bmap,
+                       const int32_t* __restrict__ bnorm, const int32_t* __restrict__ bgmin, const ExactPlan plan,
+                       int4* __restrict__ partial, int* __restrict__ err) {
+    extern __shared__ uint8_t smem_raw[];
+    // 1024-byte alignment for the 128-byte swizzle atoms.
+    const uint32_t raw_u32 = ptx::smem_u32(smem_raw);
+    uint8_t* smem = smem_raw + ((1024u - (raw_u32 & 1023u)) & 1023u);
+    uint8_t* q_smem = smem;
+    uint8_t* b_smem = smem + kQT * kQTileBytes;
+    SmemCtl* ctl = reinterpret_cast<SmemCtl*>(b_smem + kStages * kBTileBytes);
+    const uint32_t q_s = ptx::smem_u32(q_smem);
+    const uint32_t b_s = ptx::smem_u32(b_smem);
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long W = plan.units;
+    const long long G = plan.grid;
+    const long long w_begin = plan_w0(blockIdx.x, W, G);
+    const long long w_end = plan_w0(blockIdx.x + 1, W, G);
+    const int BT = plan.base_tiles;
+
+    const uint32_t bar_full = ptx::smem_u32(&ctl->full[0]);
+    const uint32_t bar_empty = ptx::smem_u32(&ctl->empty[0]);
+    const uint32_t bar_qfull = ptx::smem_u32(&ctl->qfull);
+    const uint32_t bar_qempty = ptx::smem_u32(&ctl->qempty);
+    const uint32_t bar_tfull = ptx::smem_u32(&ctl->tfull[0]);
+    const uint32_t bar_tempty = ptx::smem_u32(&ctl->tempty[0]);
+    const uint32_t bar_drain = ptx::smem_u32(&ctl->drain);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            ptx::mbar_init(bar_full + 8 * s, 1);
+            ptx::mbar_init(bar_empty + 8 * s, 1);
+        }
+        ptx::mbar_init(bar_qfull, 1);
+        ptx::mbar_init(bar_qempty, 1);
+        for (int i = 0; i < 2; ++i) {
+            ptx::mbar_init(bar_tfull + 8 * i, 1);
+            ptx::mbar_init(bar_tempty + 8 * i, kEpiWarps);
+        }
+        ptx::mbar_init(bar_drain, 1);
+        ctl->abort_flag = 0;
+        ptx::fence_mbar_init();
+    }
+    if (warp == 1) {
+        ptx::tmem_alloc(ptx::smem_u32(&ctl->tmem_base), kTmemCols);
+        ptx::tmem_relinquish();
+    }
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::tc_fence_after();
+    const uint32_t tmem = ctl->tmem_base;
+    volatile int* abort_flag = &ctl->abort_flag;
+    // A second flag that never aborts drain waits (they stay time-bounded).
+    __shared__ int no_abort;
+    if (threadIdx.x == 0) no_abort = 0;
+    __syncthreads();
+    volatile int* never = &no_abort;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ------------------------------------------------ TMA producer
+            ptx::tma_prefetch_desc(&qmap);
+            ptx::tma_prefetch_desc(&bmap);
+            int cur_g = -1, ngroups = 0;
+            long long n = 0;
+            for (long long w = w_begin; w < w_end; ++w) {
+                const int g = static_cast<int>(w / BT);
+                const int j = static_cast<int>(w - static_cast<long long>(g) * BT);
+                if (g != cur_g) {
+                    if (ngroups > 0 &&
+                        !ptx::mbar_wait(bar_qempty, (ngroups - 1) & 1, abort_flag, err, kErrWaitQuery))
+                        break;
+                    const int t0 = g * kQT;
+                    const int nqt = min(kQT, plan.q_tiles - t0);
+                    ptx::mbar_arrive_expect_tx(bar_qfull, nqt * kQTileBytes);
+                    for (int t = 0; t < nqt; ++t)
+                        ptx::tma_load_2d(q_s + t * kQTileBytes, &qmap, 0, (t0 + t) * kBM, bar_qfull);
+                    cur_g = g;
+                    ++ngroups;
+                }
+                const int s = static_cast<int>(n % kStages);
+                const uint32_t r = static_cast<uint32_t>(n / kStages);
+                if (!ptx::mbar_wait(bar_empty + 8 * s, (r & 1) ^ 1, abort_flag, err, kErrWaitProducer)) break;
+                ptx::mbar_arrive_expect_tx(bar_full + 8 * s, kBTileBytes);
+                ptx::tma_load_2d(b_s + s * kBTileBytes, &bmap, 0, j * kBN, bar_full + 8 * s);
+                ++n;
+            }
+            // Drain: every issued copy lands before the CTA may exit.
+            for (long long k = (n > kStages ? n - kStages : 0); k < n; ++k)
+                ptx::mbar_wait(bar_full + 8 * static_cast<int>(k % kStages), static_cast<uint32_t>(k / kStages) & 1,
+                               never, err, kErrWaitDrain);
+            if (ngroups > 0) ptx::mbar_wait(bar_qfull, (ngroups - 1) & 1, never, err, kErrWaitDrain);
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // -------------------------------------------------- MMA issuer
+            constexpr uint32_t idesc = ptx::idesc_make(2 /*S32*/, 0 /*u8*/, 0 /*u8*/, kBM, kBN);
+            int cur_g = -1, ngroups = 0, nqt = 0;
+            long long n = 0;
+            uint32_t it = 0;
+            bool ok = true;
+            for (long long w = w_begin; w < w_end && ok; ++w, ++n) {
+                const int g = static_cast<int>(w / BT);
+                if (g != cur_g) {
+                    if (!ptx::mbar_wait(bar_qfull, ngroups & 1, abort_flag, err, kErrWaitQuery)) break;
+                    cur_g = g;
+                    ++ngroups;
+                    nqt = min(kQT, plan.q_tiles - g * kQT);
+                }
+                const int s = static_cast<int>(n % kStages);
+                const uint32_t r = static_cast<uint32_t>(n / kStages);
+                if (!ptx::mbar_wait(bar_full + 8 * s, r & 1, abort_flag, err, kErrWaitMmaFull)) break;
+                ptx::tc_fence_after();
+                for (int t = 0; t < nqt; ++t) {
+                    const uint32_t slot = it & 1, use = it >> 1;
+                    if (!ptx::mbar_wait(bar_tempty + 8 * slot, (use & 1) ^ 1, abort_flag, err, kErrWaitMmaTmem)) {
+                        ok = false;
+                        break;
+                    }
+                    ptx::tc_fence_after();
+                    const uint32_t d = tmem + slot * kBN;
+                    const uint32_t a0 = q_s + t * kQTileBytes;
+                    const uint32_t b0 = b_s + s * kBTileBytes;
+                    #pragma unroll
+                    for (int kk = 0; kk < kDim / 32; ++kk)
+                        ptx::mma_i8(d, ptx::sdesc_sw128(a0 + kk * 32), ptx::sdesc_sw128(b0 + kk * 32), idesc,
+                                    kk > 0 ? 1u : 0u);
+                    ptx::tc_commit(bar_tfull + 8 * slot);
+                    ++it;
+                }
+                if (!ok) break;
+                ptx::tc_commit(bar_empty + 8 * s);
+                const bool last_of_group = (w + 1 == w_end) || ((w + 1) / BT != g);
+                if (last_of_group) ptx::tc_commit(bar_qempty);
+            }
+            // Drain: all issued MMAs complete before TMEM is released.
+            ptx::tc_commit(bar_drain);
+            ptx::mbar_wait(bar_drain, 0, never, err, kErrWaitDrain);
+        }
+        __syncwarp();
+    } else {
+        // ------------------------------------------------------ epilogue
+        const int e = warp - 2;
+        const int quarter = warp & 3;
+        const int half = e >> 2;
+        const uint32_t lane_base = static_cast<uint32_t>(quarter * 32) << 16;
+        int k1[kQT], i1[kQT], k2[kQT], i2[kQT];
+        #pragma unroll
+        for (int t = 0; t < kQT; ++t) { k1[t] = INT_MAX; k2[t] = INT_MAX; i1[t] = -1; i2[t] = -1; }
+        int cur_g = -1, nqt = 0, split = 0;
+        uint32_t it = 0;
+        bool ok = true;
+
+        auto flush = [&]() {
+            #pragma unroll
+            for (int t = 0; t < kQT; ++t) {
+                if (t < nqt) {
+                    const int q = (cur_g * kQT + t) * kBM + quarter * 32 + lane;
+                    partial[(static_cast<size_t>(split) * 2 + half) * plan.q_pad + q] =
+                        make_int4(k1[t], i1[t], k2[t], i2[t]);
+                }
+                k1[t] = INT_MAX; k2[t] = INT_MAX; i1[t] = -1; i2[t] = -1;
+            }
+        };
+
+        for (long long w = w_begin; w < w_end && ok; ++w) {
+            const int g = static_cast<int>(w / BT);
+            const int j = static_cast<int>(w - static_cast<long long>(g) * BT);
+            if (g != cur_g) {
+                if (cur_g >= 0) flush();
+                cur_g = g;
+                nqt = min(kQT, plan.q_tiles - g * kQT);
+                split = static_cast<int>(blockIdx.x) - plan_cta_of(static_cast<long long>(g) * BT, W, G);
+            }
+            const int row0 = j * kBN + half * 128;
+            const int4 gm = __ldg(reinterpret_cast<const int4*>(bgmin + (row0 >> 5)));
+            #pragma unroll
+            for (int t = 0; t < kQT; ++t) {
+                if (t < nqt) {
+                    const uint32_t slot = it & 1, use = it >> 1;
+                    // Every lane observes the barrier; the outcome is made
+                    // warp-uniform before the .sync.aligned TMEM loads.
+                    const bool waited =
+                        ptx::mbar_wait(bar_tfull + 8 * slot, use & 1, abort_flag, err, kErrWaitEpilogue);
+                    if (!__all_sync(0xffffffffu, waited)) {
+                        ok = false;
+                        break;
+                    }
+                    ptx::tc_fence_after();
+                    const uint32_t taddr = tmem + lane_base + slot * kBN + half * 128;
+                    uint32_t v0[32], v1[32], v2[32], v3[32];
+                    ptx::tmem_ld32(taddr, v0);
+                    ptx::tmem_ld32(taddr + 32, v1);
+                    ptx::tmem_ld32(taddr + 64, v2);
+                    ptx::tmem_ld32(taddr + 96, v3);
+                    ptx::tmem_ld_wait(v0);
+                    ptx::tmem_ld_wait(v1);
+                    ptx::tmem_ld_wait(v2);
+                    ptx::tmem_ld_wait(v3);
+                    ptx::tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) ptx::mbar_arrive(bar_tempty + 8 * slot);
+                    scan_group(v0, row0, gm.x, bnorm, k1[t], i1[t], k2[t], i2[t]);
+                    scan_group(v1, row0 + 32, gm.y, bnorm, k1[t], i1[t], k2[t], i2[t]);
+                    scan_group(v2, row0 + 64, gm.z, bnorm, k1[t], i1[t], k2[t], i2[t]);
+                    scan_group(v3, row0 + 96, gm.w, bnorm, k1[t], i1[t], k2[t], i2[t]);
+                    ++it;
+                }
+            }
+        }
+        if (cur_g >= 0) flush();
+    }
+
+    ptx::tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        ptx::tc_fence_after();
+        ptx::tmem_dealloc(tmem, kTmemCols);
+    }
+}
+
+__device__ __forceinline__ bool lex_less(int ka, int ia, int kb, int ib) {
+    return ka < kb || (ka == kb && ia < ib);
+}
+
+__global__ void __launch_bounds__(256) merge2nn_kernel(const int4* __restrict__ partial, const ExactPlan plan,
+                                                       const int32_t* __restrict__ qnorm, int metric, float thr,
+                                                       uint32_t* __restrict__ matches, float4* __restrict__ sorted,
+                                                       int32_t* __restrict__ nn_idx, float* __restrict__ nn_dist) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= plan.q_n) return;
+    const long long W = plan.units, G = plan.grid;
+    const long long BT = plan.base_tiles;
+    const int g = q / (kQT * kBM);
+    // No base rows: no CTA ran and every neighbour is absent.
+    const int c0 = W > 0 ? plan_cta_of(g * BT, W, G) : 0;
+    const int c1 = W > 0 ? plan_cta_of((g + 1) * BT - 1, W, G) : -1;
+    int a1 = INT_MAX, j1 = -1, a2 = INT_MAX, j2 = -1;
+    auto push = [&](int k, int i) {
+        if (i < 0) return;
+        if (lex_less(k, i, a1, j1) || j1 < 0) {
+            a2 = a1; j2 = j1;
+            a1 = k; j1 = i;
+        } else if (lex_less(k, i, a2, j2) || j2 < 0) {
+            a2 = k; j2 = i;
+        }
+    };
+    for (int s = 0; s <= c1 - c0; ++s) {
+        #pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int4 p = partial[(static_cast<size_t>(s) * 2 + h) * plan.q_pad + q];
+            push(p.x, p.y);
+            push(p.z, p.w);
+        }
+    }
+    const bool v1 = j1 >= 0 && a1 < kKeyPad;
+    const bool v2 = j2 >= 0 && a2 < kKeyPad;
+    const int qn = metric == kMetricL2 ? qnorm[q] : 0;
+    const float d1 = v1 ? static_cast<float>(a1 + qn) : FLT_MAX;
+    const float d2 = v2 ? static_cast<float>(a2 + qn) : FLT_MAX;
+    if (matches) {
+        bool pass = false;
+        if (v1) {
+            float f1, f2;
+            if (metric == kMetricL2) {
+                f1 = sqrtf(d1);
+                f2 = v2 ? sqrtf(d2) : INFINITY;
+            } else {
+                f1 = sqrtf(d1 + 2.0f);
+                f2 = v2 ? sqrtf(d2 + 2.0f) : INFINITY;
+            }
+            pass = (f1 / f2) < thr;
+        }
+        matches[q] = pass ? static_cast<uint32_t>(j1) : UINT32_MAX;
+    }
+    if (sorted)
+        sorted[q] = make_float4(d1, d2, v1 ? static_cast<float>(j1) : FLT_MAX, v2 ? static_cast<float>(j2) : FLT_MAX);
+    if (nn_idx) {
+        nn_idx[2 * q] = v1 ? j1 : -1;
+        nn_idx[2 * q + 1] = v2 ? j2 : -1;
+    }
+    if (nn_dist) {
+        nn_dist[2 * q] = d1;
+        nn_dist[2 * q + 1] = d2;
+    }
+}
+
+}  // namespace
+
+ExactPlan make_exact_plan(int q_n, int r_n, int num_sms) {
+    ExactPlan p{};
+    p.q_n = q_n;
+    p.r_n = r_n;
+    p.q_tiles = (q_n + kBM - 1) / kBM;
+    p.q_groups = (p.q_tiles + kQT - 1) / kQT;
+    p.q_pad = p.q_tiles * kBM;
+    p.base_tiles = (r_n + kBN - 1) / kBN;
+    p.r_pad = p.base_tiles * kBN;
+    p.units = static_cast<long long>(p.q_groups) * p.base_tiles;
+    p.grid = static_cast<int>(std::min<long long>(num_sms, p.units));
+    int ms = 1;
+    if (p.grid > 0) {
+        for (int g = 0; g < p.q_groups; ++g) {
+            const long long BT = p.base_tiles;
+            const int c0 = plan_cta_of(g * BT, p.units, p.grid);
+            const int c1 = plan_cta_of((g + 1) * BT - 1, p.units, p.grid);
+            ms = std::max(ms, c1 - c0 + 1);
+        }
+    }
+    p.max_splits = ms;
+    return p;
+}
+
+size_t exact2nn_smem_bytes() { return kSmemBytes; }
+
+cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* norm, int32_t* group_min,
+                                cudaStream_t stream) {
+    if (n_pad <= 0) return cudaSuccess;
+    row_norms_u8_kernel<<<n_pad / 32, 256, 0, stream>>>(x, n, n_pad, metric, norm, group_min);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_exact2nn_u8(const CUtensorMap& qmap, const CUtensorMap& bmap, const int32_t* bnorm,
+                               const int32_t* bgmin, const ExactPlan& plan, int4* partial, int* err,
+                               cudaStream_t stream) {
+    // The shared-memory opt-in is per device; the host API serialises calls per device.
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+        e = cudaFuncSetAttribute(exact2nn_u8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kSmemBytes));
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) attr_set[dev] = true;
+    }
+    if (plan.grid <= 0) return cudaSuccess;
+    exact2nn_u8_kernel<<<plan.grid, kThreads, kSmemBytes, stream>>>(qmap, bmap, bnorm, bgmin, plan, partial, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_merge2nn(const int4* partial, const ExactPlan& plan, const int32_t* qnorm, int metric,
+                            float threshold, uint32_t* matches, float4* sorted, int32_t* nn_idx, float* nn_dist,
+                            cudaStream_t stream) {
+    if (plan.q_n <= 0) return cudaSuccess;
+    merge2nn_kernel<<<(plan.q_n + 255) / 256, 256, 0, stream>>>(partial, plan, qnorm, metric, threshold, matches,
+                                                               sorted, nn_idx, nn_dist);
+    return cudaGetLastError();
+}
+
+}  // namespace sift

@@ -1,0 +1,80 @@
+// Exact 2-NN over 128-d descriptors: shared declarations between the kernels
+// (exact2nn.cu) and the host entry points (api.cu).
+#pragma once
+#include <cstdint>
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+namespace sift {
+
+constexpr int kDim = 128;            // descriptor length (elements)
+constexpr int kBM = 128;             // queries per tile = TMEM lanes = MMA M
+constexpr int kQT = 2;               // query tiles held by one CTA at a time
+constexpr int kBN = 256;             // base rows per tile = MMA N
+constexpr int kStages = 4;           // base-tile ring depth (u8)
+constexpr int kEpiWarps = 8;         // epilogue warps (2 per TMEM lane quarter)
+constexpr int kThreads = 64 + 32 * kEpiWarps;
+constexpr int kTmemCols = 512;       // 2 accumulator slots of kBN columns
+constexpr int32_t kKeyPad = 1 << 30; // ranking key of padding rows (never a real key)
+
+// Distance definitions of the exact path.
+enum Metric : int {
+    kMetricL2 = 0,   // full squared Euclidean distance (host_brute / device_brute)
+    kMetricDot = 1,  // -2 q.r (the ranking of cublas_2nn_f / cublas_2nn_sift)
+};
+
+// Device error codes written by bounded waits (first one wins).
+enum DeviceError : int {
+    kErrNone = 0,
+    kErrWaitProducer = 1,
+    kErrWaitMmaFull = 2,
+    kErrWaitMmaTmem = 3,
+    kErrWaitEpilogue = 4,
+    kErrWaitQuery = 5,
+    kErrWaitDrain = 6,
+};
+
+// Work decomposition of one exact search. A "unit" is (query group g, base
+// tile j); units are numbered w = g * base_tiles + j and every CTA of the
+// persistent grid owns the contiguous range [w0(c), w0(c+1)), w0(c) =
+// floor(c * W / G). cta_of(w) = floor(((w + 1) * G - 1) / W) inverts that.
+struct ExactPlan {
+    int q_n, r_n;
+    int q_tiles, q_groups, q_pad;   // q_pad = q_tiles * kBM
+    int base_tiles, r_pad;          // r_pad = base_tiles * kBN
+    long long units;                // q_groups * base_tiles
+    int grid;                       // persistent CTAs
+    int max_splits;                 // max CTAs covering one query group
+};
+
+__host__ __device__ inline long long plan_w0(long long c, long long W, long long G) { return (c * W) / G; }
+__host__ __device__ inline int plan_cta_of(long long w, long long W, long long G) {
+    return static_cast<int>(((w + 1) * G - 1) / W);
+}
+
+ExactPlan make_exact_plan(int q_n, int r_n, int num_sms);
+
+// Per-row squared norms of u8 descriptors (or zeros for kMetricDot), padded
+// to n_pad rows with kKeyPad, plus the minimum over each group of 32 rows.
+cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* norm, int32_t* group_min,
+                                cudaStream_t stream);
+
+// The fused GEMM + top-2 kernel. partial: [max_splits][2][q_pad] int4
+// {key1, idx1, key2, idx2} with key = norm(b) - 2 q.b.
+cudaError_t launch_exact2nn_u8(const CUtensorMap& qmap, const CUtensorMap& bmap, const int32_t* bnorm,
+                               const int32_t* bgmin, const ExactPlan& plan, int4* partial, int* err,
+                               cudaStream_t stream);
+
+// Merge of the per-CTA partial top-2 lists, distances, ratio test and output.
+// Any output pointer may be null.
+//   matches[q]   idx1 if the ratio test passes else UINT32_MAX
+//   sorted[q]    {d1, d2, i1, i2} as floats (FLT_MAX where absent)
+//   nn_idx[2q..] int32 indices (-1 where absent)
+//   nn_dist[2q..] float distances (FLT_MAX where absent)
+cudaError_t launch_merge2nn(const int4* partial, const ExactPlan& plan, const int32_t* qnorm, int metric,
+                            float threshold, uint32_t* matches, float4* sorted, int32_t* nn_idx, float* nn_dist,
+                            cudaStream_t stream);
+
+size_t exact2nn_smem_bytes();
+
+}  // namespace sift
