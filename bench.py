@@ -167,6 +167,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true", help="time only the device-resident path")
+    ap.add_argument("--queries", type=int, default=Q_N, help="queries per GPU (profiling of smaller cases)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -189,20 +191,21 @@ def main():
 
     from matching_sift_b200 import datagen
 
+    q_n = args.queries
     base = datagen.make_base(R_N, seed=0)
-    queries = datagen.make_queries(Q_N, base, seed=rank)
+    queries = datagen.make_queries(q_n, base, seed=rank)
     lib = ms.lib()
 
     qd = torch.from_numpy(queries).to(dev)
     rd = torch.from_numpy(base).to(dev)
-    matches = torch.empty(Q_N, dtype=torch.int32, device=dev)
-    nn_idx = torch.empty((Q_N, 2), dtype=torch.int32, device=dev)
-    nn_dist = torch.empty((Q_N, 2), dtype=torch.float32, device=dev)
+    matches = torch.empty(q_n, dtype=torch.int32, device=dev)
+    nn_idx = torch.empty((q_n, 2), dtype=torch.int32, device=dev)
+    nn_dist = torch.empty((q_n, 2), dtype=torch.float32, device=dev)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream(dev)
 
     def step():
-        rc = lib.sift2nn_match(qd.data_ptr(), rd.data_ptr(), ms.U8_DEVICE, Q_N, R_N, ms.METRIC_L2, THRESHOLD,
+        rc = lib.sift2nn_match(qd.data_ptr(), rd.data_ptr(), ms.U8_DEVICE, q_n, R_N, ms.METRIC_L2, THRESHOLD,
                                matches.data_ptr(), None, nn_idx.data_ptr(), nn_dist.data_ptr(), stream.cuda_stream)
         if rc != 0:
             raise ms.SiftError(rc, "sift2nn_match")
@@ -237,29 +240,31 @@ def main():
     kernel_ms = kt.value / max(kn.value, 1)
 
     # ---- end to end through the C ABI with host buffers
-    qh = torch.from_numpy(queries).pin_memory()
-    rh = torch.from_numpy(base).pin_memory()
-    mh = torch.empty(Q_N, dtype=torch.int32).pin_memory()
+    e2e_ms = float("nan")
+    if not args.skip_e2e:
+        qh = torch.from_numpy(queries).pin_memory()
+        rh = torch.from_numpy(base).pin_memory()
+        mh = torch.empty(q_n, dtype=torch.int32).pin_memory()
 
-    def e2e_step():
-        rc = lib.cublas_2nn_sift(qh.data_ptr(), rh.data_ptr(), ms.U8_HOST, Q_N, R_N, mh.data_ptr(), THRESHOLD,
-                                 None, 1, 0, 17)
-        if rc != 0:
-            raise ms.SiftError(rc, "cublas_2nn_sift")
+        def e2e_step():
+            rc = lib.cublas_2nn_sift(qh.data_ptr(), rh.data_ptr(), ms.U8_HOST, q_n, R_N, mh.data_ptr(), THRESHOLD,
+                                     None, 1, 0, 17)
+            if rc != 0:
+                raise ms.SiftError(rc, "cublas_2nn_sift")
 
-    for _ in range(args.warmup):
-        e2e_step()
-    e2e_ms = 0.0
-    legacy = torch.cuda.default_stream(dev)
-    for k in range(args.steps):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        a.record(legacy)
-        e2e_step()
-        b.record(legacy)
-        b.synchronize()
-        e2e_ms += a.elapsed_time(b)
-    np.testing.assert_array_equal(mh.numpy(), matches.cpu().numpy())
+        for _ in range(args.warmup):
+            e2e_step()
+        e2e_ms = 0.0
+        legacy = torch.cuda.default_stream(dev)
+        for k in range(args.steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record(legacy)
+            e2e_step()
+            b.record(legacy)
+            b.synchronize()
+            e2e_ms += a.elapsed_time(b)
+        np.testing.assert_array_equal(mh.numpy(), matches.cpu().numpy())
 
     # ---- max over ranks
     t = torch.tensor([step_ms, e2e_ms, kernel_ms], dtype=torch.float64, device=dev)
@@ -269,11 +274,11 @@ def main():
 
     if rank == 0:
         peaks, peak_src = _peaks()
-        ops = 2.0 * Q_N * R_N * DIM
+        ops = 2.0 * q_n * R_N * DIM
         achieved = ops / (kernel_ms * 1e-3) / 1e12
         peak_int8 = 2.0 * peaks["bf16_tflops"]
-        qps = world * Q_N * args.steps / (step_ms * 1e-3)
-        e2e_qps = world * Q_N * args.steps / (e2e_ms * 1e-3)
+        qps = world * q_n * args.steps / (step_ms * 1e-3)
+        e2e_qps = world * q_n * args.steps / (e2e_ms * 1e-3) if e2e_ms == e2e_ms else None
         line = {
             "metric": METRIC,
             "value": round(qps, 1),
@@ -287,11 +292,12 @@ def main():
             "vs_baseline": None,
             "dtype": "u8",
             "data": "synthetic (seeded generator standing in for ANN_SIFT1M; base seed 0, queries seed = rank)",
-            "config": {"workload": WORKLOAD, "queries_per_gpu": Q_N, "base_rows": R_N, "dim": DIM,
+            "config": {"workload": WORKLOAD if q_n == Q_N else WORKLOAD.replace("10,000", f"{q_n:,}"),
+                       "queries_per_gpu": q_n, "base_rows": R_N, "dim": DIM,
                        "ratio": THRESHOLD, "l2_between_steps": "flushed (256 MiB write outside the timed events)",
                        "parallelism": f"query-sharded x{world}, base replicated"},
-            "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s",
-                    "h2d_bytes_per_step": (Q_N + R_N) * DIM, "d2h_bytes_per_step": Q_N * 4,
+            "e2e": {"value": round(e2e_qps, 1) if e2e_qps else None, "unit": "queries/s",
+                    "h2d_bytes_per_step": (q_n + R_N) * DIM, "d2h_bytes_per_step": q_n * 4,
                     "call": "cublas_2nn_sift(type=SIFT_U8_HOST) with pinned host buffers"},
             "gpu_launches": int(launches),
             "roofline": {"bound": "tensor", "kernel": "exact2nn_u8_kernel", "achieved": round(achieved, 1),

@@ -16,19 +16,27 @@
 // Ties are broken by the lower base index (lexicographic (key, index) order),
 // which is the order of the reference's host_brute (src/knn_brute.cu:816-831).
 //
-// Warp roles (kThreads = 320):
-//   warp 0      TMA producer: query tiles (resident per query group) and a
-//               kStages ring of base tiles
-//   warp 1      TMEM allocator + single-thread MMA issuer
-//   warps 2..9  epilogue: warp w reads TMEM lane quarter (w % 4), half
-//               (w - 2) / 4 of the 256 columns of every accumulator slot
+// Work decomposition. A CTA holds kQT = 4 query tiles (512 queries) in shared
+// memory and streams base tiles of kBN = 128 rows; a unit = (query group,
+// base tile). Units are split evenly over a persistent grid of one CTA per SM.
 //
-// Epilogue filter. Per group of 32 base rows the epilogue takes the largest
-// dot product m of its query row and the smallest norm n_min of the group
-// (precomputed): if n_min - 2 m >= key2 (the query's current second-best key)
-// no row of the group can enter the top-2 and the group costs ~1 instruction
-// per element. Otherwise (rare once the top-2 has settled) the exact keys of
-// the 32 rows are formed and merged in index order.
+// Warp roles (kThreads = 576):
+//   warp 0       TMA producer: the query tiles of the current group and a
+//                kStages ring of base tiles
+//   warp 1       TMEM allocator + single-thread MMA issuer: per base tile one
+//                128 x 128 x 128 product per query tile into that tile's
+//                TMEM slot (4 slots x 128 columns)
+//   warps 2..17  epilogue: warp w owns query tile (w - 2) / 4 and TMEM lane
+//                quarter w % 4, i.e. 32 query rows, one thread per row
+//
+// Epilogue pruning. Per group of 32 base rows a thread takes the largest dot
+// product m of its query row; with n_min the smallest norm of the group
+// (precomputed), n_min - 2 m is a lower bound of every key in the group. If it
+// exceeds the thread's threshold the group is skipped (~0.7 instruction per
+// element); otherwise the same test runs per 8-row subgroup and only passing
+// subgroups form exact keys. The threshold is the thread's own second-best key
+// and an upper bound of the final second-best key that the CTAs splitting the
+// same query group share through global memory (atomicMin).
 #include <cfloat>
 #include <climits>
 #include <algorithm>
@@ -40,60 +48,80 @@ namespace sift {
 namespace {
 
 constexpr int kQTileBytes = kBM * kDim;  // 16 KB: one query tile (u8)
-constexpr int kBTileBytes = kBN * kDim;  // 32 KB: one base tile (u8)
+constexpr int kBTileBytes = kBN * kDim;  // 16 KB: one base tile (u8)
 
 struct __align__(8) SmemCtl {
     uint64_t full[kStages];
     uint64_t empty[kStages];
     uint64_t qfull, qempty;
-    uint64_t tfull[2], tempty[2];
+    uint64_t tfull[kQT], tempty[kQT];
     uint64_t drain;
     uint32_t tmem_base;
     int abort_flag;
+    int no_abort;
 };
 
 constexpr size_t kSmemBytes = 1024 + kQT * kQTileBytes + kStages * kBTileBytes + sizeof(SmemCtl);
 
-__device__ __forceinline__ int max32(const uint32_t (&v)[32]) {
-    int m[11];
-    #pragma unroll
-    for (int i = 0; i < 10; ++i)
-        m[i] = __vimax3_s32(static_cast<int>(v[3 * i]), static_cast<int>(v[3 * i + 1]), static_cast<int>(v[3 * i + 2]));
-    m[10] = max(static_cast<int>(v[30]), static_cast<int>(v[31]));
-    int a = __vimax3_s32(m[0], m[1], m[2]);
-    int b = __vimax3_s32(m[3], m[4], m[5]);
-    int c = __vimax3_s32(m[6], m[7], m[8]);
-    int d = max(m[9], m[10]);
-    return max(__vimax3_s32(a, b, c), d);
+__device__ __forceinline__ int max8(const uint32_t* v) {
+    int m = __vimax3_s32(static_cast<int>(v[0]), static_cast<int>(v[1]), static_cast<int>(v[2]));
+    m = __vimax3_s32(m, static_cast<int>(v[3]), static_cast<int>(v[4]));
+    m = __vimax3_s32(m, static_cast<int>(v[5]), static_cast<int>(v[6]));
+    return max(m, static_cast<int>(v[7]));
 }
 
-__device__ __forceinline__ void top2_update(int key, int idx, int& k1, int& i1, int& k2, int& i2) {
-    if (key < k2) {
-        if (key < k1) {
-            k2 = k1; i2 = i1;
-            k1 = key; i1 = idx;
+// Per-thread running top-2 of one query row over base rows visited in
+// increasing index order (strict '<' keeps the lower index on ties).
+struct Top2 {
+    int k1, i1, k2, i2;
+    int thr;  // prune bound: rows with key > thr cannot enter the final top-2
+};
+
+__device__ __forceinline__ void top2_update(Top2& s, int key, int idx) {
+    if (key < s.k2) {
+        if (key < s.k1) {
+            s.k2 = s.k1; s.i2 = s.i1;
+            s.k1 = key; s.i1 = idx;
         } else {
-            k2 = key; i2 = idx;
+            s.k2 = key; s.i2 = idx;
         }
+        s.thr = min(s.thr, s.k2 - 1);
     }
 }
 
 // One group of 32 consecutive base rows [row0, row0 + 32) for this thread's
-// query row; v[c] = q.b(row0 + c).
-__device__ __forceinline__ void scan_group(const uint32_t (&v)[32], int row0, int gmin,
-                                           const int32_t* __restrict__ bnorm, int& k1, int& i1, int& k2, int& i2) {
-    const int mx = max32(v);
-    const bool pass = (gmin - 2 * mx) < k2;
+// query row; v[c] = q.b(row0 + c). Two-level pruning: the group bound
+// gmin32 - 2 max(v) first, then per 8-row subgroup gmin8 - 2 max(v[8s..8s+8)).
+// Both are lower bounds of every key in their rows, so a (sub)group whose
+// bound exceeds the thread's threshold holds no candidate.
+__device__ __forceinline__ void scan_group(const uint32_t (&v)[32], int row0, int gmin32,
+                                           const int32_t* __restrict__ gmin8, const int32_t* __restrict__ bnorm,
+                                           Top2& s) {
+    int mx[4];
+    #pragma unroll
+    for (int k = 0; k < 4; ++k) mx[k] = max8(v + 8 * k);
+    const int m = max(__vimax3_s32(mx[0], mx[1], mx[2]), mx[3]);
+    const bool pass = (gmin32 - 2 * m) <= s.thr;
     if (__any_sync(0xffffffffu, pass)) {
-        if (pass) {
-            const int4* nb4 = reinterpret_cast<const int4*>(bnorm + row0);
-            #pragma unroll
-            for (int c4 = 0; c4 < 8; ++c4) {
-                const int4 nb = __ldg(nb4 + c4);
-                top2_update(nb.x - 2 * static_cast<int>(v[4 * c4 + 0]), row0 + 4 * c4 + 0, k1, i1, k2, i2);
-                top2_update(nb.y - 2 * static_cast<int>(v[4 * c4 + 1]), row0 + 4 * c4 + 1, k1, i1, k2, i2);
-                top2_update(nb.z - 2 * static_cast<int>(v[4 * c4 + 2]), row0 + 4 * c4 + 2, k1, i1, k2, i2);
-                top2_update(nb.w - 2 * static_cast<int>(v[4 * c4 + 3]), row0 + 4 * c4 + 3, k1, i1, k2, i2);
+        const int4 g8 = __ldg(reinterpret_cast<const int4*>(gmin8 + (row0 >> 3)));
+        const int gs[4] = {g8.x, g8.y, g8.z, g8.w};
+        #pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const bool ps = pass && (gs[k] - 2 * mx[k]) <= s.thr;
+            if (__any_sync(0xffffffffu, ps)) {
+                if (ps) {
+                    const int4* nb4 = reinterpret_cast<const int4*>(bnorm + row0 + 8 * k);
+                    const int4 na = __ldg(nb4), nb = __ldg(nb4 + 1);
+                    const int base = row0 + 8 * k;
+                    top2_update(s, na.x - 2 * static_cast<int>(v[8 * k + 0]), base + 0);
+                    top2_update(s, na.y - 2 * static_cast<int>(v[8 * k + 1]), base + 1);
+                    top2_update(s, na.z - 2 * static_cast<int>(v[8 * k + 2]), base + 2);
+                    top2_update(s, na.w - 2 * static_cast<int>(v[8 * k + 3]), base + 3);
+                    top2_update(s, nb.x - 2 * static_cast<int>(v[8 * k + 4]), base + 4);
+                    top2_update(s, nb.y - 2 * static_cast<int>(v[8 * k + 5]), base + 5);
+                    top2_update(s, nb.z - 2 * static_cast<int>(v[8 * k + 6]), base + 6);
+                    top2_update(s, nb.w - 2 * static_cast<int>(v[8 * k + 7]), base + 7);
+                }
             }
         }
     }
@@ -101,7 +129,8 @@ __device__ __forceinline__ void scan_group(const uint32_t (&v)[32], int row0, in
 
 __global__ void __launch_bounds__(256) row_norms_u8_kernel(const uint8_t* __restrict__ x, int n, int n_pad,
                                                            int metric, int32_t* __restrict__ norm,
-                                                           int32_t* __restrict__ gmin) {
+                                                           int32_t* __restrict__ gmin8, int32_t* __restrict__ gmin32,
+                                                           int32_t* __restrict__ thresh) {
     // 32 rows per block, 8 threads per row, 16 bytes per thread.
     const int row = blockIdx.x * 32 + (threadIdx.x >> 3);
     const int sub = threadIdx.x & 7;
@@ -117,25 +146,31 @@ __global__ void __launch_bounds__(256) row_norms_u8_kernel(const uint8_t* __rest
     s += __shfl_xor_sync(0xffffffffu, s, 2);
     s += __shfl_xor_sync(0xffffffffu, s, 4);
     const int32_t v = row < n ? (metric == kMetricL2 ? static_cast<int32_t>(s) : 0) : kKeyPad;
-    if (sub == 0 && row < n_pad && norm) norm[row] = v;
-    int m = v;
-    m = min(m, __shfl_xor_sync(0xffffffffu, m, 8));
-    m = min(m, __shfl_xor_sync(0xffffffffu, m, 16));
-    __shared__ int wmin[8];
-    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = m;
+    __shared__ int32_t nrm[32];
+    if (sub == 0) {
+        nrm[threadIdx.x >> 3] = v;
+        if (norm) norm[row] = v;
+        if (thresh) thresh[row] = INT_MAX;
+    }
     __syncthreads();
-    if (threadIdx.x == 0 && gmin) {
-        int mm = wmin[0];
+    if (threadIdx.x < 4 && gmin8) {
+        int m = nrm[8 * threadIdx.x];
         #pragma unroll
-        for (int i = 1; i < 8; ++i) mm = min(mm, wmin[i]);
-        gmin[blockIdx.x] = mm;
+        for (int i = 1; i < 8; ++i) m = min(m, nrm[8 * threadIdx.x + i]);
+        gmin8[blockIdx.x * 4 + threadIdx.x] = m;
+    }
+    if (threadIdx.x == 32 && gmin32) {
+        int m = nrm[0];
+        #pragma unroll
+        for (int i = 1; i < 32; ++i) m = min(m, nrm[i]);
+        gmin32[blockIdx.x] = m;
     }
 }
 
 __global__ void __launch_bounds__(kThreads, 1)
     exact2nn_u8_kernel(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap bmap,
-                       const int32_t* __restrict__ bnorm, const int32_t* __restrict__ bgmin, const ExactPlan plan,
-                       int4* __restrict__ partial, int* __restrict__ err) {
+                       const BaseNorms bn, const ExactPlan plan, int4* __restrict__ partial,
+                       int32_t* __restrict__ thresh, int* __restrict__ err) {
     extern __shared__ uint8_t smem_raw[];
     // 1024-byte alignment for the 128-byte swizzle atoms.
     const uint32_t raw_u32 = ptx::smem_u32(smem_raw);
@@ -153,6 +188,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     const long long w_begin = plan_w0(blockIdx.x, W, G);
     const long long w_end = plan_w0(blockIdx.x + 1, W, G);
     const int BT = plan.base_tiles;
+    const int g_begin = static_cast<int>(w_begin / BT);
+    const int j_begin = static_cast<int>(w_begin - static_cast<long long>(g_begin) * BT);
 
     const uint32_t bar_full = ptx::smem_u32(&ctl->full[0]);
     const uint32_t bar_empty = ptx::smem_u32(&ctl->empty[0]);
@@ -169,12 +206,13 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         ptx::mbar_init(bar_qfull, 1);
         ptx::mbar_init(bar_qempty, 1);
-        for (int i = 0; i < 2; ++i) {
+        for (int i = 0; i < kQT; ++i) {
             ptx::mbar_init(bar_tfull + 8 * i, 1);
-            ptx::mbar_init(bar_tempty + 8 * i, kEpiWarps);
+            ptx::mbar_init(bar_tempty + 8 * i, 4);  // the four lane-quarter warps of tile i
         }
         ptx::mbar_init(bar_drain, 1);
         ctl->abort_flag = 0;
+        ctl->no_abort = 0;
         ptx::fence_mbar_init();
     }
     if (warp == 1) {
@@ -186,11 +224,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     ptx::tc_fence_after();
     const uint32_t tmem = ctl->tmem_base;
     volatile int* abort_flag = &ctl->abort_flag;
-    // A second flag that never aborts drain waits (they stay time-bounded).
-    __shared__ int no_abort;
-    if (threadIdx.x == 0) no_abort = 0;
-    __syncthreads();
-    volatile int* never = &no_abort;
+    volatile int* never = &ctl->no_abort;  // drain waits: time-bounded, never aborted early
 
     if (warp == 0) {
         if (lane == 0) {
@@ -198,10 +232,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             ptx::tma_prefetch_desc(&qmap);
             ptx::tma_prefetch_desc(&bmap);
             int cur_g = -1, ngroups = 0;
+            int g = g_begin, j = j_begin;
             long long n = 0;
             for (long long w = w_begin; w < w_end; ++w) {
-                const int g = static_cast<int>(w / BT);
-                const int j = static_cast<int>(w - static_cast<long long>(g) * BT);
                 if (g != cur_g) {
                     if (ngroups > 0 &&
                         !ptx::mbar_wait(bar_qempty, (ngroups - 1) & 1, abort_flag, err, kErrWaitQuery))
@@ -220,6 +253,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 ptx::mbar_arrive_expect_tx(bar_full + 8 * s, kBTileBytes);
                 ptx::tma_load_2d(b_s + s * kBTileBytes, &bmap, 0, j * kBN, bar_full + 8 * s);
                 ++n;
+                if (++j == BT) { j = 0; ++g; }
             }
             // Drain: every issued copy lands before the CTA may exit.
             for (long long k = (n > kStages ? n - kStages : 0); k < n; ++k)
@@ -233,11 +267,11 @@ __global__ void __launch_bounds__(kThreads, 1)
             // -------------------------------------------------- MMA issuer
             constexpr uint32_t idesc = ptx::idesc_make(2 /*S32*/, 0 /*u8*/, 0 /*u8*/, kBM, kBN);
             int cur_g = -1, ngroups = 0, nqt = 0;
+            int g = g_begin, j = j_begin;
+            uint32_t use_parity = 0;  // bit t: parity of the accumulator uses of tile t so far
             long long n = 0;
-            uint32_t it = 0;
             bool ok = true;
             for (long long w = w_begin; w < w_end && ok; ++w, ++n) {
-                const int g = static_cast<int>(w / BT);
                 if (g != cur_g) {
                     if (!ptx::mbar_wait(bar_qfull, ngroups & 1, abort_flag, err, kErrWaitQuery)) break;
                     cur_g = g;
@@ -248,27 +282,31 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const uint32_t r = static_cast<uint32_t>(n / kStages);
                 if (!ptx::mbar_wait(bar_full + 8 * s, r & 1, abort_flag, err, kErrWaitMmaFull)) break;
                 ptx::tc_fence_after();
-                for (int t = 0; t < nqt; ++t) {
-                    const uint32_t slot = it & 1, use = it >> 1;
-                    if (!ptx::mbar_wait(bar_tempty + 8 * slot, (use & 1) ^ 1, abort_flag, err, kErrWaitMmaTmem)) {
-                        ok = false;
-                        break;
+                const uint32_t b0 = b_s + s * kBTileBytes;
+                #pragma unroll
+                for (int t = 0; t < kQT; ++t) {
+                    if (t < nqt && ok) {
+                        if (!ptx::mbar_wait(bar_tempty + 8 * t, ((use_parity >> t) & 1) ^ 1, abort_flag, err,
+                                            kErrWaitMmaTmem)) {
+                            ok = false;
+                        } else {
+                            ptx::tc_fence_after();
+                            const uint32_t d = tmem + t * kBN;
+                            const uint32_t a0 = q_s + t * kQTileBytes;
+                            #pragma unroll
+                            for (int kk = 0; kk < kDim / 32; ++kk)
+                                ptx::mma_i8(d, ptx::sdesc_sw128(a0 + kk * 32), ptx::sdesc_sw128(b0 + kk * 32), idesc,
+                                            kk > 0 ? 1u : 0u);
+                            ptx::tc_commit(bar_tfull + 8 * t);
+                            use_parity ^= 1u << t;
+                        }
                     }
-                    ptx::tc_fence_after();
-                    const uint32_t d = tmem + slot * kBN;
-                    const uint32_t a0 = q_s + t * kQTileBytes;
-                    const uint32_t b0 = b_s + s * kBTileBytes;
-                    #pragma unroll
-                    for (int kk = 0; kk < kDim / 32; ++kk)
-                        ptx::mma_i8(d, ptx::sdesc_sw128(a0 + kk * 32), ptx::sdesc_sw128(b0 + kk * 32), idesc,
-                                    kk > 0 ? 1u : 0u);
-                    ptx::tc_commit(bar_tfull + 8 * slot);
-                    ++it;
                 }
                 if (!ok) break;
                 ptx::tc_commit(bar_empty + 8 * s);
-                const bool last_of_group = (w + 1 == w_end) || ((w + 1) / BT != g);
+                const bool last_of_group = (w + 1 == w_end) || (j + 1 == BT);
                 if (last_of_group) ptx::tc_commit(bar_qempty);
+                if (++j == BT) { j = 0; ++g; }
             }
             // Drain: all issued MMAs complete before TMEM is released.
             ptx::tc_commit(bar_drain);
@@ -278,74 +316,64 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else {
         // ------------------------------------------------------ epilogue
         const int e = warp - 2;
-        const int quarter = warp & 3;
-        const int half = e >> 2;
-        const uint32_t lane_base = static_cast<uint32_t>(quarter * 32) << 16;
-        int k1[kQT], i1[kQT], k2[kQT], i2[kQT];
-        #pragma unroll
-        for (int t = 0; t < kQT; ++t) { k1[t] = INT_MAX; k2[t] = INT_MAX; i1[t] = -1; i2[t] = -1; }
-        int cur_g = -1, nqt = 0, split = 0;
-        uint32_t it = 0;
+        const int t = e >> 2;          // query tile of this warp
+        const int quarter = warp & 3;  // TMEM lane quarter this warp may access
+        const uint32_t taddr0 = tmem + (static_cast<uint32_t>(quarter * 32) << 16) + t * kBN;
+        Top2 st{INT_MAX, -1, INT_MAX, -1, INT_MAX};
+        int published = INT_MAX;
+        int cur_g = -1, nqt = 0, split = 0, q = 0;
+        int g = g_begin, j = j_begin;
+        uint32_t use = 0;
         bool ok = true;
 
-        auto flush = [&]() {
-            #pragma unroll
-            for (int t = 0; t < kQT; ++t) {
-                if (t < nqt) {
-                    const int q = (cur_g * kQT + t) * kBM + quarter * 32 + lane;
-                    partial[(static_cast<size_t>(split) * 2 + half) * plan.q_pad + q] =
-                        make_int4(k1[t], i1[t], k2[t], i2[t]);
-                }
-                k1[t] = INT_MAX; k2[t] = INT_MAX; i1[t] = -1; i2[t] = -1;
-            }
-        };
-
         for (long long w = w_begin; w < w_end && ok; ++w) {
-            const int g = static_cast<int>(w / BT);
-            const int j = static_cast<int>(w - static_cast<long long>(g) * BT);
             if (g != cur_g) {
-                if (cur_g >= 0) flush();
+                if (cur_g >= 0 && t < nqt)
+                    partial[static_cast<size_t>(split) * plan.q_pad + q] = make_int4(st.k1, st.i1, st.k2, st.i2);
+                st = Top2{INT_MAX, -1, INT_MAX, -1, INT_MAX};
+                published = INT_MAX;
                 cur_g = g;
                 nqt = min(kQT, plan.q_tiles - g * kQT);
                 split = static_cast<int>(blockIdx.x) - plan_cta_of(static_cast<long long>(g) * BT, W, G);
+                q = (g * kQT + t) * kBM + quarter * 32 + lane;
             }
-            const int row0 = j * kBN + half * 128;
-            const int4 gm = __ldg(reinterpret_cast<const int4*>(bgmin + (row0 >> 5)));
-            #pragma unroll
-            for (int t = 0; t < kQT; ++t) {
-                if (t < nqt) {
-                    const uint32_t slot = it & 1, use = it >> 1;
-                    // Every lane observes the barrier; the outcome is made
-                    // warp-uniform before the .sync.aligned TMEM loads.
-                    const bool waited =
-                        ptx::mbar_wait(bar_tfull + 8 * slot, use & 1, abort_flag, err, kErrWaitEpilogue);
-                    if (!__all_sync(0xffffffffu, waited)) {
-                        ok = false;
-                        break;
-                    }
-                    ptx::tc_fence_after();
-                    const uint32_t taddr = tmem + lane_base + slot * kBN + half * 128;
-                    uint32_t v0[32], v1[32], v2[32], v3[32];
-                    ptx::tmem_ld32(taddr, v0);
-                    ptx::tmem_ld32(taddr + 32, v1);
-                    ptx::tmem_ld32(taddr + 64, v2);
-                    ptx::tmem_ld32(taddr + 96, v3);
-                    ptx::tmem_ld_wait(v0);
-                    ptx::tmem_ld_wait(v1);
-                    ptx::tmem_ld_wait(v2);
-                    ptx::tmem_ld_wait(v3);
-                    ptx::tc_fence_before();
-                    __syncwarp();
-                    if (lane == 0) ptx::mbar_arrive(bar_tempty + 8 * slot);
-                    scan_group(v0, row0, gm.x, bnorm, k1[t], i1[t], k2[t], i2[t]);
-                    scan_group(v1, row0 + 32, gm.y, bnorm, k1[t], i1[t], k2[t], i2[t]);
-                    scan_group(v2, row0 + 64, gm.z, bnorm, k1[t], i1[t], k2[t], i2[t]);
-                    scan_group(v3, row0 + 96, gm.w, bnorm, k1[t], i1[t], k2[t], i2[t]);
-                    ++it;
+            if (t < nqt) {
+                // Bound shared with the other CTAs that scan this query's group.
+                st.thr = min(st.thr, __ldcg(thresh + q));
+                const int row0 = j * kBN;
+                const int4 gm = __ldg(reinterpret_cast<const int4*>(bn.gmin32 + (row0 >> 5)));
+                const bool waited = ptx::mbar_wait(bar_tfull + 8 * t, use & 1, abort_flag, err, kErrWaitEpilogue);
+                if (!__all_sync(0xffffffffu, waited)) {
+                    ok = false;
+                    break;
+                }
+                ++use;
+                ptx::tc_fence_after();
+                uint32_t va[32];
+                ptx::tmem_ld32(taddr0, va);
+                ptx::tmem_ld_wait(va);
+                scan_group(va, row0, gm.x, bn.gmin8, bn.norm, st);
+                ptx::tmem_ld32(taddr0 + 32, va);
+                ptx::tmem_ld_wait(va);
+                scan_group(va, row0 + 32, gm.y, bn.gmin8, bn.norm, st);
+                ptx::tmem_ld32(taddr0 + 64, va);
+                ptx::tmem_ld_wait(va);
+                scan_group(va, row0 + 64, gm.z, bn.gmin8, bn.norm, st);
+                ptx::tmem_ld32(taddr0 + 96, va);
+                ptx::tmem_ld_wait(va);
+                ptx::tc_fence_before();
+                __syncwarp();
+                if (lane == 0) ptx::mbar_arrive(bar_tempty + 8 * t);
+                scan_group(va, row0 + 96, gm.w, bn.gmin8, bn.norm, st);
+                if (st.k2 < published) {
+                    atomicMin(thresh + q, st.k2);
+                    published = st.k2;
                 }
             }
+            if (++j == BT) { j = 0; ++g; }
         }
-        if (cur_g >= 0) flush();
+        if (cur_g >= 0 && t < nqt)
+            partial[static_cast<size_t>(split) * plan.q_pad + q] = make_int4(st.k1, st.i1, st.k2, st.i2);
     }
 
     ptx::tc_fence_before();
@@ -383,12 +411,9 @@ __global__ void __launch_bounds__(256) merge2nn_kernel(const int4* __restrict__ 
         }
     };
     for (int s = 0; s <= c1 - c0; ++s) {
-        #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int4 p = partial[(static_cast<size_t>(s) * 2 + h) * plan.q_pad + q];
-            push(p.x, p.y);
-            push(p.z, p.w);
-        }
+        const int4 p = partial[static_cast<size_t>(s) * plan.q_pad + q];
+        push(p.x, p.y);
+        push(p.z, p.w);
     }
     const bool v1 = j1 >= 0 && a1 < kKeyPad;
     const bool v2 = j2 >= 0 && a2 < kKeyPad;
@@ -450,16 +475,15 @@ ExactPlan make_exact_plan(int q_n, int r_n, int num_sms) {
 
 size_t exact2nn_smem_bytes() { return kSmemBytes; }
 
-cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* norm, int32_t* group_min,
-                                cudaStream_t stream) {
+cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* norm, int32_t* gmin8,
+                                int32_t* gmin32, int32_t* thresh, cudaStream_t stream) {
     if (n_pad <= 0) return cudaSuccess;
-    row_norms_u8_kernel<<<n_pad / 32, 256, 0, stream>>>(x, n, n_pad, metric, norm, group_min);
+    row_norms_u8_kernel<<<n_pad / 32, 256, 0, stream>>>(x, n, n_pad, metric, norm, gmin8, gmin32, thresh);
     return cudaGetLastError();
 }
 
-cudaError_t launch_exact2nn_u8(const CUtensorMap& qmap, const CUtensorMap& bmap, const int32_t* bnorm,
-                               const int32_t* bgmin, const ExactPlan& plan, int4* partial, int* err,
-                               cudaStream_t stream) {
+cudaError_t launch_exact2nn_u8(const CUtensorMap& qmap, const CUtensorMap& bmap, const BaseNorms& bn,
+                               const ExactPlan& plan, int4* partial, int32_t* thresh, int* err, cudaStream_t stream) {
     // The shared-memory opt-in is per device; the host API serialises calls per device.
     static bool attr_set[64] = {};
     int dev = 0;
@@ -472,7 +496,7 @@ cudaError_t launch_exact2nn_u8(const CUtensorMap& qmap, const CUtensorMap& bmap,
         if (dev >= 0 && dev < 64) attr_set[dev] = true;
     }
     if (plan.grid <= 0) return cudaSuccess;
-    exact2nn_u8_kernel<<<plan.grid, kThreads, kSmemBytes, stream>>>(qmap, bmap, bnorm, bgmin, plan, partial, err);
+    exact2nn_u8_kernel<<<plan.grid, kThreads, kSmemBytes, stream>>>(qmap, bmap, bn, plan, partial, thresh, err);
     return cudaGetLastError();
 }
 

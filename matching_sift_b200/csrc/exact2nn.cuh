@@ -9,12 +9,12 @@ namespace sift {
 
 constexpr int kDim = 128;            // descriptor length (elements)
 constexpr int kBM = 128;             // queries per tile = TMEM lanes = MMA M
-constexpr int kQT = 2;               // query tiles held by one CTA at a time
-constexpr int kBN = 256;             // base rows per tile = MMA N
-constexpr int kStages = 4;           // base-tile ring depth (u8)
-constexpr int kEpiWarps = 8;         // epilogue warps (2 per TMEM lane quarter)
+constexpr int kQT = 4;               // query tiles held by one CTA at a time
+constexpr int kBN = 128;             // base rows per unit = MMA N
+constexpr int kStages = 8;           // base-tile ring depth
+constexpr int kEpiWarps = 4 * kQT;   // one epilogue warp per (query tile, TMEM lane quarter)
 constexpr int kThreads = 64 + 32 * kEpiWarps;
-constexpr int kTmemCols = 512;       // 2 accumulator slots of kBN columns
+constexpr int kTmemCols = kQT * kBN; // one accumulator slot of kBN columns per query tile
 constexpr int32_t kKeyPad = 1 << 30; // ranking key of padding rows (never a real key)
 
 // Distance definitions of the exact path.
@@ -55,15 +55,24 @@ __host__ __device__ inline int plan_cta_of(long long w, long long W, long long G
 ExactPlan make_exact_plan(int q_n, int r_n, int num_sms);
 
 // Per-row squared norms of u8 descriptors (or zeros for kMetricDot), padded
-// to n_pad rows with kKeyPad, plus the minimum over each group of 32 rows.
-cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* norm, int32_t* group_min,
-                                cudaStream_t stream);
+// to n_pad rows (a multiple of 32) with kKeyPad, plus the minimum over each
+// group of 8 rows (gmin8) and of 32 rows (gmin32); both optional. When
+// `thresh` is given, thresh[0 .. n_pad) is set to INT_MAX (the per-query
+// shared pruning threshold of the search kernel).
+cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* norm, int32_t* gmin8,
+                                int32_t* gmin32, int32_t* thresh, cudaStream_t stream);
 
-// The fused GEMM + top-2 kernel. partial: [max_splits][2][q_pad] int4
-// {key1, idx1, key2, idx2} with key = norm(b) - 2 q.b.
-cudaError_t launch_exact2nn_u8(const CUtensorMap& qmap, const CUtensorMap& bmap, const int32_t* bnorm,
-                               const int32_t* bgmin, const ExactPlan& plan, int4* partial, int* err,
-                               cudaStream_t stream);
+// The fused GEMM + top-2 kernel. partial: [max_splits][q_pad] int4
+// {key1, idx1, key2, idx2} with key = norm(b) - 2 q.b. thresh: [q_pad]
+// per-query upper bounds of the second-best key shared by the CTAs that
+// split one query group.
+struct BaseNorms {
+    const int32_t* norm;    // [r_pad]
+    const int32_t* gmin8;   // [r_pad / 8]
+    const int32_t* gmin32;  // [r_pad / 32]
+};
+cudaError_t launch_exact2nn_u8(const CUtensorMap& qmap, const CUtensorMap& bmap, const BaseNorms& bn,
+                               const ExactPlan& plan, int4* partial, int32_t* thresh, int* err, cudaStream_t stream);
 
 // Merge of the per-CTA partial top-2 lists, distances, ratio test and output.
 // Any output pointer may be null.

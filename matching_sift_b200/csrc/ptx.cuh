@@ -46,19 +46,30 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
         : "memory");
     return done != 0;
 }
+// try_wait with a suspend-time hint: the thread may sleep (instead of
+// spinning) until the phase completes or about `ns` nanoseconds pass.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint32_t bar, uint32_t parity, uint32_t ns) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity), "r"(ns)
+        : "memory");
+    return done != 0;
+}
 
 // Waits until the phase with the given parity has completed. Returns false
 // (after recording `code` in *err and raising the CTA abort flag) when the
 // wait exceeds kWaitTimeoutNs or another thread has already aborted.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* err,
                                           int code) {
-    #pragma unroll 1
-    for (int i = 0; i < 32; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = globaltimer();
     #pragma unroll 1
     while (true) {
-        if (mbar_try_wait(bar, parity)) return true;
+        if (mbar_try_wait_sleep(bar, parity, 20000u)) return true;
         if (*abort_flag) return false;
         if (globaltimer() - t0 > kWaitTimeoutNs) {
             *abort_flag = 1;
