@@ -212,9 +212,7 @@ int exact_match(const MatchArgs& a) {
     const size_t o_ru8 = (need_pack || stage_u8) ? L.take(static_cast<size_t>(r_n) * kDim + 16) : 0;
     const size_t o_qf = stage_f32 ? L.take(static_cast<size_t>(q_n) * kDim * 4) : 0;
     const size_t o_rf = stage_f32 ? L.take(static_cast<size_t>(r_n) * kDim * 4 + 16) : 0;
-    const size_t o_bnorm = L.take(static_cast<size_t>(plan.r_pad) * 4 + 16);
-    const size_t o_bgmin8 = L.take(static_cast<size_t>(plan.r_pad / 8) * 4 + 16);
-    const size_t o_bgmin32 = L.take(static_cast<size_t>(plan.r_pad / 32) * 4 + 16);
+    const size_t o_brec = L.take(static_cast<size_t>(plan.base_tiles) * kRecInts * 4 + 16);
     const size_t o_qnorm = L.take(static_cast<size_t>(plan.q_pad) * 4);
     const size_t o_thr = L.take(static_cast<size_t>(plan.q_pad) * 4);
     const size_t o_part = L.take(static_cast<size_t>(plan.max_splits) * plan.q_pad * sizeof(int4));
@@ -263,13 +261,11 @@ int exact_match(const MatchArgs& a) {
     }
 
     // ---- norms
-    int32_t* bnorm = reinterpret_cast<int32_t*>(A + o_bnorm);
-    int32_t* bgmin8 = reinterpret_cast<int32_t*>(A + o_bgmin8);
-    int32_t* bgmin32 = reinterpret_cast<int32_t*>(A + o_bgmin32);
+    int32_t* brec = reinterpret_cast<int32_t*>(A + o_brec);
     int32_t* qnorm = reinterpret_cast<int32_t*>(A + o_qnorm);
     int32_t* thresh = reinterpret_cast<int32_t*>(A + o_thr);
-    SIFT_CUDA(launch_row_norms_u8(rd, r_n, plan.r_pad, a.metric, bnorm, bgmin8, bgmin32, nullptr, st));
-    SIFT_CUDA(launch_row_norms_u8(qd, q_n, plan.q_pad, kMetricL2, qnorm, nullptr, nullptr, thresh, st));
+    SIFT_CUDA(launch_row_norms_u8(rd, r_n, plan.r_pad, a.metric, nullptr, brec, nullptr, st));
+    SIFT_CUDA(launch_row_norms_u8(qd, q_n, plan.q_pad, kMetricL2, qnorm, nullptr, thresh, st));
     g_launches += (plan.r_pad > 0 ? 1 : 0) + 1;
 
     // ---- fused GEMM + top-2
@@ -285,8 +281,7 @@ int exact_match(const MatchArgs& a) {
             SIFT_CUDA(cudaEventCreate(&e1));
             SIFT_CUDA(cudaEventRecord(e0, st));
         }
-        const BaseNorms bn{bnorm, bgmin8, bgmin32};
-        SIFT_CUDA(launch_exact2nn_u8(qmap, bmap, bn, plan, partial, thresh, c.d_status, st));
+        SIFT_CUDA(launch_exact2nn_u8(qmap, bmap, brec, plan, partial, thresh, c.d_status, st));
         ++g_launches;
         if (prof) {
             SIFT_CUDA(cudaEventRecord(e1, st));

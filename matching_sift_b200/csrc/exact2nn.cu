@@ -47,12 +47,14 @@ namespace sift {
 
 namespace {
 
-constexpr int kQTileBytes = kBM * kDim;  // 16 KB: one query tile (u8)
-constexpr int kBTileBytes = kBN * kDim;  // 16 KB: one base tile (u8)
+constexpr int kQTileBytes = kBM * kDim;           // 16 KB: one query tile (u8)
+constexpr int kBTileBytes = kBN * kDim;           // 16 KB: one base tile (u8)
+constexpr int kRecBytes = kRecInts * 4;           // 640 B: norms record of one base tile
 
 struct __align__(8) SmemCtl {
-    uint64_t full[kStages];
-    uint64_t empty[kStages];
+    uint64_t full[kStages];    // base tile + norms record landed (TMA)
+    uint64_t empty[kStages];   // MMAs reading the base tile done (tcgen05.commit)
+    uint64_t nempty[kStages];  // all epilogue warps done with the norms record
     uint64_t qfull, qempty;
     uint64_t tfull[kQT], tempty[kQT];
     uint64_t drain;
@@ -61,7 +63,8 @@ struct __align__(8) SmemCtl {
     int no_abort;
 };
 
-constexpr size_t kSmemBytes = 1024 + kQT * kQTileBytes + kStages * kBTileBytes + sizeof(SmemCtl);
+constexpr size_t kSmemBytes =
+    1024 + kQT * kQTileBytes + kStages * kBTileBytes + kStages * kRecBytes + sizeof(SmemCtl);
 
 __device__ __forceinline__ int max8(const uint32_t* v) {
     int m = __vimax3_s32(static_cast<int>(v[0]), static_cast<int>(v[1]), static_cast<int>(v[2]));
@@ -90,28 +93,28 @@ __device__ __forceinline__ void top2_update(Top2& s, int key, int idx) {
 }
 
 // One group of 32 consecutive base rows [row0, row0 + 32) for this thread's
-// query row; v[c] = q.b(row0 + c). Two-level pruning: the group bound
-// gmin32 - 2 max(v) first, then per 8-row subgroup gmin8 - 2 max(v[8s..8s+8)).
-// Both are lower bounds of every key in their rows, so a (sub)group whose
-// bound exceeds the thread's threshold holds no candidate.
-__device__ __forceinline__ void scan_group(const uint32_t (&v)[32], int row0, int gmin32,
-                                           const int32_t* __restrict__ gmin8, const int32_t* __restrict__ bnorm,
-                                           Top2& s) {
+// query row; v[c] = q.b(row0 + c); rec points at the group's 32 norms in the
+// shared-memory record, gm8 at its four 8-row minima. Two-level pruning: the
+// group bound gmin32 - 2 max(v) first, then per 8-row subgroup
+// gmin8 - 2 max(v[8k..8k+8)). Both bound every key of their rows from below,
+// so a (sub)group whose bound exceeds the thread's threshold holds no candidate.
+__device__ __forceinline__ void scan_group(const uint32_t (&v)[32], int row0, int gmin32, const int32_t* nrm,
+                                           const int32_t* gm8, Top2& s) {
     int mx[4];
     #pragma unroll
     for (int k = 0; k < 4; ++k) mx[k] = max8(v + 8 * k);
     const int m = max(__vimax3_s32(mx[0], mx[1], mx[2]), mx[3]);
     const bool pass = (gmin32 - 2 * m) <= s.thr;
     if (__any_sync(0xffffffffu, pass)) {
-        const int4 g8 = __ldg(reinterpret_cast<const int4*>(gmin8 + (row0 >> 3)));
+        const int4 g8 = *reinterpret_cast<const int4*>(gm8);
         const int gs[4] = {g8.x, g8.y, g8.z, g8.w};
         #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const bool ps = pass && (gs[k] - 2 * mx[k]) <= s.thr;
             if (__any_sync(0xffffffffu, ps)) {
                 if (ps) {
-                    const int4* nb4 = reinterpret_cast<const int4*>(bnorm + row0 + 8 * k);
-                    const int4 na = __ldg(nb4), nb = __ldg(nb4 + 1);
+                    const int4 na = *reinterpret_cast<const int4*>(nrm + 8 * k);
+                    const int4 nb = *reinterpret_cast<const int4*>(nrm + 8 * k + 4);
                     const int base = row0 + 8 * k;
                     top2_update(s, na.x - 2 * static_cast<int>(v[8 * k + 0]), base + 0);
                     top2_update(s, na.y - 2 * static_cast<int>(v[8 * k + 1]), base + 1);
@@ -129,7 +132,7 @@ __device__ __forceinline__ void scan_group(const uint32_t (&v)[32], int row0, in
 
 __global__ void __launch_bounds__(256) row_norms_u8_kernel(const uint8_t* __restrict__ x, int n, int n_pad,
                                                            int metric, int32_t* __restrict__ norm,
-                                                           int32_t* __restrict__ gmin8, int32_t* __restrict__ gmin32,
+                                                           int32_t* __restrict__ rec,
                                                            int32_t* __restrict__ thresh) {
     // 32 rows per block, 8 threads per row, 16 bytes per thread.
     const int row = blockIdx.x * 32 + (threadIdx.x >> 3);
@@ -147,29 +150,34 @@ __global__ void __launch_bounds__(256) row_norms_u8_kernel(const uint8_t* __rest
     s += __shfl_xor_sync(0xffffffffu, s, 4);
     const int32_t v = row < n ? (metric == kMetricL2 ? static_cast<int32_t>(s) : 0) : kKeyPad;
     __shared__ int32_t nrm[32];
+    // Record of base tile (row / kBN): [0, 128) norms, [128, 144) 8-row minima,
+    // [144, 148) 32-row minima.
+    int32_t* r = rec ? rec + static_cast<size_t>(blockIdx.x / 4) * kRecInts : nullptr;
+    const int part = blockIdx.x & 3;  // which 32-row quarter of the tile
     if (sub == 0) {
         nrm[threadIdx.x >> 3] = v;
         if (norm) norm[row] = v;
+        if (r) r[part * 32 + (threadIdx.x >> 3)] = v;
         if (thresh) thresh[row] = INT_MAX;
     }
     __syncthreads();
-    if (threadIdx.x < 4 && gmin8) {
+    if (threadIdx.x < 4 && r) {
         int m = nrm[8 * threadIdx.x];
         #pragma unroll
         for (int i = 1; i < 8; ++i) m = min(m, nrm[8 * threadIdx.x + i]);
-        gmin8[blockIdx.x * 4 + threadIdx.x] = m;
+        r[128 + part * 4 + threadIdx.x] = m;
     }
-    if (threadIdx.x == 32 && gmin32) {
+    if (threadIdx.x == 32 && r) {
         int m = nrm[0];
         #pragma unroll
         for (int i = 1; i < 32; ++i) m = min(m, nrm[i]);
-        gmin32[blockIdx.x] = m;
+        r[144 + part] = m;
     }
 }
 
 __global__ void __launch_bounds__(kThreads, 1)
     exact2nn_u8_kernel(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap bmap,
-                       const BaseNorms bn, const ExactPlan plan, int4* __restrict__ partial,
+                       const int32_t* __restrict__ brec, const ExactPlan plan, int4* __restrict__ partial,
                        int32_t* __restrict__ thresh, int* __restrict__ err) {
     extern __shared__ uint8_t smem_raw[];
     // 1024-byte alignment for the 128-byte swizzle atoms.
@@ -177,22 +185,25 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint8_t* smem = smem_raw + ((1024u - (raw_u32 & 1023u)) & 1023u);
     uint8_t* q_smem = smem;
     uint8_t* b_smem = smem + kQT * kQTileBytes;
-    SmemCtl* ctl = reinterpret_cast<SmemCtl*>(b_smem + kStages * kBTileBytes);
+    int32_t* r_smem = reinterpret_cast<int32_t*>(b_smem + kStages * kBTileBytes);
+    SmemCtl* ctl = reinterpret_cast<SmemCtl*>(r_smem + kStages * kRecInts);
     const uint32_t q_s = ptx::smem_u32(q_smem);
     const uint32_t b_s = ptx::smem_u32(b_smem);
+    const uint32_t r_s = ptx::smem_u32(r_smem);
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const long long W = plan.units;
     const long long G = plan.grid;
     const long long w_begin = plan_w0(blockIdx.x, W, G);
-    const long long w_end = plan_w0(blockIdx.x + 1, W, G);
+    const int n_units = static_cast<int>(plan_w0(blockIdx.x + 1, W, G) - w_begin);
     const int BT = plan.base_tiles;
     const int g_begin = static_cast<int>(w_begin / BT);
     const int j_begin = static_cast<int>(w_begin - static_cast<long long>(g_begin) * BT);
 
     const uint32_t bar_full = ptx::smem_u32(&ctl->full[0]);
     const uint32_t bar_empty = ptx::smem_u32(&ctl->empty[0]);
+    const uint32_t bar_nempty = ptx::smem_u32(&ctl->nempty[0]);
     const uint32_t bar_qfull = ptx::smem_u32(&ctl->qfull);
     const uint32_t bar_qempty = ptx::smem_u32(&ctl->qempty);
     const uint32_t bar_tfull = ptx::smem_u32(&ctl->tfull[0]);
@@ -203,6 +214,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int s = 0; s < kStages; ++s) {
             ptx::mbar_init(bar_full + 8 * s, 1);
             ptx::mbar_init(bar_empty + 8 * s, 1);
+            ptx::mbar_init(bar_nempty + 8 * s, kEpiWarps);
         }
         ptx::mbar_init(bar_qfull, 1);
         ptx::mbar_init(bar_qempty, 1);
@@ -233,8 +245,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             ptx::tma_prefetch_desc(&bmap);
             int cur_g = -1, ngroups = 0;
             int g = g_begin, j = j_begin;
-            long long n = 0;
-            for (long long w = w_begin; w < w_end; ++w) {
+            int n = 0;
+            for (; n < n_units; ++n) {
                 if (g != cur_g) {
                     if (ngroups > 0 &&
                         !ptx::mbar_wait(bar_qempty, (ngroups - 1) & 1, abort_flag, err, kErrWaitQuery))
@@ -247,18 +259,19 @@ __global__ void __launch_bounds__(kThreads, 1)
                     cur_g = g;
                     ++ngroups;
                 }
-                const int s = static_cast<int>(n % kStages);
-                const uint32_t r = static_cast<uint32_t>(n / kStages);
-                if (!ptx::mbar_wait(bar_empty + 8 * s, (r & 1) ^ 1, abort_flag, err, kErrWaitProducer)) break;
-                ptx::mbar_arrive_expect_tx(bar_full + 8 * s, kBTileBytes);
+                const int s = n % kStages;
+                const uint32_t par = ((n / kStages) & 1) ^ 1;
+                if (!ptx::mbar_wait(bar_empty + 8 * s, par, abort_flag, err, kErrWaitProducer)) break;
+                if (!ptx::mbar_wait(bar_nempty + 8 * s, par, abort_flag, err, kErrWaitProducer)) break;
+                ptx::mbar_arrive_expect_tx(bar_full + 8 * s, kBTileBytes + kRecBytes);
                 ptx::tma_load_2d(b_s + s * kBTileBytes, &bmap, 0, j * kBN, bar_full + 8 * s);
-                ++n;
+                ptx::bulk_load(r_s + s * kRecBytes, brec + static_cast<size_t>(j) * kRecInts, kRecBytes,
+                               bar_full + 8 * s);
                 if (++j == BT) { j = 0; ++g; }
             }
             // Drain: every issued copy lands before the CTA may exit.
-            for (long long k = (n > kStages ? n - kStages : 0); k < n; ++k)
-                ptx::mbar_wait(bar_full + 8 * static_cast<int>(k % kStages), static_cast<uint32_t>(k / kStages) & 1,
-                               never, err, kErrWaitDrain);
+            for (int k = (n > kStages ? n - kStages : 0); k < n; ++k)
+                ptx::mbar_wait(bar_full + 8 * (k % kStages), (k / kStages) & 1, never, err, kErrWaitDrain);
             if (ngroups > 0) ptx::mbar_wait(bar_qfull, (ngroups - 1) & 1, never, err, kErrWaitDrain);
         }
         __syncwarp();
@@ -269,18 +282,16 @@ __global__ void __launch_bounds__(kThreads, 1)
             int cur_g = -1, ngroups = 0, nqt = 0;
             int g = g_begin, j = j_begin;
             uint32_t use_parity = 0;  // bit t: parity of the accumulator uses of tile t so far
-            long long n = 0;
             bool ok = true;
-            for (long long w = w_begin; w < w_end && ok; ++w, ++n) {
+            for (int n = 0; n < n_units && ok; ++n) {
                 if (g != cur_g) {
                     if (!ptx::mbar_wait(bar_qfull, ngroups & 1, abort_flag, err, kErrWaitQuery)) break;
                     cur_g = g;
                     ++ngroups;
                     nqt = min(kQT, plan.q_tiles - g * kQT);
                 }
-                const int s = static_cast<int>(n % kStages);
-                const uint32_t r = static_cast<uint32_t>(n / kStages);
-                if (!ptx::mbar_wait(bar_full + 8 * s, r & 1, abort_flag, err, kErrWaitMmaFull)) break;
+                const int s = n % kStages;
+                if (!ptx::mbar_wait(bar_full + 8 * s, (n / kStages) & 1, abort_flag, err, kErrWaitMmaFull)) break;
                 ptx::tc_fence_after();
                 const uint32_t b0 = b_s + s * kBTileBytes;
                 #pragma unroll
@@ -304,7 +315,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
                 if (!ok) break;
                 ptx::tc_commit(bar_empty + 8 * s);
-                const bool last_of_group = (w + 1 == w_end) || (j + 1 == BT);
+                const bool last_of_group = (n + 1 == n_units) || (j + 1 == BT);
                 if (last_of_group) ptx::tc_commit(bar_qempty);
                 if (++j == BT) { j = 0; ++g; }
             }
@@ -324,9 +335,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         int cur_g = -1, nqt = 0, split = 0, q = 0;
         int g = g_begin, j = j_begin;
         uint32_t use = 0;
-        bool ok = true;
 
-        for (long long w = w_begin; w < w_end && ok; ++w) {
+        for (int n = 0; n < n_units; ++n) {
             if (g != cur_g) {
                 if (cur_g >= 0 && t < nqt)
                     partial[static_cast<size_t>(split) * plan.q_pad + q] = make_int4(st.k1, st.i1, st.k2, st.i2);
@@ -337,39 +347,47 @@ __global__ void __launch_bounds__(kThreads, 1)
                 split = static_cast<int>(blockIdx.x) - plan_cta_of(static_cast<long long>(g) * BT, W, G);
                 q = (g * kQT + t) * kBM + quarter * 32 + lane;
             }
-            if (t < nqt) {
-                // Bound shared with the other CTAs that scan this query's group.
-                st.thr = min(st.thr, __ldcg(thresh + q));
-                const int row0 = j * kBN;
-                const int4 gm = __ldg(reinterpret_cast<const int4*>(bn.gmin32 + (row0 >> 5)));
-                const bool waited = ptx::mbar_wait(bar_tfull + 8 * t, use & 1, abort_flag, err, kErrWaitEpilogue);
-                if (!__all_sync(0xffffffffu, waited)) {
-                    ok = false;
-                    break;
-                }
+            const bool active = t < nqt;
+            // Bound shared with the other CTAs that scan this query's group;
+            // loaded before the waits so its latency hides behind them.
+            const int shared_thr = active ? __ldcg(thresh + q) : INT_MAX;
+            const int s = n % kStages;
+            bool waited = ptx::mbar_wait(bar_full + 8 * s, (n / kStages) & 1, abort_flag, err, kErrWaitEpilogue);
+            if (active && waited)
+                waited = ptx::mbar_wait(bar_tfull + 8 * t, use & 1, abort_flag, err, kErrWaitEpilogue);
+            if (!__all_sync(0xffffffffu, waited)) break;
+            if (active) {
                 ++use;
                 ptx::tc_fence_after();
-                uint32_t va[32];
+                st.thr = min(st.thr, shared_thr);
+                const int32_t* rec = r_smem + s * kRecInts;
+                const int4 gm = *reinterpret_cast<const int4*>(rec + 144);
+                const int row0 = j * kBN;
+                // TMEM loads are software-pipelined: group k + 1 is in flight
+                // while group k is scanned.
+                uint32_t va[32], vb[32];
                 ptx::tmem_ld32(taddr0, va);
                 ptx::tmem_ld_wait(va);
-                scan_group(va, row0, gm.x, bn.gmin8, bn.norm, st);
-                ptx::tmem_ld32(taddr0 + 32, va);
-                ptx::tmem_ld_wait(va);
-                scan_group(va, row0 + 32, gm.y, bn.gmin8, bn.norm, st);
+                ptx::tmem_ld32(taddr0 + 32, vb);
+                scan_group(va, row0, gm.x, rec, rec + 128, st);
+                ptx::tmem_ld_wait(vb);
                 ptx::tmem_ld32(taddr0 + 64, va);
+                scan_group(vb, row0 + 32, gm.y, rec + 32, rec + 132, st);
                 ptx::tmem_ld_wait(va);
-                scan_group(va, row0 + 64, gm.z, bn.gmin8, bn.norm, st);
-                ptx::tmem_ld32(taddr0 + 96, va);
-                ptx::tmem_ld_wait(va);
+                ptx::tmem_ld32(taddr0 + 96, vb);
+                scan_group(va, row0 + 64, gm.z, rec + 64, rec + 136, st);
+                ptx::tmem_ld_wait(vb);
                 ptx::tc_fence_before();
                 __syncwarp();
                 if (lane == 0) ptx::mbar_arrive(bar_tempty + 8 * t);
-                scan_group(va, row0 + 96, gm.w, bn.gmin8, bn.norm, st);
+                scan_group(vb, row0 + 96, gm.w, rec + 96, rec + 140, st);
                 if (st.k2 < published) {
                     atomicMin(thresh + q, st.k2);
                     published = st.k2;
                 }
             }
+            __syncwarp();
+            if (lane == 0) ptx::mbar_arrive(bar_nempty + 8 * s);
             if (++j == BT) { j = 0; ++g; }
         }
         if (cur_g >= 0 && t < nqt)
@@ -475,14 +493,14 @@ ExactPlan make_exact_plan(int q_n, int r_n, int num_sms) {
 
 size_t exact2nn_smem_bytes() { return kSmemBytes; }
 
-cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* norm, int32_t* gmin8,
-                                int32_t* gmin32, int32_t* thresh, cudaStream_t stream) {
+cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* norm, int32_t* rec,
+                                int32_t* thresh, cudaStream_t stream) {
     if (n_pad <= 0) return cudaSuccess;
-    row_norms_u8_kernel<<<n_pad / 32, 256, 0, stream>>>(x, n, n_pad, metric, norm, gmin8, gmin32, thresh);
+    row_norms_u8_kernel<<<n_pad / 32, 256, 0, stream>>>(x, n, n_pad, metric, norm, rec, thresh);
     return cudaGetLastError();
 }
 
-cudaError_t launch_exact2nn_u8(const CUtensorMap& qmap, const CUtensorMap& bmap, const BaseNorms& bn,
+cudaError_t launch_exact2nn_u8(const CUtensorMap& qmap, const CUtensorMap& bmap, const int32_t* brec,
                                const ExactPlan& plan, int4* partial, int32_t* thresh, int* err, cudaStream_t stream) {
     // The shared-memory opt-in is per device; the host API serialises calls per device.
     static bool attr_set[64] = {};
@@ -496,7 +514,7 @@ cudaError_t launch_exact2nn_u8(const CUtensorMap& qmap, const CUtensorMap& bmap,
         if (dev >= 0 && dev < 64) attr_set[dev] = true;
     }
     if (plan.grid <= 0) return cudaSuccess;
-    exact2nn_u8_kernel<<<plan.grid, kThreads, kSmemBytes, stream>>>(qmap, bmap, bn, plan, partial, thresh, err);
+    exact2nn_u8_kernel<<<plan.grid, kThreads, kSmemBytes, stream>>>(qmap, bmap, brec, plan, partial, thresh, err);
     return cudaGetLastError();
 }
 

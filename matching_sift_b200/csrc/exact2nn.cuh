@@ -16,6 +16,7 @@ constexpr int kEpiWarps = 4 * kQT;   // one epilogue warp per (query tile, TMEM 
 constexpr int kThreads = 64 + 32 * kEpiWarps;
 constexpr int kTmemCols = kQT * kBN; // one accumulator slot of kBN columns per query tile
 constexpr int32_t kKeyPad = 1 << 30; // ranking key of padding rows (never a real key)
+constexpr int kRecInts = 160;        // per-base-tile record: 128 norms, 16 8-row minima, 4 32-row minima, pad
 
 // Distance definitions of the exact path.
 enum Metric : int {
@@ -55,23 +56,21 @@ __host__ __device__ inline int plan_cta_of(long long w, long long W, long long G
 ExactPlan make_exact_plan(int q_n, int r_n, int num_sms);
 
 // Per-row squared norms of u8 descriptors (or zeros for kMetricDot), padded
-// to n_pad rows (a multiple of 32) with kKeyPad, plus the minimum over each
-// group of 8 rows (gmin8) and of 32 rows (gmin32); both optional. When
-// `thresh` is given, thresh[0 .. n_pad) is set to INT_MAX (the per-query
-// shared pruning threshold of the search kernel).
-cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* norm, int32_t* gmin8,
-                                int32_t* gmin32, int32_t* thresh, cudaStream_t stream);
+// to n_pad rows (a multiple of kBN) with kKeyPad. Outputs (each optional):
+//   norm[n_pad]                       plain per-row norms
+//   rec[n_pad / kBN][kRecInts]        per base tile of kBN rows: the 128 norms,
+//                                     the 16 minima over 8-row groups and the
+//                                     4 minima over 32-row groups
+//   thresh[n_pad]                     set to INT_MAX (the per-query shared
+//                                     pruning bound of the search kernel)
+cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* norm, int32_t* rec,
+                                int32_t* thresh, cudaStream_t stream);
 
 // The fused GEMM + top-2 kernel. partial: [max_splits][q_pad] int4
-// {key1, idx1, key2, idx2} with key = norm(b) - 2 q.b. thresh: [q_pad]
-// per-query upper bounds of the second-best key shared by the CTAs that
-// split one query group.
-struct BaseNorms {
-    const int32_t* norm;    // [r_pad]
-    const int32_t* gmin8;   // [r_pad / 8]
-    const int32_t* gmin32;  // [r_pad / 32]
-};
-cudaError_t launch_exact2nn_u8(const CUtensorMap& qmap, const CUtensorMap& bmap, const BaseNorms& bn,
+// {key1, idx1, key2, idx2} with key = norm(b) - 2 q.b. brec: base records
+// (see launch_row_norms_u8). thresh: [q_pad] per-query upper bounds of the
+// second-best key shared by the CTAs that split one query group.
+cudaError_t launch_exact2nn_u8(const CUtensorMap& qmap, const CUtensorMap& bmap, const int32_t* brec,
                                const ExactPlan& plan, int4* partial, int32_t* thresh, int* err, cudaStream_t stream);
 
 // Merge of the per-CTA partial top-2 lists, distances, ratio test and output.
