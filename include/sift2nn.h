@@ -151,6 +151,11 @@ SIFT_API void sift_profile_enable(int on);
    kernel time in milliseconds and the number of timed launches. */
 SIFT_API int sift_profile_collect(double* total_ms, int* launches);
 
+/* Selects the exact-search kernel for subsequent calls in this process:
+   0 (default) the CTA-pair kernel (tcgen05 cta_group::2), 1 the single-CTA
+   kernel. Both return identical results. */
+SIFT_API int sift_set_kernel_variant(int variant);
+
 #ifdef __cplusplus
 }
 #endif

@@ -36,6 +36,7 @@ std::mutex g_init_mu;
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 thread_local int t_last_status = SIFT_OK;
 std::atomic<long long> g_launches{0};
+std::atomic<int> g_variant{0};  // 0: CTA-pair kernel, 1: single-CTA kernel
 std::atomic<bool> g_profile{false};
 std::mutex g_prof_mu;
 std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_prof_events;
@@ -167,7 +168,8 @@ int exact_match(const MatchArgs& a) {
     const int q_n = static_cast<int>(a.q_n), r_n = static_cast<int>(a.r_n);
     if (q_n == 0) return SIFT_OK;
 
-    const ExactPlan plan = make_exact_plan(q_n, r_n, c.num_sms);
+    const bool use_pair = g_variant.load() == 0;
+    const ExactPlan plan = use_pair ? make_exact_plan(q_n, r_n, c.num_sms / 2, 2) : make_exact_plan(q_n, r_n, c.num_sms, 1);
 
     // Output placement: direct when the device can write the pointer, else staged.
     const bool m_dev = !a.matches || is_device_accessible(a.matches);
@@ -215,7 +217,7 @@ int exact_match(const MatchArgs& a) {
     const size_t o_brec = L.take(static_cast<size_t>(plan.base_tiles) * kRecInts * 4 + 16);
     const size_t o_qnorm = L.take(static_cast<size_t>(plan.q_pad) * 4);
     const size_t o_thr = L.take(static_cast<size_t>(plan.q_pad) * 4);
-    const size_t o_part = L.take(static_cast<size_t>(plan.max_splits) * plan.q_pad * sizeof(int4));
+    const size_t o_part = L.take(static_cast<size_t>(plan.max_splits) * plan.parts * plan.q_pad * sizeof(int4));
     const size_t o_m = (a.matches && !m_dev) ? L.take(static_cast<size_t>(q_n) * 4) : 0;
     const size_t o_s = (a.sorted && !s_dev) ? L.take(static_cast<size_t>(q_n) * 16) : 0;
     const size_t o_i = (a.nn_idx && !i_dev) ? L.take(static_cast<size_t>(q_n) * 8) : 0;
@@ -273,7 +275,7 @@ int exact_match(const MatchArgs& a) {
     if (r_n > 0) {
         CUtensorMap qmap, bmap;
         SIFT_TRY(encode_u8_rows(&qmap, qd, q_n, kBM));
-        SIFT_TRY(encode_u8_rows(&bmap, rd, r_n, kBN));
+        SIFT_TRY(encode_u8_rows(&bmap, rd, r_n, use_pair ? kBN / 2 : kBN));
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         const bool prof = g_profile.load();
         if (prof) {
@@ -281,7 +283,10 @@ int exact_match(const MatchArgs& a) {
             SIFT_CUDA(cudaEventCreate(&e1));
             SIFT_CUDA(cudaEventRecord(e0, st));
         }
-        SIFT_CUDA(launch_exact2nn_u8(qmap, bmap, brec, plan, partial, thresh, c.d_status, st));
+        if (use_pair)
+            SIFT_CUDA(launch_exact2nn_u8_pair(qmap, bmap, brec, plan, partial, thresh, c.d_status, st));
+        else
+            SIFT_CUDA(launch_exact2nn_u8(qmap, bmap, brec, plan, partial, thresh, c.d_status, st));
         ++g_launches;
         if (prof) {
             SIFT_CUDA(cudaEventRecord(e1, st));
@@ -346,6 +351,11 @@ int profile_collect(double* total_ms, int* launches) {
 }
 
 long long launch_count() { return g_launches.load(); }
+int set_variant(int v) {
+    if (v != 0 && v != 1) return SIFT_ERR_INVALID_ARG;
+    g_variant.store(v);
+    return SIFT_OK;
+}
 void profile_enable(bool on) { g_profile.store(on); }
 
 void set_last_status(int s) { t_last_status = s; }
@@ -439,6 +449,7 @@ const char* sift_version(void) { return "sift2nn-b200 0.1.0 (sm_100a)"; }
 
 long long sift_launch_count(void) { return sift::launch_count(); }
 void sift_profile_enable(int on) { sift::profile_enable(on != 0); }
+int sift_set_kernel_variant(int variant) { return sift::set_variant(variant); }
 int sift_profile_collect(double* total_ms, int* launches) { return sift::profile_collect(total_ms, launches); }
 
 }  // extern "C"

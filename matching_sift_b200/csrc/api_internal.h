@@ -26,6 +26,7 @@ void set_last_status(int s);
 int profile_collect(double* total_ms, int* launches);
 long long launch_count();
 void profile_enable(bool on);
+int set_variant(int v);
 int last_status();
 
 }  // namespace sift

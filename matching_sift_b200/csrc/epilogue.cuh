@@ -1,0 +1,76 @@
+// Epilogue building blocks shared by the exact-search kernels: per-thread
+// running top-2 of one query row and the pruned scan of 32 accumulator
+// columns (see exact2nn.cu for the pruning argument).
+#pragma once
+#include <climits>
+#include <cstdint>
+
+namespace sift {
+namespace {
+
+__device__ __forceinline__ int max8(const uint32_t* v) {
+    int m = __vimax3_s32(static_cast<int>(v[0]), static_cast<int>(v[1]), static_cast<int>(v[2]));
+    m = __vimax3_s32(m, static_cast<int>(v[3]), static_cast<int>(v[4]));
+    m = __vimax3_s32(m, static_cast<int>(v[5]), static_cast<int>(v[6]));
+    return max(m, static_cast<int>(v[7]));
+}
+
+// Per-thread running top-2 of one query row over base rows visited in
+// increasing index order (strict '<' keeps the lower index on ties).
+struct Top2 {
+    int k1, i1, k2, i2;
+    int thr;  // prune bound: rows with key > thr cannot enter the final top-2
+};
+
+__device__ __forceinline__ void top2_update(Top2& s, int key, int idx) {
+    if (key < s.k2) {
+        if (key < s.k1) {
+            s.k2 = s.k1; s.i2 = s.i1;
+            s.k1 = key; s.i1 = idx;
+        } else {
+            s.k2 = key; s.i2 = idx;
+        }
+        s.thr = min(s.thr, s.k2 - 1);
+    }
+}
+
+// One group of 32 consecutive base rows [row0, row0 + 32) for this thread's
+// query row; v[c] = q.b(row0 + c); rec points at the group's 32 norms in the
+// shared-memory record, gm8 at its four 8-row minima. Two-level pruning: the
+// group bound gmin32 - 2 max(v) first, then per 8-row subgroup
+// gmin8 - 2 max(v[8k..8k+8)). Both bound every key of their rows from below,
+// so a (sub)group whose bound exceeds the thread's threshold holds no candidate.
+__device__ __forceinline__ void scan_group(const uint32_t (&v)[32], int row0, int gmin32, const int32_t* nrm,
+                                           const int32_t* gm8, Top2& s) {
+    int mx[4];
+    #pragma unroll
+    for (int k = 0; k < 4; ++k) mx[k] = max8(v + 8 * k);
+    const int m = max(__vimax3_s32(mx[0], mx[1], mx[2]), mx[3]);
+    const bool pass = (gmin32 - 2 * m) <= s.thr;
+    if (__any_sync(0xffffffffu, pass)) {
+        const int4 g8 = *reinterpret_cast<const int4*>(gm8);
+        const int gs[4] = {g8.x, g8.y, g8.z, g8.w};
+        #pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const bool ps = pass && (gs[k] - 2 * mx[k]) <= s.thr;
+            if (__any_sync(0xffffffffu, ps)) {
+                if (ps) {
+                    const int4 na = *reinterpret_cast<const int4*>(nrm + 8 * k);
+                    const int4 nb = *reinterpret_cast<const int4*>(nrm + 8 * k + 4);
+                    const int base = row0 + 8 * k;
+                    top2_update(s, na.x - 2 * static_cast<int>(v[8 * k + 0]), base + 0);
+                    top2_update(s, na.y - 2 * static_cast<int>(v[8 * k + 1]), base + 1);
+                    top2_update(s, na.z - 2 * static_cast<int>(v[8 * k + 2]), base + 2);
+                    top2_update(s, na.w - 2 * static_cast<int>(v[8 * k + 3]), base + 3);
+                    top2_update(s, nb.x - 2 * static_cast<int>(v[8 * k + 4]), base + 4);
+                    top2_update(s, nb.y - 2 * static_cast<int>(v[8 * k + 5]), base + 5);
+                    top2_update(s, nb.z - 2 * static_cast<int>(v[8 * k + 6]), base + 6);
+                    top2_update(s, nb.w - 2 * static_cast<int>(v[8 * k + 7]), base + 7);
+                }
+            }
+        }
+    }
+}
+
+}  // namespace
+}  // namespace sift

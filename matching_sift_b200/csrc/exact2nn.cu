@@ -42,6 +42,7 @@
 #include <algorithm>
 #include "exact2nn.cuh"
 #include "ptx.cuh"
+#include "epilogue.cuh"
 
 namespace sift {
 
@@ -65,70 +66,6 @@ struct __align__(8) SmemCtl {
 
 constexpr size_t kSmemBytes =
     1024 + kQT * kQTileBytes + kStages * kBTileBytes + kStages * kRecBytes + sizeof(SmemCtl);
-
-__device__ __forceinline__ int max8(const uint32_t* v) {
-    int m = __vimax3_s32(static_cast<int>(v[0]), static_cast<int>(v[1]), static_cast<int>(v[2]));
-    m = __vimax3_s32(m, static_cast<int>(v[3]), static_cast<int>(v[4]));
-    m = __vimax3_s32(m, static_cast<int>(v[5]), static_cast<int>(v[6]));
-    return max(m, static_cast<int>(v[7]));
-}
-
-// Per-thread running top-2 of one query row over base rows visited in
-// increasing index order (strict '<' keeps the lower index on ties).
-struct Top2 {
-    int k1, i1, k2, i2;
-    int thr;  // prune bound: rows with key > thr cannot enter the final top-2
-};
-
-__device__ __forceinline__ void top2_update(Top2& s, int key, int idx) {
-    if (key < s.k2) {
-        if (key < s.k1) {
-            s.k2 = s.k1; s.i2 = s.i1;
-            s.k1 = key; s.i1 = idx;
-        } else {
-            s.k2 = key; s.i2 = idx;
-        }
-        s.thr = min(s.thr, s.k2 - 1);
-    }
-}
-
-// One group of 32 consecutive base rows [row0, row0 + 32) for this thread's
-// query row; v[c] = q.b(row0 + c); rec points at the group's 32 norms in the
-// shared-memory record, gm8 at its four 8-row minima. Two-level pruning: the
-// group bound gmin32 - 2 max(v) first, then per 8-row subgroup
-// gmin8 - 2 max(v[8k..8k+8)). Both bound every key of their rows from below,
-// so a (sub)group whose bound exceeds the thread's threshold holds no candidate.
-__device__ __forceinline__ void scan_group(const uint32_t (&v)[32], int row0, int gmin32, const int32_t* nrm,
-                                           const int32_t* gm8, Top2& s) {
-    int mx[4];
-    #pragma unroll
-    for (int k = 0; k < 4; ++k) mx[k] = max8(v + 8 * k);
-    const int m = max(__vimax3_s32(mx[0], mx[1], mx[2]), mx[3]);
-    const bool pass = (gmin32 - 2 * m) <= s.thr;
-    if (__any_sync(0xffffffffu, pass)) {
-        const int4 g8 = *reinterpret_cast<const int4*>(gm8);
-        const int gs[4] = {g8.x, g8.y, g8.z, g8.w};
-        #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const bool ps = pass && (gs[k] - 2 * mx[k]) <= s.thr;
-            if (__any_sync(0xffffffffu, ps)) {
-                if (ps) {
-                    const int4 na = *reinterpret_cast<const int4*>(nrm + 8 * k);
-                    const int4 nb = *reinterpret_cast<const int4*>(nrm + 8 * k + 4);
-                    const int base = row0 + 8 * k;
-                    top2_update(s, na.x - 2 * static_cast<int>(v[8 * k + 0]), base + 0);
-                    top2_update(s, na.y - 2 * static_cast<int>(v[8 * k + 1]), base + 1);
-                    top2_update(s, na.z - 2 * static_cast<int>(v[8 * k + 2]), base + 2);
-                    top2_update(s, na.w - 2 * static_cast<int>(v[8 * k + 3]), base + 3);
-                    top2_update(s, nb.x - 2 * static_cast<int>(v[8 * k + 4]), base + 4);
-                    top2_update(s, nb.y - 2 * static_cast<int>(v[8 * k + 5]), base + 5);
-                    top2_update(s, nb.z - 2 * static_cast<int>(v[8 * k + 6]), base + 6);
-                    top2_update(s, nb.w - 2 * static_cast<int>(v[8 * k + 7]), base + 7);
-                }
-            }
-        }
-    }
-}
 
 __global__ void __launch_bounds__(256) row_norms_u8_kernel(const uint8_t* __restrict__ x, int n, int n_pad,
                                                            int metric, int32_t* __restrict__ norm,
@@ -363,24 +300,22 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const int32_t* rec = r_smem + s * kRecInts;
                 const int4 gm = *reinterpret_cast<const int4*>(rec + 144);
                 const int row0 = j * kBN;
-                // TMEM loads are software-pipelined: group k + 1 is in flight
-                // while group k is scanned.
-                uint32_t va[32], vb[32];
+                uint32_t va[32];
                 ptx::tmem_ld32(taddr0, va);
                 ptx::tmem_ld_wait(va);
-                ptx::tmem_ld32(taddr0 + 32, vb);
                 scan_group(va, row0, gm.x, rec, rec + 128, st);
-                ptx::tmem_ld_wait(vb);
-                ptx::tmem_ld32(taddr0 + 64, va);
-                scan_group(vb, row0 + 32, gm.y, rec + 32, rec + 132, st);
+                ptx::tmem_ld32(taddr0 + 32, va);
                 ptx::tmem_ld_wait(va);
-                ptx::tmem_ld32(taddr0 + 96, vb);
+                scan_group(va, row0 + 32, gm.y, rec + 32, rec + 132, st);
+                ptx::tmem_ld32(taddr0 + 64, va);
+                ptx::tmem_ld_wait(va);
                 scan_group(va, row0 + 64, gm.z, rec + 64, rec + 136, st);
-                ptx::tmem_ld_wait(vb);
+                ptx::tmem_ld32(taddr0 + 96, va);
+                ptx::tmem_ld_wait(va);
                 ptx::tc_fence_before();
                 __syncwarp();
                 if (lane == 0) ptx::mbar_arrive(bar_tempty + 8 * t);
-                scan_group(vb, row0 + 96, gm.w, rec + 96, rec + 140, st);
+                scan_group(va, row0 + 96, gm.w, rec + 96, rec + 140, st);
                 if (st.k2 < published) {
                     atomicMin(thresh + q, st.k2);
                     published = st.k2;
@@ -428,7 +363,7 @@ __global__ void __launch_bounds__(256) merge2nn_kernel(const int4* __restrict__ 
             a2 = k; j2 = i;
         }
     };
-    for (int s = 0; s <= c1 - c0; ++s) {
+    for (int s = 0; s < (c1 - c0 + 1) * plan.parts; ++s) {
         const int4 p = partial[static_cast<size_t>(s) * plan.q_pad + q];
         push(p.x, p.y);
         push(p.z, p.w);
@@ -467,8 +402,9 @@ __global__ void __launch_bounds__(256) merge2nn_kernel(const int4* __restrict__ 
 
 }  // namespace
 
-ExactPlan make_exact_plan(int q_n, int r_n, int num_sms) {
+ExactPlan make_exact_plan(int q_n, int r_n, int num_sms, int parts) {
     ExactPlan p{};
+    p.parts = parts;
     p.q_n = q_n;
     p.r_n = r_n;
     p.q_tiles = (q_n + kBM - 1) / kBM;

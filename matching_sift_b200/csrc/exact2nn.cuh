@@ -44,8 +44,9 @@ struct ExactPlan {
     int q_tiles, q_groups, q_pad;   // q_pad = q_tiles * kBM
     int base_tiles, r_pad;          // r_pad = base_tiles * kBN
     long long units;                // q_groups * base_tiles
-    int grid;                       // persistent CTAs
+    int grid;                       // persistent CTAs (CTA pairs for the pair kernel)
     int max_splits;                 // max CTAs covering one query group
+    int parts;                      // partial top-2 lists per (split, query): column slices
 };
 
 __host__ __device__ inline long long plan_w0(long long c, long long W, long long G) { return (c * W) / G; }
@@ -53,7 +54,9 @@ __host__ __device__ inline int plan_cta_of(long long w, long long W, long long G
     return static_cast<int>(((w + 1) * G - 1) / W);
 }
 
-ExactPlan make_exact_plan(int q_n, int r_n, int num_sms);
+// num_workers: persistent CTAs (or CTA pairs); parts: partial top-2 lists
+// each worker writes per query (one per disjoint column slice it scans).
+ExactPlan make_exact_plan(int q_n, int r_n, int num_workers, int parts);
 
 // Per-row squared norms of u8 descriptors (or zeros for kMetricDot), padded
 // to n_pad rows (a multiple of kBN) with kKeyPad. Outputs (each optional):
@@ -66,12 +69,19 @@ ExactPlan make_exact_plan(int q_n, int r_n, int num_sms);
 cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* norm, int32_t* rec,
                                 int32_t* thresh, cudaStream_t stream);
 
-// The fused GEMM + top-2 kernel. partial: [max_splits][q_pad] int4
+// The fused GEMM + top-2 kernel. partial: [max_splits][parts][q_pad] int4
 // {key1, idx1, key2, idx2} with key = norm(b) - 2 q.b. brec: base records
 // (see launch_row_norms_u8). thresh: [q_pad] per-query upper bounds of the
 // second-best key shared by the CTAs that split one query group.
 cudaError_t launch_exact2nn_u8(const CUtensorMap& qmap, const CUtensorMap& bmap, const int32_t* brec,
                                const ExactPlan& plan, int4* partial, int32_t* thresh, int* err, cudaStream_t stream);
+
+// The same search on CTA pairs (tcgen05 cta_group::2, exact2nn_pair.cu).
+// plan.grid counts pairs; bmap_half must use a box of kBN / 2 rows.
+cudaError_t launch_exact2nn_u8_pair(const CUtensorMap& qmap, const CUtensorMap& bmap_half, const int32_t* brec,
+                                    const ExactPlan& plan, int4* partial, int32_t* thresh, int* err,
+                                    cudaStream_t stream);
+size_t exact2nn_pair_smem_bytes();
 
 // Merge of the per-CTA partial top-2 lists, distances, ratio test and output.
 // Any output pointer may be null.

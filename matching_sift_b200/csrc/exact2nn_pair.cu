@@ -1,0 +1,357 @@
+// Exact 2-NN search kernel on CTA pairs (tcgen05 cta_group::2).
+//
+// Same arithmetic, pruning and outputs as exact2nn_u8_kernel (exact2nn.cu);
+// this kernel only changes how the tensor cores are fed. A cluster of two
+// CTAs on the two SMs of a TPC issues M = 256 MMAs: each CTA keeps its own
+// 128 query rows of a 256-row "pair tile" in shared memory and loads half
+// (64 rows) of every 128-row base tile; the leader CTA issues one
+// 256 x 128 x 32 MMA per K step and the accumulator rows land in the TMEM of
+// the CTA that owns them. Compared with single-CTA 128 x 128 MMAs this halves
+// the base bytes every SM streams per MMA, and it leaves room in TMEM for two
+// accumulator buffers per query tile, so the MMA of the next base tile runs
+// while the epilogue is still scanning the previous one.
+//
+// Per CTA: 2 query tiles x 128 rows (a work group of the pair = 512 queries,
+// the same grouping as the single-CTA kernel), TMEM 4 slots x 128 columns =
+// (query tile, buffer); unit n uses buffer n % 2.
+//
+// Warp roles (kPThreads = 576 per CTA):
+//   warp 0       TMA producer (both CTAs): its own query rows, its half of
+//                each base tile (completion counted on the leader's barrier)
+//                and the full norms record of the tile (local barrier)
+//   warp 1       TMEM allocator (both CTAs); MMA issuer (leader CTA only)
+//   warps 2..17  epilogue (both CTAs): warp w owns query tile (w - 2) / 8,
+//                buffer ((w - 2) / 4) % 2 (so it scans every other unit, all
+//                128 columns) and TMEM lane quarter w % 4
+//
+// The MMA issuer is the critical path: on sm_100a every mbarrier test and
+// every tcgen05.commit costs the issuing thread on the order of a hundred
+// cycles, against 64 cycles per 256 x 128 x 32 MMA. So per unit (8 MMAs) it
+// waits on one stage barrier and one accumulator barrier, both tested one unit
+// ahead so the test latency overlaps MMA issue, and commits once.
+//
+// Barriers and who signals them (L = only the leader's copy is used):
+//   full[s]    (L) both CTAs' base halves of stage s landed        TMA tx
+//   rfull[s]   norms record of stage s landed (per CTA)            TMA tx
+//   sfree[s]   the 8 epilogue warps that scanned stage s's unit are
+//              done: its MMAs completed (they waited on tfull) and its
+//              record is no longer read (per CTA)                  arrive
+//   qfull      (L) query tiles of both CTAs landed                  TMA tx
+//   qempty     MMAs of the current query group done (both CTAs)     commit, multicast
+//   tfull[b]   both query tiles' accumulators of buffer b done      commit, multicast
+//   tempty[b]  (L) the 8 warps of buffer b in each CTA read it      remote arrive
+// Every wait is bounded (2 s); an expired wait raises the CTA's abort flag
+// and records an error code, and every role still reaches the teardown.
+#include <climits>
+#include "exact2nn.cuh"
+#include "ptx.cuh"
+#include "epilogue.cuh"
+
+namespace sift {
+
+namespace {
+
+constexpr int kPQT = 2;                          // query tiles per CTA
+constexpr int kPHalf = kBN / 2;                  // base rows loaded per CTA per unit
+constexpr int kPQTileBytes = kBM * kDim;         // 16 KB
+constexpr int kPBHalfBytes = kPHalf * kDim;      // 8 KB
+constexpr int kPRecBytes = kRecInts * 4;         // 640 B
+constexpr int kPStages = 12;
+constexpr int kPSlots = 2 * kPQT;                // (query tile, buffer)
+constexpr int kPEpiWarps = 16;
+constexpr int kPThreads = 64 + 32 * kPEpiWarps;
+constexpr int kPTmemCols = kPSlots * kBN;        // 512
+constexpr uint16_t kPairMask = 0x3;
+static_assert(kPEpiWarps == 4 * kPSlots, "one epilogue warp per (slot, lane quarter)");
+static_assert(kPQT * 2 * kBM == kQT * kBM, "a pair covers one query group");
+
+struct __align__(8) PairCtl {
+    uint64_t full[kPStages];
+    uint64_t rfull[kPStages];
+    uint64_t sfree[kPStages];
+    uint64_t qfull, qempty;
+    uint64_t tfull[2], tempty[2];
+    uint64_t drain;
+    uint32_t tmem_base;
+    int abort_flag;
+    int no_abort;
+};
+
+constexpr size_t kPSmemBytes =
+    1024 + kPQT * kPQTileBytes + kPStages * kPBHalfBytes + kPStages * kPRecBytes + sizeof(PairCtl);
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
+    exact2nn_u8_pair_kernel(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap bmap,
+                            const int32_t* __restrict__ brec, const ExactPlan plan, int4* __restrict__ partial,
+                            int32_t* __restrict__ thresh, int* __restrict__ err) {
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw_u32 = ptx::smem_u32(smem_raw);
+    uint8_t* smem = smem_raw + ((1024u - (raw_u32 & 1023u)) & 1023u);
+    uint8_t* q_smem = smem;
+    uint8_t* b_smem = smem + kPQT * kPQTileBytes;
+    int32_t* r_smem = reinterpret_cast<int32_t*>(b_smem + kPStages * kPBHalfBytes);
+    PairCtl* ctl = reinterpret_cast<PairCtl*>(r_smem + kPStages * kRecInts);
+    const uint32_t q_s = ptx::smem_u32(q_smem);
+    const uint32_t b_s = ptx::smem_u32(b_smem);
+    const uint32_t r_s = ptx::smem_u32(r_smem);
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const uint32_t rank = ptx::cluster_ctarank();
+    const bool leader = rank == 0;
+    const int pair = static_cast<int>(blockIdx.x >> 1);
+    const long long W = plan.units;
+    const long long G = plan.grid;  // pairs
+    const long long w_begin = plan_w0(pair, W, G);
+    const int n_units = static_cast<int>(plan_w0(pair + 1, W, G) - w_begin);
+    const int BT = plan.base_tiles;
+    const int g_begin = static_cast<int>(w_begin / BT);
+    const int j_begin = static_cast<int>(w_begin - static_cast<long long>(g_begin) * BT);
+
+    const uint32_t bar_full = ptx::smem_u32(&ctl->full[0]);
+    const uint32_t bar_rfull = ptx::smem_u32(&ctl->rfull[0]);
+    const uint32_t bar_sfree = ptx::smem_u32(&ctl->sfree[0]);
+    const uint32_t bar_qfull = ptx::smem_u32(&ctl->qfull);
+    const uint32_t bar_qempty = ptx::smem_u32(&ctl->qempty);
+    const uint32_t bar_tfull = ptx::smem_u32(&ctl->tfull[0]);
+    const uint32_t bar_tempty = ptx::smem_u32(&ctl->tempty[0]);
+    const uint32_t bar_drain = ptx::smem_u32(&ctl->drain);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kPStages; ++s) {
+            ptx::mbar_init(bar_full + 8 * s, 1);
+            ptx::mbar_init(bar_rfull + 8 * s, 1);
+            ptx::mbar_init(bar_sfree + 8 * s, kPEpiWarps / 2);
+        }
+        ptx::mbar_init(bar_qfull, 1);
+        ptx::mbar_init(bar_qempty, 1);
+        for (int b = 0; b < 2; ++b) {
+            ptx::mbar_init(bar_tfull + 8 * b, 1);
+            ptx::mbar_init(bar_tempty + 8 * b, 2 * kPEpiWarps / 2);  // 8 warps of buffer b in each CTA
+        }
+        ptx::mbar_init(bar_drain, 1);
+        ctl->abort_flag = 0;
+        ctl->no_abort = 0;
+        ptx::fence_mbar_init();
+    }
+    if (warp == 1) {
+        ptx::tmem_alloc_pair(ptx::smem_u32(&ctl->tmem_base), kPTmemCols);
+        ptx::tmem_relinquish_pair();
+    }
+    ptx::tc_fence_before();
+    __syncthreads();
+    // Both CTAs' barriers are initialised before any cross-CTA signal.
+    ptx::cluster_sync();
+    ptx::tc_fence_after();
+    const uint32_t tmem = ctl->tmem_base;
+    volatile int* abort_flag = &ctl->abort_flag;
+    volatile int* never = &ctl->no_abort;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ------------------------------------------------ TMA producer
+            ptx::tma_prefetch_desc(&qmap);
+            ptx::tma_prefetch_desc(&bmap);
+            const uint32_t lead_qfull = ptx::mapa(bar_qfull, 0);
+            const uint32_t lead_full = ptx::mapa(bar_full, 0);
+            int cur_g = -1, ngroups = 0;
+            int g = g_begin, j = j_begin;
+            int n = 0;
+            for (; n < n_units; ++n) {
+                if (g != cur_g) {
+                    if (ngroups > 0 &&
+                        !ptx::mbar_wait_cluster(bar_qempty, (ngroups - 1) & 1, abort_flag, err, kErrWaitQuery))
+                        break;
+                    if (leader) ptx::mbar_arrive_expect_tx(bar_qfull, 2 * kPQT * kPQTileBytes);
+                    for (int t = 0; t < kPQT; ++t)
+                        ptx::tma_load_2d_pair(q_s + t * kPQTileBytes, &qmap, 0,
+                                              ((g * kPQT + t) * 2 + static_cast<int>(rank)) * kBM, lead_qfull);
+                    cur_g = g;
+                    ++ngroups;
+                }
+                const int s = n % kPStages;
+                if (!ptx::mbar_wait(bar_sfree + 8 * s, ((n / kPStages) & 1) ^ 1, abort_flag, err, kErrWaitProducer))
+                    break;
+                if (leader) ptx::mbar_arrive_expect_tx(bar_full + 8 * s, 2 * kPBHalfBytes);
+                ptx::tma_load_2d_pair(b_s + s * kPBHalfBytes, &bmap, 0, j * kBN + static_cast<int>(rank) * kPHalf,
+                                      lead_full + 8 * s);
+                ptx::mbar_arrive_expect_tx(bar_rfull + 8 * s, kPRecBytes);
+                ptx::bulk_load(r_s + s * kPRecBytes, brec + static_cast<size_t>(j) * kRecInts, kPRecBytes,
+                               bar_rfull + 8 * s);
+                if (++j == BT) { j = 0; ++g; }
+            }
+            // Drain: this CTA's copies land before it may exit. Records are
+            // counted locally; base halves are consumed once the epilogue
+            // has released the stage.
+            for (int k = (n > kPStages ? n - kPStages : 0); k < n; ++k) {
+                ptx::mbar_wait(bar_rfull + 8 * (k % kPStages), (k / kPStages) & 1, never, err, kErrWaitDrain);
+                ptx::mbar_wait(bar_sfree + 8 * (k % kPStages), (k / kPStages) & 1, never, err, kErrWaitDrain);
+            }
+            if (ngroups > 0)
+                ptx::mbar_wait_cluster(bar_qempty, (ngroups - 1) & 1, never, err, kErrWaitDrain);
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0 && leader) {
+            // -------------------------------------------------- MMA issuer
+            constexpr uint32_t idesc = ptx::idesc_make(2 /*S32*/, 0 /*u8*/, 0 /*u8*/, 2 * kBM, kBN);
+            const uint64_t a_desc0 = ptx::sdesc_sw128(q_s);
+            const uint64_t b_desc0 = ptx::sdesc_sw128(b_s);
+            int cur_g = -1, ngroups = 0;
+            int g = g_begin, j = j_begin;
+            // Barrier tests of unit n issued while unit n - 1's MMAs are issued.
+            bool pre_full = ptx::mbar_try_wait(bar_full, 0);
+            bool pre_tempty = ptx::mbar_try_wait(bar_tempty, 1);
+            for (int n = 0; n < n_units; ++n) {
+                if (g != cur_g) {
+                    if (!ptx::mbar_wait_cluster(bar_qfull, ngroups & 1, abort_flag, err, kErrWaitQuery)) break;
+                    cur_g = g;
+                    ++ngroups;
+                }
+                const int s = n % kPStages;
+                const int buf = n & 1;
+                if (!pre_full &&
+                    !ptx::mbar_wait_cluster(bar_full + 8 * s, (n / kPStages) & 1, abort_flag, err, kErrWaitMmaFull))
+                    break;
+                if (!pre_tempty && !ptx::mbar_wait_cluster(bar_tempty + 8 * buf, ((n >> 1) & 1) ^ 1, abort_flag, err,
+                                                           kErrWaitMmaTmem))
+                    break;
+                // Test the barriers of unit n + 1 now; their latency hides behind this unit's MMAs.
+                if (n + 1 < n_units) {
+                    pre_full = ptx::mbar_try_wait(bar_full + 8 * ((n + 1) % kPStages), ((n + 1) / kPStages) & 1);
+                    pre_tempty = ptx::mbar_try_wait(bar_tempty + 8 * (buf ^ 1), (((n + 1) >> 1) & 1) ^ 1);
+                }
+                ptx::tc_fence_after();
+                const uint64_t b_desc = b_desc0 + static_cast<uint64_t>((s * kPBHalfBytes) >> 4);
+                #pragma unroll
+                for (int t = 0; t < kPQT; ++t) {
+                    const uint32_t d = tmem + (t * 2 + buf) * kBN;
+                    const uint64_t a_desc = a_desc0 + static_cast<uint64_t>((t * kPQTileBytes) >> 4);
+                    #pragma unroll
+                    for (int kk = 0; kk < kDim / 32; ++kk)
+                        ptx::mma_i8_pair(d, a_desc + 2 * kk, b_desc + 2 * kk, idesc, kk > 0 ? 1u : 0u);
+                }
+                ptx::tc_commit_pair_mc(bar_tfull + 8 * buf, kPairMask);
+                const bool last_of_group = (n + 1 == n_units) || (j + 1 == BT);
+                if (last_of_group) ptx::tc_commit_pair_mc(bar_qempty, kPairMask);
+                if (++j == BT) { j = 0; ++g; }
+            }
+            // Drain: all issued MMAs complete before TMEM is released.
+            ptx::tc_commit_pair(bar_drain);
+            ptx::mbar_wait(bar_drain, 0, never, err, kErrWaitDrain);
+        }
+        __syncwarp();
+    } else {
+        // ------------------------------------------------------ epilogue
+        const int e = warp - 2;
+        const int t = e >> 3;             // query tile of this warp
+        const int buf = (e >> 2) & 1;     // accumulator buffer = parity of the units this warp scans
+        const int quarter = warp & 3;     // TMEM lane quarter this warp may access
+        const uint32_t taddr = tmem + (static_cast<uint32_t>(quarter * 32) << 16) + (t * 2 + buf) * kBN;
+        const uint32_t lead_tempty = ptx::mapa(bar_tempty + 8 * buf, 0);
+        Top2 st{INT_MAX, -1, INT_MAX, -1, INT_MAX};
+        int published = INT_MAX;
+        int cur_g = -1, split = 0, q = 0;
+        bool active = false;
+        int g = g_begin, j = j_begin;
+
+        for (int n = 0; n < n_units; ++n) {
+            if (g != cur_g) {
+                if (cur_g >= 0 && active)
+                    partial[(static_cast<size_t>(split) * 2 + buf) * plan.q_pad + q] =
+                        make_int4(st.k1, st.i1, st.k2, st.i2);
+                st = Top2{INT_MAX, -1, INT_MAX, -1, INT_MAX};
+                published = INT_MAX;
+                cur_g = g;
+                const int tile = (g * kPQT + t) * 2 + static_cast<int>(rank);
+                active = tile < plan.q_tiles;
+                split = pair - plan_cta_of(static_cast<long long>(g) * BT, W, G);
+                q = tile * kBM + quarter * 32 + lane;
+            }
+            if ((n & 1) == buf) {
+                const int shared_thr = active ? __ldcg(thresh + q) : INT_MAX;
+                const int s = n % kPStages;
+                const uint32_t rpar = (n / kPStages) & 1, tpar = (static_cast<uint32_t>(n) >> 1) & 1;
+                // Both tests are issued back to back so their latencies overlap.
+                const bool r_ok = ptx::mbar_try_wait(bar_rfull + 8 * s, rpar);
+                const bool t_ok = ptx::mbar_try_wait_cluster(bar_tfull + 8 * buf, tpar, 0u);
+                bool waited = true;
+                if (!r_ok) waited = ptx::mbar_wait(bar_rfull + 8 * s, rpar, abort_flag, err, kErrWaitEpilogue);
+                if (waited && !t_ok)
+                    waited = ptx::mbar_wait_cluster(bar_tfull + 8 * buf, tpar, abort_flag, err, kErrWaitEpilogue);
+                if (!__all_sync(0xffffffffu, waited)) break;
+                ptx::tc_fence_after();
+                if (active) {
+                    st.thr = min(st.thr, shared_thr);
+                    const int32_t* rec = r_smem + s * kRecInts;
+                    const int4 gm = *reinterpret_cast<const int4*>(rec + 144);
+                    const int row0 = j * kBN;
+                    uint32_t va[32];
+                    ptx::tmem_ld32(taddr, va);
+                    ptx::tmem_ld_wait(va);
+                    scan_group(va, row0, gm.x, rec, rec + 128, st);
+                    ptx::tmem_ld32(taddr + 32, va);
+                    ptx::tmem_ld_wait(va);
+                    scan_group(va, row0 + 32, gm.y, rec + 32, rec + 132, st);
+                    ptx::tmem_ld32(taddr + 64, va);
+                    ptx::tmem_ld_wait(va);
+                    scan_group(va, row0 + 64, gm.z, rec + 64, rec + 136, st);
+                    ptx::tmem_ld32(taddr + 96, va);
+                    ptx::tmem_ld_wait(va);
+                    ptx::tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) ptx::mbar_arrive_cluster_relaxed(lead_tempty);
+                    scan_group(va, row0 + 96, gm.w, rec + 96, rec + 140, st);
+                    if (st.k2 < published) {
+                        atomicMin(thresh + q, st.k2);
+                        published = st.k2;
+                    }
+                } else {
+                    ptx::tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) ptx::mbar_arrive_cluster_relaxed(lead_tempty);
+                }
+                __syncwarp();
+                if (lane == 0) ptx::mbar_arrive(bar_sfree + 8 * s);
+            }
+            if (++j == BT) { j = 0; ++g; }
+        }
+        if (cur_g >= 0 && active)
+            partial[(static_cast<size_t>(split) * 2 + buf) * plan.q_pad + q] = make_int4(st.k1, st.i1, st.k2, st.i2);
+    }
+
+    ptx::tc_fence_before();
+    __syncthreads();
+    // The leader's MMAs into this CTA's TMEM are drained and no CTA of the
+    // pair signals the other after this point.
+    ptx::cluster_sync();
+    if (warp == 1) {
+        ptx::tc_fence_after();
+        ptx::tmem_dealloc_pair(tmem, kPTmemCols);
+    }
+}
+
+}  // namespace
+
+size_t exact2nn_pair_smem_bytes() { return kPSmemBytes; }
+
+cudaError_t launch_exact2nn_u8_pair(const CUtensorMap& qmap, const CUtensorMap& bmap_half, const int32_t* brec,
+                                    const ExactPlan& plan, int4* partial, int32_t* thresh, int* err,
+                                    cudaStream_t stream) {
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+        e = cudaFuncSetAttribute(exact2nn_u8_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kPSmemBytes));
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) attr_set[dev] = true;
+    }
+    if (plan.grid <= 0) return cudaSuccess;
+    exact2nn_u8_pair_kernel<<<2 * plan.grid, kPThreads, kPSmemBytes, stream>>>(qmap, bmap_half, brec, plan, partial,
+                                                                               thresh, err);
+    return cudaGetLastError();
+}
+
+}  // namespace sift

@@ -19,6 +19,17 @@ GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 FLT_MAX = np.float32(np.finfo(np.float32).max)
 
 
+KERNELS = {"pair": 0, "single": 1}
+
+
+@pytest.fixture(params=sorted(KERNELS))
+def kernel(request):
+    """Runs a test once per exact-search kernel (CTA-pair and single-CTA)."""
+    ms.lib().sift_set_kernel_variant(KERNELS[request.param])
+    yield request.param
+    ms.lib().sift_set_kernel_variant(0)
+
+
 def _run(q, r, dev, metric=ms.METRIC_L2, threshold=0.8):
     import torch
 
@@ -40,7 +51,7 @@ def _check_against_oracle(q, r, got, metric=ms.METRIC_L2):
 
 
 @pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "host_brute_*.npz"))), ids=os.path.basename)
-def test_golden_host_brute(cuda_device, path):
+def test_golden_host_brute(cuda_device, kernel, path):
     z = np.load(path)
     q, r, ref = z["q"], z["r"], z["sorted"]
     got = _run(q, r, cuda_device)
@@ -48,7 +59,7 @@ def test_golden_host_brute(cuda_device, path):
 
 
 @pytest.mark.parametrize("metric", [ms.METRIC_L2, ms.METRIC_DOT])
-def test_config1_vs_oracle(cuda_device, metric):
+def test_config1_vs_oracle(cuda_device, kernel, metric):
     """1,000 queries x 10,000 base rows from the seeded generator."""
     q, r = datagen.make_workload(1000, 10000, seed=0)
     got = _run(q, r, cuda_device, metric=metric)
@@ -59,13 +70,13 @@ def test_config1_vs_oracle(cuda_device, metric):
 
 @pytest.mark.parametrize("q_n,r_n", [(1, 1), (1, 2), (3, 300), (127, 255), (128, 256), (129, 257), (255, 513),
                                      (256, 1000), (300, 4097), (1000, 77), (2048, 1)])
-def test_ragged_sizes(cuda_device, q_n, r_n):
+def test_ragged_sizes(cuda_device, kernel, q_n, r_n):
     q, r = datagen.make_workload(q_n, r_n, seed=q_n * 7 + r_n)
     got = _run(q, r, cuda_device)
     _check_against_oracle(q, r, got)
 
 
-def test_ties_choose_lower_index(cuda_device):
+def test_ties_choose_lower_index(cuda_device, kernel):
     base = datagen.make_base(300, seed=1)
     r = np.concatenate([base, base, base], axis=0)  # every row three times
     q = np.concatenate([base[::3], datagen.make_base(50, seed=2)], axis=0)
@@ -75,7 +86,7 @@ def test_ties_choose_lower_index(cuda_device):
     assert (got["nn_idx"][:100, 1] == np.arange(0, 300, 3) + 300).all()
 
 
-def test_extreme_values(cuda_device):
+def test_extreme_values(cuda_device, kernel):
     r = np.stack([np.zeros(128, np.uint8), np.full(128, 255, np.uint8)] * 200)
     q = np.stack([np.full(128, 255, np.uint8), np.zeros(128, np.uint8), np.full(128, 128, np.uint8)] * 50)
     got = _run(q, r, cuda_device)
@@ -93,7 +104,7 @@ def test_no_base_rows(cuda_device):
     assert (out["matches"].cpu().numpy().astype(np.int64) & 0xFFFFFFFF == 0xFFFFFFFF).all()
 
 
-def test_scale_subset_vs_oracle(cuda_device):
+def test_scale_subset_vs_oracle(cuda_device, kernel):
     """10,000 x 1,000,000: 96 random queries checked against the oracle, all
     queries checked by recomputing both distances from the returned indices."""
     q, r = datagen.make_workload(10000, 1000000, seed=0)
