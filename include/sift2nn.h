@@ -125,6 +125,24 @@ SIFT_API int sift_last_status(void);
 SIFT_API int sift2nn_match(const void* q, const void* r, int type, uint32_t q_n, uint32_t r_n, int metric, float threshold,
                   uint32_t* matches, sift_float4* sorted, int32_t* nn_idx, float* nn_dist, void* stream);
 
+/* Exact 2-NN that allocates no memory at all (no counterpart in the
+   reference). For callers that cannot allocate device memory at call time:
+   code whose device memory is owned by a custom allocator or pool, real-time
+   loops that cannot take cudaMalloc's implicit synchronisation, hosts that
+   give the library a fixed memory budget up front. The search and results
+   are those of sift2nn_match with type SIFT_U8_DEVICE and SIFT_METRIC_L2;
+   q, r (16-byte aligned uint8 [n][128]) and the outputs (matches[q_n],
+   nn_idx[2*q_n], nn_dist[2*q_n]; any may be NULL) are device memory the
+   caller owns. All scratch lives in one 8 MiB __device__ array of the library
+   (held by every GPU that loads it, until exit), which limits q_n to 16384 and
+   r_n to 1048576: larger sizes return SIFT_ERR_INVALID_ARG. Calls on one
+   device share that array, so calls that overlap on the GPU race: serialise
+   them. The first call on a device looks the array's address up with
+   cudaGetSymbolAddress; make it before any stream capture. Asynchronous on
+   `stream` (NULL = legacy default stream). */
+SIFT_API int sift2nn_match_noalloc(const uint8_t* q, const uint8_t* r, uint32_t q_n, uint32_t r_n, float threshold,
+                                   uint32_t* matches, int32_t* nn_idx, float* nn_dist, void* stream);
+
 /* Synchronises `stream` and returns the device status of the calls issued on
    the current device since the last check (SIFT_OK, SIFT_ERR_DEVICE_TIMEOUT
    when a bounded wait inside a kernel expired, SIFT_ERR_CUDA). */
