@@ -109,12 +109,11 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def _profile_traffic():
-    """DRAM bytes per launch of the search kernel from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "exact2nn_u8_10000x1M.md")
+def _profile_value(name, key):
+    """A `key: value` line of a committed profile summary under profiles/, if present."""
     try:
-        for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
+        for line in open(os.path.join(ROOT, "profiles", name)):
+            if line.startswith(key + ":"):
                 return float(line.split(":", 1)[1].strip())
     except OSError:
         pass
@@ -276,9 +275,13 @@ def main():
         peaks, peak_src = _peaks()
         ops = 2.0 * q_n * R_N * DIM
         achieved = ops / (kernel_ms * 1e-3) / 1e12
-        peak_int8 = 2.0 * peaks["bf16_tflops"]
+        # Dense int8 peak measured on this pool's B200 by matching_sift_b200/peak_int8
+        # (profiles/tcgen05_int8_peak.md); MEASURED_PEAKS.json has no int8 figure.
+        peak_int8 = _profile_value("tcgen05_int8_peak.md", "peak_int8_tops") or 4550.0
+        bf16x2 = 2.0 * peaks["bf16_tflops"]
         qps = world * q_n * args.steps / (step_ms * 1e-3)
         e2e_qps = world * q_n * args.steps / (e2e_ms * 1e-3) if e2e_ms == e2e_ms else None
+        traffic = _profile_value("exact2nn_u8_pair_10000x1M.md", "traffic_bytes_per_launch") if q_n == Q_N else None
         line = {
             "metric": METRIC,
             "value": round(qps, 1),
@@ -300,12 +303,13 @@ def main():
                     "h2d_bytes_per_step": (q_n + R_N) * DIM, "d2h_bytes_per_step": q_n * 4,
                     "call": "cublas_2nn_sift(type=SIFT_U8_HOST) with pinned host buffers"},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "tensor", "kernel": "exact2nn_u8_kernel", "achieved": round(achieved, 1),
+            "roofline": {"bound": "tensor", "kernel": "exact2nn_u8_pair_kernel", "achieved": round(achieved, 1),
                          "peak": round(peak_int8, 1), "unit": "TFLOP/s", "frac": round(achieved / peak_int8, 4),
-                         "traffic": _profile_traffic(),
+                         "traffic": traffic,
                          "ops_per_launch": ops, "kernel_ms": round(kernel_ms, 4),
-                         "peak_note": f"dense int8 peak taken as 2 x {peak_src} bf16 burst "
-                                      f"({peaks['bf16_tflops']} TFLOP/s); nominal 4500"},
+                         "peak_note": "dense int8 tcgen05 peak measured on this pool's B200 (int8 ops counted as 2 "
+                                      "per MAC; MEASURED_PEAKS.json has no int8 figure)",
+                         "frac_of_2x_bf16_" + peak_src: round(achieved / bf16x2, 4)},
             "clocks": clocks.summary(),
         }
         if not args.no_cpu_baseline:

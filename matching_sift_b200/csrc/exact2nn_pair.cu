@@ -216,11 +216,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
                 if (!pre_tempty && !ptx::mbar_wait_cluster(bar_tempty + 8 * buf, ((n >> 1) & 1) ^ 1, abort_flag, err,
                                                            kErrWaitMmaTmem))
                     break;
-                // Test the barriers of unit n + 1 now; their latency hides behind this unit's MMAs.
-                if (n + 1 < n_units) {
-                    pre_full = ptx::mbar_try_wait(bar_full + 8 * ((n + 1) % kPStages), ((n + 1) / kPStages) & 1);
-                    pre_tempty = ptx::mbar_try_wait(bar_tempty + 8 * (buf ^ 1), (((n + 1) >> 1) & 1) ^ 1);
-                }
                 ptx::tc_fence_after();
                 const uint64_t b_desc = b_desc0 + static_cast<uint64_t>((s * kPBHalfBytes) >> 4);
                 #pragma unroll
@@ -234,6 +229,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
                 ptx::tc_commit_pair_mc(bar_tfull + 8 * buf, kPairMask);
                 const bool last_of_group = (n + 1 == n_units) || (j + 1 == BT);
                 if (last_of_group) ptx::tc_commit_pair_mc(bar_qempty, kPairMask);
+                // Test the barriers of unit n + 1 now, behind this unit's queued MMAs.
+                if (n + 1 < n_units) {
+                    pre_full = ptx::mbar_try_wait(bar_full + 8 * ((n + 1) % kPStages), ((n + 1) / kPStages) & 1);
+                    pre_tempty = ptx::mbar_try_wait(bar_tempty + 8 * (buf ^ 1), (((n + 1) >> 1) & 1) ^ 1);
+                }
                 if (++j == BT) { j = 0; ++g; }
             }
             // Drain: all issued MMAs complete before TMEM is released.

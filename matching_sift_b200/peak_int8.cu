@@ -1,0 +1,122 @@
+// Dense int8 tensor-core peak of this GPU, and the issue cost of the
+// synchronisation the search kernels put between MMAs.
+//
+// One CTA per SM (or one CTA pair per TPC for cta_group::2), operands resident
+// in shared memory, one thread issuing back-to-back tcgen05.mma.kind::i8 with
+// K = 32 into TMEM, then one commit + bounded wait. MODE adds, per group of 4
+// MMAs: 1 = a tcgen05.commit, 2 = + tcgen05.fence::after_thread_sync,
+// 3 = + an mbarrier.try_wait on an already completed phase.
+// The MAC/clk/SM figure of MODE 0 is the roofline denominator bench.py uses.
+//
+//   make -C matching_sift_b200 peak && matching_sift_b200/peak_int8
+#include <cstdio>
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "csrc/ptx.cuh"
+
+using namespace sift;
+
+template <int M, int N, bool PAIR, int MODE>
+__global__ void __launch_bounds__(128, 1) bench_kernel(int iters, unsigned long long* cycles) {
+    extern __shared__ __align__(1024) uint8_t sm[];
+    uint8_t* base = sm + ((1024 - (ptx::smem_u32(sm) & 1023)) & 1023);
+    __shared__ uint64_t bar;
+    __shared__ uint64_t side[4];
+    __shared__ uint32_t tbase;
+    __shared__ int flag_abort, flag_err;
+    const int warp = threadIdx.x >> 5;
+    // zero operands
+    for (int i = threadIdx.x; i < (128 * 128 + 256 * 128) / 16; i += blockDim.x)
+        reinterpret_cast<uint4*>(base)[i] = make_uint4(0, 0, 0, 0);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (threadIdx.x == 0) {
+        ptx::mbar_init(ptx::smem_u32(&bar), 1);
+        for (int i = 0; i < 4; ++i) ptx::mbar_init(ptx::smem_u32(&side[i]), 1);
+        ptx::fence_mbar_init(); flag_abort = 0; flag_err = 0;
+    }
+    if (warp == 0) {
+        if (PAIR) { ptx::tmem_alloc_pair(ptx::smem_u32(&tbase), 512); ptx::tmem_relinquish_pair(); }
+        else { ptx::tmem_alloc(ptx::smem_u32(&tbase), 512); ptx::tmem_relinquish(); }
+    }
+    ptx::tc_fence_before();
+    __syncthreads();
+    if (PAIR) ptx::cluster_sync();
+    ptx::tc_fence_after();
+    const uint32_t tmem = tbase;
+    const uint32_t rank = PAIR ? ptx::cluster_ctarank() : 0;
+    unsigned long long t0 = clock64();
+    if (threadIdx.x == 0 && rank == 0) {
+        const uint32_t a0 = ptx::smem_u32(base), b0 = a0 + 128 * 128;
+        const uint64_t ad = ptx::sdesc_sw128(a0), bd = ptx::sdesc_sw128(b0);
+        constexpr uint32_t idesc = ptx::idesc_make(2, 0, 0, M, N);
+        for (int i = 0; i < iters; ++i) {
+            const uint32_t k = i & 3;
+            const uint32_t d = tmem + (((i >> 2) & 1) ? (512 - N) : 0);
+            if (MODE >= 3 && k == 0) (void)ptx::mbar_try_wait(ptx::smem_u32(&side[(i >> 2) & 3]), 1);  // a completed phase
+            if (MODE >= 2 && k == 0) ptx::tc_fence_after();
+            if (PAIR) ptx::mma_i8_pair(d, ad + 2 * k, bd + 2 * k, idesc, k > 0);
+            else ptx::mma_i8(d, ad + 2 * k, bd + 2 * k, idesc, k > 0);
+            if (MODE >= 1 && k == 3) {
+                if (PAIR) ptx::tc_commit_pair(ptx::smem_u32(&side[(i >> 2) & 3]));
+                else ptx::tc_commit(ptx::smem_u32(&side[(i >> 2) & 3]));
+            }
+        }
+        if (PAIR) ptx::tc_commit_pair(ptx::smem_u32(&bar)); else ptx::tc_commit(ptx::smem_u32(&bar));
+        ptx::mbar_wait(ptx::smem_u32(&bar), 0, &flag_abort, &flag_err, 1);
+    }
+    __syncwarp();
+    unsigned long long t1 = clock64();
+    if (threadIdx.x == 0 && rank == 0) atomicAdd(cycles, t1 - t0);
+    ptx::tc_fence_before();
+    __syncthreads();
+    if (PAIR) ptx::cluster_sync();
+    if (warp == 0) {
+        ptx::tc_fence_after();
+        if (PAIR) ptx::tmem_dealloc_pair(tmem, 512); else ptx::tmem_dealloc(tmem, 512);
+    }
+}
+
+template <int M, int N, bool PAIR, int MODE = 0>
+void run(const char* name, int sms) {
+    auto k = bench_kernel<M, N, PAIR, MODE>;
+    size_t smem = 1024 + 128 * 128 + 256 * 128;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    unsigned long long* d; cudaMalloc(&d, 8);
+    const int iters = 40000;
+    int grid = sms;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    cfg.gridDim = dim3(grid); cfg.blockDim = dim3(128); cfg.dynamicSmemBytes = smem;
+    if (PAIR) { attr[0].id = cudaLaunchAttributeClusterDimension; attr[0].val.clusterDim.x = 2; attr[0].val.clusterDim.y = 1; attr[0].val.clusterDim.z = 1; cfg.attrs = attr; cfg.numAttrs = 1; }
+    for (int rep = 0; rep < 3; ++rep) {
+        cudaMemset(d, 0, 8);
+        cudaEvent_t e0, e1; cudaEventCreate(&e0); cudaEventCreate(&e1);
+        cudaEventRecord(e0);
+        cudaError_t e = cudaLaunchKernelEx(&cfg, k, iters, d);
+        cudaEventRecord(e1); cudaEventSynchronize(e1);
+        if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) { printf("%s launch error\n", name); return; }
+        float ms; cudaEventElapsedTime(&ms, e0, e1);
+        unsigned long long cyc; cudaMemcpy(&cyc, d, 8, cudaMemcpyDeviceToHost);
+        const int issuers = PAIR ? grid / 2 : grid;
+        double macs = (double)M * N * 32 * iters * issuers;   // M counts both CTAs for a pair
+        double avg_cyc = (double)cyc / issuers;
+        double mac_per_clk_sm = (double)M * N * 32 * iters / avg_cyc / (PAIR ? 2 : 1);
+        printf("%-22s %8.3f ms  %7.1f TOP/s  cycles/MMA %6.1f  MAC/clk/SM %7.0f\n", name, ms, 2 * macs / (ms * 1e-3) / 1e12,
+               avg_cyc / iters, mac_per_clk_sm);
+    }
+}
+
+int main() {
+    int sms; cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    run<128, 64, false, 0>("1cta M128 N64", sms);
+    run<128, 128, false, 0>("1cta M128 N128", sms);
+    run<128, 256, false, 0>("1cta M128 N256", sms);
+    run<256, 128, true, 0>("pair M256 N128", sms);
+    run<256, 256, true, 0>("pair M256 N256", sms);
+    run<128, 128, false, 1>("1cta N128 +commit", sms);
+    run<128, 128, false, 2>("1cta N128 +fence", sms);
+    run<128, 128, false, 3>("1cta N128 +trywait", sms);
+    run<256, 128, true, 1>("pair N128 +commit", sms);
+    run<256, 128, true, 3>("pair N128 +all", sms);
+    return 0;
+}
