@@ -105,6 +105,18 @@ SIFT_API void device_brute(des_t_f* q_points, des_t_f* r_points, int q_n, int r_
    (there is no CPU path in this library). */
 SIFT_API void host_brute(des_t_f* q_points, des_t_f* r_points, int q_points_size, int r_points_size, sift_float4* sorted);
 
+/* Random-hyperplane LSH 2-NN. Replaces lsh_gpu, include/lsh_h.h:69 /
+   src/lsh_h.cu:722. Hyperplanes: l tables of nbits +/-1 planes drawn with the C
+   library's rand() in the reference's order (make_vec_h, src/lsh_h.cu:88-100),
+   so a caller that seeds rand() identically gets the reference's hash family.
+   matches[q] = nearest base row among the members of the query's bucket in
+   any table (exact squared distance, lower index on ties), UINT32_MAX when no
+   bucket holds a candidate. threshold, handle, stream_n and lsh_type are
+   accepted and ignored, as in the reference. Unlike the reference, the
+   caller's buffers are not freed. Synchronises. */
+SIFT_API int lsh_gpu(void* q_points, void* r_points, int type, uint32_t q_n, uint32_t r_n, uint32_t* matches,
+                     float threshold, cublasHandle_t handle, int stream_n, int l, int lsh_type, int nbits);
+
 /* Status of the last void call above on this thread (SIFT_OK or SIFT_ERR_*). */
 SIFT_API int sift_last_status(void);
 
@@ -124,6 +136,22 @@ SIFT_API int sift_last_status(void);
    host output makes the call synchronous. */
 SIFT_API int sift2nn_match(const void* q, const void* r, int type, uint32_t q_n, uint32_t r_n, int metric, float threshold,
                   uint32_t* matches, sift_float4* sorted, int32_t* nn_idx, float* nn_dist, void* stream);
+
+/* LSH codes of n u8 descriptors (device memory, 16-byte aligned):
+   codes[t * n + i] bit j is set when x_i . planes[t][j] < 0, for L tables of
+   k bits (k <= 32, L * k <= 256). planes: int8 [L][k][128] in device memory.
+   The dot products are exact (u8 x s8 -> s32 on the tensor cores). */
+SIFT_API int sift_lsh_hash(const uint8_t* x, uint32_t n, const int8_t* planes, int L, int k, uint32_t* codes,
+                           void* stream);
+
+/* LSH 2-NN with caller-given int8 hyperplanes [L][k][128] (host or device
+   memory): each query is compared exactly with the base rows that share its
+   code in at least one table. Outputs as sift2nn_match (nn_dist = squared
+   distances; -1 / FLT_MAX where fewer than 1 / 2 candidates); matches applies
+   the ratio test when threshold > 0, else holds the nearest candidate. */
+SIFT_API int sift_lsh_match(const void* q, const void* r, int type, uint32_t q_n, uint32_t r_n, const int8_t* planes,
+                            int L, int k, float threshold, uint32_t* matches, int32_t* nn_idx, float* nn_dist,
+                            void* stream);
 
 /* Exact 2-NN that allocates no memory at all (no counterpart in the
    reference). For callers that cannot allocate device memory at call time:

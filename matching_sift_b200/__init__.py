@@ -19,7 +19,8 @@ from ._native import (FLOAT_DEVICE, FLOAT_HOST, HALF_DEVICE, METRIC_DOT, METRIC_
                       SiftError, check, lib, status_string)
 
 __all__ = [
-    "cublas_2nn_sift", "cublas_2nn_f", "device_brute", "host_brute", "match", "stream_status", "version",
+    "cublas_2nn_sift", "cublas_2nn_f", "device_brute", "host_brute", "lsh_gpu", "match", "lsh_match", "lsh_hash",
+    "stream_status", "version",
     "SiftError", "FLOAT_HOST", "FLOAT_DEVICE", "HALF_DEVICE", "U8_DEVICE", "U8_HOST", "METRIC_L2", "METRIC_DOT",
 ]
 
@@ -69,6 +70,13 @@ def host_brute(q_points, r_points, q_points_size, r_points_size, sorted) -> None
     check(lib().sift_last_status(), "host_brute")
 
 
+def lsh_gpu(q_points, r_points, type, q_n, r_n, matches, threshold, handle=None, stream_n=2, l=1, lsh_type=0,
+            nbits=16) -> int:
+    """Random-hyperplane LSH 2-NN (reference src/lsh_h.cu:722). Returns the status code."""
+    return lib().lsh_gpu(_ptr(q_points), _ptr(r_points), type, q_n, r_n, _ptr(matches), threshold, _ptr(handle),
+                         stream_n, l, lsh_type, nbits)
+
+
 def stream_status(stream=None) -> int:
     return lib().sift_stream_status(_ptr(stream) if stream is not None else None)
 
@@ -110,4 +118,39 @@ def match(q, r, threshold: float = 0.8, metric: int = METRIC_L2, stream=None, ou
     check(rc, "sift2nn_match")
     if "matches" in out:
         out["matches"] = out["matches"].view(torch.uint32) if hasattr(torch, "uint32") else out["matches"]
+    return out
+
+
+def lsh_hash(x, planes, stream=None):
+    """LSH codes [L, n] (int32 view of uint32) of uint8 CUDA rows x [n, 128] for int8 planes [L, k, 128]."""
+    import torch
+
+    L, k = planes.shape[0], planes.shape[1]
+    x = x.contiguous()
+    planes = planes.contiguous()
+    codes = torch.empty((L, x.shape[0]), dtype=torch.int32, device=x.device)
+    s = stream if stream is not None else torch.cuda.current_stream(x.device)
+    check(lib().sift_lsh_hash(x.data_ptr(), x.shape[0], planes.data_ptr(), L, k, codes.data_ptr(), s.cuda_stream),
+          "sift_lsh_hash")
+    return codes
+
+
+def lsh_match(q, r, planes, threshold: float = 0.0, stream=None):
+    """LSH 2-NN of uint8 CUDA tensors with int8 hyperplanes planes [L, k, 128].
+
+    Returns {"matches", "nn_idx", "nn_dist"} like match(); only base rows
+    sharing a code with the query in some table are candidates.
+    """
+    import torch
+
+    L, k = planes.shape[0], planes.shape[1]
+    q, r, planes = q.contiguous(), r.contiguous(), planes.contiguous()
+    n = q.shape[0]
+    out = {"matches": torch.empty(n, dtype=torch.int32, device=q.device),
+           "nn_idx": torch.empty((n, 2), dtype=torch.int32, device=q.device),
+           "nn_dist": torch.empty((n, 2), dtype=torch.float32, device=q.device)}
+    s = stream if stream is not None else torch.cuda.current_stream(q.device)
+    check(lib().sift_lsh_match(q.data_ptr(), r.data_ptr(), U8_DEVICE, n, r.shape[0], planes.data_ptr(), L, k,
+                               threshold, out["matches"].data_ptr(), out["nn_idx"].data_ptr(),
+                               out["nn_dist"].data_ptr(), s.cuda_stream), "sift_lsh_match")
     return out

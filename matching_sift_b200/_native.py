@@ -40,6 +40,11 @@ _PROTOS = {
     "sift_profile_enable": (None, [ctypes.c_int]),
     "sift_profile_collect": (ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]),
     "sift_set_kernel_variant": (ctypes.c_int, [ctypes.c_int]),
+    "lsh_gpu": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, _vp, ctypes.c_float, _vp,
+                               ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "sift_lsh_hash": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "sift_lsh_match": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, _vp, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_float, _vp, _vp, _vp, _vp]),
     "sift2nn_match_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, _vp, _vp,
                                              _vp, _vp]),
 }

@@ -14,6 +14,8 @@
 #include "api_internal.h"
 #include "exact2nn.cuh"
 #include "pack.cuh"
+#include "lsh.cuh"
+#include <cstdlib>
 
 namespace sift {
 
@@ -152,6 +154,101 @@ int collect_device_status(DeviceCtx& c, cudaStream_t st) {
 
 }  // namespace
 
+// Where the u8 descriptors a kernel reads come from, for every memory type.
+struct InputPlan {
+    const void* q_src = nullptr;
+    const void* r_src = nullptr;
+    bool need_pack = false;  // float / half -> u8 conversion
+    bool stage_u8 = false;   // copy u8 rows into the arena
+    bool stage_f32 = false;  // copy host float rows into the arena first
+    size_t o_qu8 = 0, o_ru8 = 0, o_qf = 0, o_rf = 0;
+};
+
+int plan_inputs(const void* q, const void* r, int type, int q_n, int r_n, Layout& L, InputPlan& ip) {
+    if (q_n > 0 && !q) return SIFT_ERR_INVALID_ARG;
+    if (r_n > 0 && !r) return SIFT_ERR_INVALID_ARG;
+    if (type < SIFT_FLOAT_HOST || type > SIFT_U8_HOST) return SIFT_ERR_INVALID_ARG;
+    ip.q_src = q;
+    ip.r_src = r;
+    ip.need_pack = type != SIFT_U8_DEVICE && type != SIFT_U8_HOST;
+    ip.stage_u8 = type == SIFT_U8_HOST;
+    if (type == SIFT_U8_DEVICE) {
+        // TMA needs 16-byte aligned rows; unaligned device input is copied.
+        ip.stage_u8 = (reinterpret_cast<uintptr_t>(q) & 15) || (reinterpret_cast<uintptr_t>(r) & 15);
+    }
+    if (type == SIFT_FLOAT_HOST) {
+        // Zero-copy like the reference (src/knn_brute.cu:58, :223) when the
+        // memory is mapped pinned memory; otherwise stage it.
+        void* qm = nullptr;
+        void* rm = nullptr;
+        if (cudaHostGetDevicePointer(&qm, const_cast<void*>(q), 0) == cudaSuccess &&
+            (r_n == 0 || cudaHostGetDevicePointer(&rm, const_cast<void*>(r), 0) == cudaSuccess) &&
+            !(reinterpret_cast<uintptr_t>(qm) & 15) && !(reinterpret_cast<uintptr_t>(rm) & 15)) {
+            ip.q_src = qm;
+            ip.r_src = rm;
+        } else {
+            cudaGetLastError();
+            ip.stage_f32 = true;
+        }
+    }
+    if ((type == SIFT_FLOAT_DEVICE || type == SIFT_HALF_DEVICE) &&
+        ((reinterpret_cast<uintptr_t>(q) & 15) || (reinterpret_cast<uintptr_t>(r) & 15)))
+        return SIFT_ERR_INVALID_ARG;
+    if (ip.need_pack || ip.stage_u8) {
+        ip.o_qu8 = L.take(static_cast<size_t>(q_n) * kDim);
+        ip.o_ru8 = L.take(static_cast<size_t>(r_n) * kDim + 16);
+    }
+    if (ip.stage_f32) {
+        ip.o_qf = L.take(static_cast<size_t>(q_n) * kDim * 4);
+        ip.o_rf = L.take(static_cast<size_t>(r_n) * kDim * 4 + 16);
+    }
+    return SIFT_OK;
+}
+
+// Produces 16-byte aligned device u8 rows for both sides (arena A laid out by plan_inputs).
+int stage_inputs(DeviceCtx& c, char* A, const InputPlan& ip, int type, const void* q, const void* r, int q_n,
+                 int r_n, cudaStream_t st, const uint8_t*& qd, const uint8_t*& rd) {
+    if (type == SIFT_U8_DEVICE && !ip.stage_u8) {
+        qd = static_cast<const uint8_t*>(q);
+        rd = static_cast<const uint8_t*>(r);
+        return SIFT_OK;
+    }
+    if (ip.stage_u8) {
+        const cudaMemcpyKind k = type == SIFT_U8_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+        SIFT_CUDA(cudaMemcpyAsync(A + ip.o_qu8, q, static_cast<size_t>(q_n) * kDim, k, st));
+        if (r_n) SIFT_CUDA(cudaMemcpyAsync(A + ip.o_ru8, r, static_cast<size_t>(r_n) * kDim, k, st));
+        qd = reinterpret_cast<uint8_t*>(A + ip.o_qu8);
+        rd = reinterpret_cast<uint8_t*>(A + ip.o_ru8);
+        return SIFT_OK;
+    }
+    const void* q_src = ip.q_src;
+    const void* r_src = ip.r_src;
+    if (ip.stage_f32) {
+        SIFT_CUDA(cudaMemcpyAsync(A + ip.o_qf, q, static_cast<size_t>(q_n) * kDim * 4, cudaMemcpyHostToDevice, st));
+        if (r_n)
+            SIFT_CUDA(cudaMemcpyAsync(A + ip.o_rf, r, static_cast<size_t>(r_n) * kDim * 4, cudaMemcpyHostToDevice, st));
+        q_src = A + ip.o_qf;
+        r_src = A + ip.o_rf;
+    }
+    SIFT_CUDA(cudaMemsetAsync(c.d_status + 1, 0, sizeof(int), st));
+    uint8_t* qo = reinterpret_cast<uint8_t*>(A + ip.o_qu8);
+    uint8_t* ro = reinterpret_cast<uint8_t*>(A + ip.o_ru8);
+    g_launches += r_n > 0 ? 2 : 1;
+    if (type == SIFT_HALF_DEVICE) {
+        SIFT_CUDA(launch_pack_f16_u8(q_src, q_n, qo, c.d_status + 1, c.num_sms, st));
+        SIFT_CUDA(launch_pack_f16_u8(r_src, r_n, ro, c.d_status + 1, c.num_sms, st));
+    } else {
+        SIFT_CUDA(launch_pack_f32_u8(static_cast<const float*>(q_src), q_n, qo, c.d_status + 1, c.num_sms, st));
+        SIFT_CUDA(launch_pack_f32_u8(static_cast<const float*>(r_src), r_n, ro, c.d_status + 1, c.num_sms, st));
+    }
+    SIFT_CUDA(cudaMemcpyAsync(c.h_status + 1, c.d_status + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SIFT_CUDA(cudaStreamSynchronize(st));
+    if (c.h_status[1] != 0) return SIFT_ERR_NOT_INTEGER;
+    qd = qo;
+    rd = ro;
+    return SIFT_OK;
+}
+
 // Core of every exact entry point.
 int exact_match(const MatchArgs& a) {
     if (a.q_n > 0 && !a.q) return SIFT_ERR_INVALID_ARG;
@@ -178,42 +275,9 @@ int exact_match(const MatchArgs& a) {
     const bool d_dev = !a.nn_dist || is_device_accessible(a.nn_dist);
     const bool host_out = !(m_dev && s_dev && i_dev && d_dev);
 
-    // Input placement.
-    const uint8_t* qd = nullptr;
-    const uint8_t* rd = nullptr;
-    const void* q_src = a.q;
-    const void* r_src = a.r;
-    bool need_pack = a.type != SIFT_U8_DEVICE && a.type != SIFT_U8_HOST;
-    bool stage_u8 = a.type == SIFT_U8_HOST;
-    bool stage_f32 = false;
-    if (a.type == SIFT_U8_DEVICE) {
-        // TMA needs 16-byte aligned rows; unaligned device input is copied.
-        stage_u8 = (reinterpret_cast<uintptr_t>(a.q) & 15) || (reinterpret_cast<uintptr_t>(a.r) & 15);
-    }
-    if (a.type == SIFT_FLOAT_HOST) {
-        // Zero-copy like the reference (src/knn_brute.cu:58, :223) when the
-        // memory is mapped pinned memory; otherwise stage it.
-        void* qm = nullptr;
-        void* rm = nullptr;
-        if (cudaHostGetDevicePointer(&qm, const_cast<void*>(a.q), 0) == cudaSuccess &&
-            (r_n == 0 || cudaHostGetDevicePointer(&rm, const_cast<void*>(a.r), 0) == cudaSuccess) &&
-            !(reinterpret_cast<uintptr_t>(qm) & 15) && !(reinterpret_cast<uintptr_t>(rm) & 15)) {
-            q_src = qm;
-            r_src = rm;
-        } else {
-            cudaGetLastError();
-            stage_f32 = true;
-        }
-    }
-    if ((a.type == SIFT_FLOAT_DEVICE || a.type == SIFT_HALF_DEVICE) &&
-        ((reinterpret_cast<uintptr_t>(a.q) & 15) || (reinterpret_cast<uintptr_t>(a.r) & 15)))
-        return SIFT_ERR_INVALID_ARG;
-
     Layout L;
-    const size_t o_qu8 = (need_pack || stage_u8) ? L.take(static_cast<size_t>(q_n) * kDim) : 0;
-    const size_t o_ru8 = (need_pack || stage_u8) ? L.take(static_cast<size_t>(r_n) * kDim + 16) : 0;
-    const size_t o_qf = stage_f32 ? L.take(static_cast<size_t>(q_n) * kDim * 4) : 0;
-    const size_t o_rf = stage_f32 ? L.take(static_cast<size_t>(r_n) * kDim * 4 + 16) : 0;
+    InputPlan ip;
+    SIFT_TRY(plan_inputs(a.q, a.r, a.type, q_n, r_n, L, ip));
     const size_t o_brec = L.take(static_cast<size_t>(plan.base_tiles) * kRecInts * 4 + 16);
     const size_t o_qnorm = L.take(static_cast<size_t>(plan.q_pad) * 4);
     const size_t o_thr = L.take(static_cast<size_t>(plan.q_pad) * 4);
@@ -226,41 +290,9 @@ int exact_match(const MatchArgs& a) {
     char* A = c.arena;
 
     // ---- inputs
-    if (a.type == SIFT_U8_DEVICE && !stage_u8) {
-        qd = static_cast<const uint8_t*>(a.q);
-        rd = static_cast<const uint8_t*>(a.r);
-    } else if (stage_u8) {
-        const cudaMemcpyKind k = a.type == SIFT_U8_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
-        SIFT_CUDA(cudaMemcpyAsync(A + o_qu8, a.q, static_cast<size_t>(q_n) * kDim, k, st));
-        if (r_n) SIFT_CUDA(cudaMemcpyAsync(A + o_ru8, a.r, static_cast<size_t>(r_n) * kDim, k, st));
-        qd = reinterpret_cast<uint8_t*>(A + o_qu8);
-        rd = reinterpret_cast<uint8_t*>(A + o_ru8);
-    } else {
-        if (stage_f32) {
-            SIFT_CUDA(cudaMemcpyAsync(A + o_qf, a.q, static_cast<size_t>(q_n) * kDim * 4, cudaMemcpyHostToDevice, st));
-            if (r_n)
-                SIFT_CUDA(
-                    cudaMemcpyAsync(A + o_rf, a.r, static_cast<size_t>(r_n) * kDim * 4, cudaMemcpyHostToDevice, st));
-            q_src = A + o_qf;
-            r_src = A + o_rf;
-        }
-        SIFT_CUDA(cudaMemsetAsync(c.d_status + 1, 0, sizeof(int), st));
-        uint8_t* qo = reinterpret_cast<uint8_t*>(A + o_qu8);
-        uint8_t* ro = reinterpret_cast<uint8_t*>(A + o_ru8);
-        g_launches += r_n > 0 ? 2 : 1;
-        if (a.type == SIFT_HALF_DEVICE) {
-            SIFT_CUDA(launch_pack_f16_u8(q_src, q_n, qo, c.d_status + 1, c.num_sms, st));
-            SIFT_CUDA(launch_pack_f16_u8(r_src, r_n, ro, c.d_status + 1, c.num_sms, st));
-        } else {
-            SIFT_CUDA(launch_pack_f32_u8(static_cast<const float*>(q_src), q_n, qo, c.d_status + 1, c.num_sms, st));
-            SIFT_CUDA(launch_pack_f32_u8(static_cast<const float*>(r_src), r_n, ro, c.d_status + 1, c.num_sms, st));
-        }
-        SIFT_CUDA(cudaMemcpyAsync(c.h_status + 1, c.d_status + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-        SIFT_CUDA(cudaStreamSynchronize(st));
-        if (c.h_status[1] != 0) return SIFT_ERR_NOT_INTEGER;
-        qd = qo;
-        rd = ro;
-    }
+    const uint8_t* qd = nullptr;
+    const uint8_t* rd = nullptr;
+    SIFT_TRY(stage_inputs(c, A, ip, a.type, a.q, a.r, q_n, r_n, st, qd, rd));
 
     // ---- norms
     int32_t* brec = reinterpret_cast<int32_t*>(A + o_brec);
@@ -317,6 +349,134 @@ int exact_match(const MatchArgs& a) {
         return collect_device_status(c, st);
     }
     return SIFT_OK;
+}
+
+
+// Hyperplane rows are int8: dims {128, rows}, box {128, box_rows}.
+int encode_i8_rows(CUtensorMap* m, const void* base, uint64_t rows, uint32_t box_rows) {
+    return encode_u8_rows(m, base, rows, box_rows);
+}
+
+int lsh_match(const LshArgs& a) {
+    if (a.L < 1 || a.k < 1 || a.k > 32 || a.L * a.k > kLshMaxPlanes || !a.planes) return SIFT_ERR_INVALID_ARG;
+    if (a.q_n > 0x7fffffffu / 32 || a.r_n > 0x7fffffffu / 32) return SIFT_ERR_INVALID_ARG;
+    DeviceCtx* cp = nullptr;
+    int dev = 0;
+    SIFT_TRY(ensure_ready(cp, dev));
+    DeviceCtx& c = *cp;
+    std::lock_guard<std::mutex> lk(c.mu);
+    cudaStream_t st = static_cast<cudaStream_t>(a.stream);
+    const int q_n = static_cast<int>(a.q_n), r_n = static_cast<int>(a.r_n);
+    if (q_n == 0) return SIFT_OK;
+    const int L_ = a.L, k = a.k, P = lsh_planes_padded(L_, k);
+    const int top = k < kLshMaxTopBits ? k : kLshMaxTopBits;
+    const int shift = k - top, nbins = 1 << top;
+    const int r_pad = ((r_n + 127) / 128) * 128, q_pad = ((q_n + 127) / 128) * 128;
+
+    const bool m_dev = !a.matches || is_device_accessible(a.matches);
+    const bool i_dev = !a.nn_idx || is_device_accessible(a.nn_idx);
+    const bool d_dev = !a.nn_dist || is_device_accessible(a.nn_dist);
+    const bool host_out = !(m_dev && i_dev && d_dev);
+    const bool planes_dev = is_device_accessible(a.planes) && !(reinterpret_cast<uintptr_t>(a.planes) & 15);
+
+    Layout L;
+    InputPlan ip;
+    SIFT_TRY(plan_inputs(a.q, a.r, a.type, q_n, r_n, L, ip));
+    const size_t o_pl = planes_dev ? 0 : L.take(static_cast<size_t>(L_) * k * kDim);
+    const size_t o_cr = L.take(static_cast<size_t>(L_) * r_n * 4 + 16);
+    const size_t o_cq = L.take(static_cast<size_t>(L_) * q_n * 4);
+    const size_t o_hist = L.take(static_cast<size_t>(L_) * nbins * 4);
+    const size_t o_start = L.take(static_cast<size_t>(L_) * (nbins + 1) * 4);
+    const size_t o_order = L.take(static_cast<size_t>(L_) * r_n * 4 + 16);
+    const size_t o_ocode = L.take(static_cast<size_t>(L_) * r_n * 4 + 16);
+    const size_t o_qn = L.take(static_cast<size_t>(q_pad) * 4);
+    const size_t o_rn = L.take(static_cast<size_t>(r_pad) * 4 + 16);
+    const size_t o_m = (a.matches && !m_dev) ? L.take(static_cast<size_t>(q_n) * 4) : 0;
+    const size_t o_i = (a.nn_idx && !i_dev) ? L.take(static_cast<size_t>(q_n) * 8) : 0;
+    const size_t o_d = (a.nn_dist && !d_dev) ? L.take(static_cast<size_t>(q_n) * 8) : 0;
+    SIFT_TRY(ensure_arena(c, L.off));
+    char* A = c.arena;
+
+    const uint8_t* qd = nullptr;
+    const uint8_t* rd = nullptr;
+    SIFT_TRY(stage_inputs(c, A, ip, a.type, a.q, a.r, q_n, r_n, st, qd, rd));
+    const int8_t* pl = a.planes;
+    if (!planes_dev) {
+        SIFT_CUDA(cudaMemcpyAsync(A + o_pl, a.planes, static_cast<size_t>(L_) * k * kDim, cudaMemcpyDefault, st));
+        pl = reinterpret_cast<const int8_t*>(A + o_pl);
+    }
+    uint32_t* codes_r = reinterpret_cast<uint32_t*>(A + o_cr);
+    uint32_t* codes_q = reinterpret_cast<uint32_t*>(A + o_cq);
+    int* hist = reinterpret_cast<int*>(A + o_hist);
+    int* start = reinterpret_cast<int*>(A + o_start);
+    int* order = reinterpret_cast<int*>(A + o_order);
+    uint32_t* ocode = reinterpret_cast<uint32_t*>(A + o_ocode);
+    int32_t* qnorm = reinterpret_cast<int32_t*>(A + o_qn);
+    int32_t* rnorm = reinterpret_cast<int32_t*>(A + o_rn);
+
+    SIFT_CUDA(launch_row_norms_u8(rd, r_n, r_pad, kMetricL2, rnorm, nullptr, nullptr, st));
+    SIFT_CUDA(launch_row_norms_u8(qd, q_n, q_pad, kMetricL2, qnorm, nullptr, nullptr, st));
+    g_launches += (r_pad > 0 ? 1 : 0) + 1;
+    CUtensorMap pmap, qmap, rmap;
+    SIFT_TRY(encode_i8_rows(&pmap, pl, static_cast<uint64_t>(L_) * k, static_cast<uint32_t>(P)));
+    SIFT_TRY(encode_u8_rows(&qmap, qd, q_n, 128));
+    if (r_n > 0) {
+        SIFT_TRY(encode_u8_rows(&rmap, rd, r_n, 128));
+        SIFT_CUDA(launch_lsh_hash(rmap, pmap, r_n, P, L_, k, codes_r, c.d_status, c.num_sms, st));
+        ++g_launches;
+    }
+    SIFT_CUDA(launch_lsh_hash(qmap, pmap, q_n, P, L_, k, codes_q, c.d_status, c.num_sms, st));
+    SIFT_CUDA(launch_lsh_buckets(codes_r, r_n, L_, shift, nbins, hist, start, order, ocode, c.num_sms, st));
+    uint32_t* m_out = (a.matches && !m_dev) ? reinterpret_cast<uint32_t*>(A + o_m) : a.matches;
+    int32_t* i_out = (a.nn_idx && !i_dev) ? reinterpret_cast<int32_t*>(A + o_i) : a.nn_idx;
+    float* d_out = (a.nn_dist && !d_dev) ? reinterpret_cast<float*>(A + o_d) : a.nn_dist;
+    SIFT_CUDA(launch_lsh_scan(qd, rd, q_n, r_n, L_, shift, nbins, codes_q, start, order, ocode, qnorm, rnorm,
+                              a.threshold, a.ratio ? 1 : 0, m_out, i_out, d_out, st));
+    g_launches += 1 + (r_n > 0 ? 3 : 0) + 1;
+    if (a.matches && !m_dev)
+        SIFT_CUDA(cudaMemcpyAsync(a.matches, m_out, static_cast<size_t>(q_n) * 4, cudaMemcpyDeviceToHost, st));
+    if (a.nn_idx && !i_dev)
+        SIFT_CUDA(cudaMemcpyAsync(a.nn_idx, i_out, static_cast<size_t>(q_n) * 8, cudaMemcpyDeviceToHost, st));
+    if (a.nn_dist && !d_dev)
+        SIFT_CUDA(cudaMemcpyAsync(a.nn_dist, d_out, static_cast<size_t>(q_n) * 8, cudaMemcpyDeviceToHost, st));
+    const bool host_in = a.type == SIFT_U8_HOST || a.type == SIFT_FLOAT_HOST || !planes_dev;
+    if (a.sync || host_out || host_in) {
+        SIFT_CUDA(cudaStreamSynchronize(st));
+        return collect_device_status(c, st);
+    }
+    return SIFT_OK;
+}
+
+int lsh_hash(const uint8_t* x, uint32_t n, const int8_t* planes, int L_, int k, uint32_t* codes, void* stream) {
+    if (L_ < 1 || k < 1 || k > 32 || L_ * k > kLshMaxPlanes || !planes || (n && (!x || !codes)))
+        return SIFT_ERR_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(x) & 15) || (reinterpret_cast<uintptr_t>(planes) & 15) ||
+        !is_device_accessible(planes) || (n && !is_device_accessible(x)) || (n && !is_device_accessible(codes)))
+        return SIFT_ERR_INVALID_ARG;
+    DeviceCtx* cp = nullptr;
+    int dev = 0;
+    SIFT_TRY(ensure_ready(cp, dev));
+    std::lock_guard<std::mutex> lk(cp->mu);
+    if (n == 0) return SIFT_OK;
+    const int P = lsh_planes_padded(L_, k);
+    CUtensorMap pmap, xmap;
+    SIFT_TRY(encode_i8_rows(&pmap, planes, static_cast<uint64_t>(L_) * k, static_cast<uint32_t>(P)));
+    SIFT_TRY(encode_u8_rows(&xmap, x, n, 128));
+    SIFT_CUDA(launch_lsh_hash(xmap, pmap, static_cast<int>(n), P, L_, k, codes, cp->d_status, cp->num_sms,
+                              static_cast<cudaStream_t>(stream)));
+    ++g_launches;
+    return SIFT_OK;
+}
+
+// The reference draws each hyperplane component as +1 / -1 from the C
+// library's rand() (make_vector_h_sum_1, src/lsh_h.cu:61-83), nbits planes per
+// table in table order (make_vec_h, src/lsh_h.cu:89-100).
+void reference_planes(int L_, int nbits, int8_t* out) {
+    for (int t = 0; t < L_; ++t)
+        for (int j = 0; j < nbits; ++j)
+            for (int d = 0; d < kDim; ++d)
+                out[(static_cast<size_t>(t) * nbits + j) * kDim + d] =
+                    ((static_cast<float>(rand()) / static_cast<float>(RAND_MAX)) - 0.5f) >= 0 ? 1 : -1;
 }
 
 int stream_status(void* stream) {
@@ -430,6 +590,39 @@ int sift2nn_match(const void* q, const void* r, int type, uint32_t q_n, uint32_t
 }
 
 int sift_stream_status(void* stream) { return sift::stream_status(stream); }
+
+int sift_lsh_hash(const uint8_t* x, uint32_t n, const int8_t* planes, int L, int k, uint32_t* codes, void* stream) {
+    return sift::lsh_hash(x, n, planes, L, k, codes, stream);
+}
+
+int sift_lsh_match(const void* q, const void* r, int type, uint32_t q_n, uint32_t r_n, const int8_t* planes, int L,
+                   int k, float threshold, uint32_t* matches, int32_t* nn_idx, float* nn_dist, void* stream) {
+    sift::LshArgs a{};
+    a.q = q; a.r = r; a.type = type; a.q_n = q_n; a.r_n = r_n; a.planes = planes; a.L = L; a.k = k;
+    a.threshold = threshold; a.ratio = threshold > 0.0f; a.matches = matches; a.nn_idx = nn_idx; a.nn_dist = nn_dist;
+    a.stream = stream; a.sync = false;
+    return sift::lsh_match(a);
+}
+
+int sift_impl_lsh_gpu(void* q_points, void* r_points, int type, uint32_t q_n, uint32_t r_n, uint32_t* matches, int l,
+                      int nbits) {
+    if (l < 1 || nbits < 1 || nbits > 32 || l * nbits > sift::kLshMaxPlanes || (q_n && !matches))
+        return SIFT_ERR_INVALID_ARG;
+    int8_t* planes = static_cast<int8_t*>(malloc(static_cast<size_t>(l) * nbits * sift::kDim));
+    if (!planes) return SIFT_ERR_ALLOC;
+    sift::reference_planes(l, nbits, planes);
+    sift::LshArgs a{};
+    a.q = q_points; a.r = r_points; a.type = type; a.q_n = q_n; a.r_n = r_n; a.planes = planes; a.L = l;
+    a.k = nbits; a.threshold = 0.0f; a.ratio = false; a.matches = matches; a.sync = true;
+    const int rc = sift::lsh_match(a);
+    free(planes);
+    return rc;
+}
+
+int lsh_gpu(void* q_points, void* r_points, int type, uint32_t q_n, uint32_t r_n, uint32_t* matches, float,
+            cublasHandle_t, int, int l, int, int nbits) {
+    return sift_impl_lsh_gpu(q_points, r_points, type, q_n, r_n, matches, l, nbits);
+}
 
 const char* sift_status_string(int s) {
     switch (s) {

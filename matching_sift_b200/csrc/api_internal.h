@@ -21,6 +21,25 @@ struct MatchArgs {
 };
 
 int exact_match(const MatchArgs& a);
+
+struct LshArgs {
+    const void* q = nullptr;
+    const void* r = nullptr;
+    int type = SIFT_U8_DEVICE;
+    uint32_t q_n = 0, r_n = 0;
+    const int8_t* planes = nullptr;  // [L][k][128] int8, host or device
+    int L = 1, k = 16;
+    float threshold = 0.8f;
+    bool ratio = false;  // apply the ratio test to `matches`
+    uint32_t* matches = nullptr;
+    int32_t* nn_idx = nullptr;
+    float* nn_dist = nullptr;
+    void* stream = nullptr;
+    bool sync = false;
+};
+int lsh_match(const LshArgs& a);
+int lsh_hash(const uint8_t* x, uint32_t n, const int8_t* planes, int L, int k, uint32_t* codes, void* stream);
+void reference_planes(int L, int nbits, int8_t* out);
 int stream_status(void* stream);
 void set_last_status(int s);
 int profile_collect(double* total_ms, int* launches);
@@ -38,4 +57,6 @@ int sift_impl_cublas_2nn_sift(void* q_points, void* r_points, int type, uint32_t
 void sift_impl_cublas_2nn_f(void* q_points, void* r_points, int q_n, int r_n, void* sorted);
 void sift_impl_device_brute(void* q_points, void* r_points, int q_n, int r_n, void* sorted);
 void sift_impl_host_brute(void* q_points, void* r_points, int q_n, int r_n, void* sorted);
+int sift_impl_lsh_gpu(void* q_points, void* r_points, int type, uint32_t q_n, uint32_t r_n, uint32_t* matches, int l,
+                      int nbits);
 }

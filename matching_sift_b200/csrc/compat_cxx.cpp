@@ -19,6 +19,8 @@ int sift_impl_cublas_2nn_sift(void* q_points, void* r_points, int type, uint32_t
 void sift_impl_cublas_2nn_f(void* q_points, void* r_points, int q_n, int r_n, void* sorted);
 void sift_impl_device_brute(void* q_points, void* r_points, int q_n, int r_n, void* sorted);
 void sift_impl_host_brute(void* q_points, void* r_points, int q_n, int r_n, void* sorted);
+int sift_impl_lsh_gpu(void* q_points, void* r_points, int type, uint32_t q_n, uint32_t r_n, uint32_t* matches, int l,
+                      int nbits);
 }
 
 // include/knn_brute.h:22
@@ -40,4 +42,10 @@ SIFT_CXX_API void device_brute(des_t_f* q_points, des_t_f* r_points, int q_n, in
 // include/knn_brute.h:29
 SIFT_CXX_API void host_brute(des_t_f* q_points, des_t_f* r_points, int q_points_size, int r_points_size, float4* sorted) {
     sift_impl_host_brute(q_points, r_points, q_points_size, r_points_size, sorted);
+}
+
+// include/lsh_h.h:69
+SIFT_CXX_API int lsh_gpu(void* q_points, void* r_points, int type, uint32_t q_n, uint32_t r_n, uint32_t* matches,
+                         float, cublasHandle_t, int, int l, int, int nbits) {
+    return sift_impl_lsh_gpu(q_points, r_points, type, q_n, r_n, matches, l, nbits);
 }

@@ -72,6 +72,15 @@ def make_hyperplanes(nbits: int, n_tables: int = 1, seed: int = 0) -> np.ndarray
     return rng.standard_normal((n_tables, nbits, DIM)).astype(np.float32)
 
 
+def quantize_planes(planes: np.ndarray, scale: float = 32.0) -> np.ndarray:
+    """int8 hyperplanes: rint(planes * scale) clamped to [-127, 127].
+
+    The LSH kernels compute exact integer dot products (u8 x s8 on the tensor
+    cores), so hyperplanes are used in this quantised form everywhere.
+    """
+    return np.clip(np.rint(planes * scale), -127, 127).astype(np.int8)
+
+
 def make_pairs(n_pairs: int, lo: int = 500, hi: int = 8000, seed: int = 0, overlap: float = 0.4):
     """Image pairs with uneven keypoint counts (log-uniform in [lo, hi]).
 
