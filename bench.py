@@ -168,6 +168,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true", help="time only the device-resident path")
     ap.add_argument("--queries", type=int, default=Q_N, help="queries per GPU (profiling of smaller cases)")
+    ap.add_argument("--no-variants", action="store_true", help="skip the FP16 leg")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -238,6 +239,13 @@ def main():
     step_ms = float(sum(a.elapsed_time(b) for a, b in ev))
     kernel_ms = kt.value / max(kn.value, 1)
 
+    # ---- the same search on FP16 rows (kind::f16 kernel), device-resident
+    variants = {}
+    if not args.no_variants:
+        variants["fp16"] = fp16_leg(args, lib, ms, torch, qd, rd, flush, stream, q_n)
+        if not torch.equal(variants["fp16"].pop("nn_idx"), nn_idx):
+            raise RuntimeError("FP16 and u8 kernels disagree")
+
     # ---- end to end through the C ABI with host buffers
     e2e_ms = float("nan")
     if not args.skip_e2e:
@@ -266,10 +274,15 @@ def main():
         np.testing.assert_array_equal(mh.numpy(), matches.cpu().numpy())
 
     # ---- max over ranks
-    t = torch.tensor([step_ms, e2e_ms, kernel_ms], dtype=torch.float64, device=dev)
+    vkeys = sorted(variants)
+    t = torch.tensor([step_ms, e2e_ms, kernel_ms] + [variants[k][f] for k in vkeys for f in ("step_ms", "kernel_ms")],
+                     dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    step_ms, e2e_ms, kernel_ms = t.tolist()
+    vals = t.tolist()
+    step_ms, e2e_ms, kernel_ms = vals[:3]
+    for n, k in enumerate(vkeys):
+        variants[k]["step_ms"], variants[k]["kernel_ms"] = vals[3 + 2 * n], vals[4 + 2 * n]
 
     if rank == 0:
         peaks, peak_src = _peaks()
@@ -312,6 +325,20 @@ def main():
                          "frac_of_2x_bf16_" + peak_src: round(achieved / bf16x2, 4)},
             "clocks": clocks.summary(),
         }
+        if "fp16" in variants:
+            v = variants["fp16"]
+            f16_peak = peaks["bf16_tflops"]
+            ach = ops / (v["kernel_ms"] * 1e-3) / 1e12
+            line["variants"] = {"fp16": {
+                "value": round(world * q_n * v["steps"] / (v["step_ms"] * 1e-3), 1), "unit": "queries/s",
+                "ms_per_step": round(v["step_ms"] / v["steps"], 4), "steps": v["steps"], "dtype": "f16",
+                "call": "sift2nn_match(type=SIFT_HALF_DEVICE): FP16 rows searched in place by "
+                        "exact2nn_f16_pair_kernel (kind::f16, f32 accumulation), same results as u8",
+                "roofline": {"bound": "tensor", "kernel": "exact2nn_f16_pair_kernel", "achieved": round(ach, 1),
+                             "peak": round(f16_peak, 1), "unit": "TFLOP/s", "frac": round(ach / f16_peak, 4),
+                             "kernel_ms": round(v["kernel_ms"], 4),
+                             "peak_note": f"dense bf16 cuBLAS ({peak_src}), the same tensor rate as f16"},
+                "gpu_launches": v["launches"], "clocks": v["clocks"]}}
         if not args.no_cpu_baseline:
             rate, sample, threads, kind = cpu_reference_rate(queries, base, 15.0)
             line["cpu_baseline"] = {"value": round(rate, 2), "unit": "queries/s", "cores": threads, "kind": kind,
@@ -320,6 +347,48 @@ def main():
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def fp16_leg(args, lib, ms, torch, qd, rd, flush, stream, q_n):
+    """Device-resident timing of the FP16 kernel on the same rows as half."""
+    import ctypes
+
+    qh = qd.to(torch.float16)
+    rh = rd.to(torch.float16)
+    matches = torch.empty(q_n, dtype=torch.int32, device=qd.device)
+    nn_idx = torch.empty((q_n, 2), dtype=torch.int32, device=qd.device)
+    nn_dist = torch.empty((q_n, 2), dtype=torch.float32, device=qd.device)
+
+    def step():
+        rc = lib.sift2nn_match(qh.data_ptr(), rh.data_ptr(), ms.HALF_DEVICE, q_n, R_N, ms.METRIC_L2, THRESHOLD,
+                               matches.data_ptr(), None, nn_idx.data_ptr(), nn_dist.data_ptr(), stream.cuda_stream)
+        if rc != 0:
+            raise ms.SiftError(rc, "sift2nn_match (FP16)")
+
+    steps = max(3, args.steps // 2)
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    launches0 = lib.sift_launch_count()
+    lib.sift_profile_enable(1)
+    with ClockSampler(qd.device.index or 0) as clocks:
+        for k in range(steps):
+            flush.fill_(k)
+            ev[k][0].record(stream)
+            step()
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+    lib.sift_profile_enable(0)
+    launches = lib.sift_launch_count() - launches0
+    kt, kn = ctypes.c_double(0.0), ctypes.c_int(0)
+    lib.sift_profile_collect(ctypes.byref(kt), ctypes.byref(kn))
+    if ms.stream_status(stream.cuda_stream) != 0:
+        raise RuntimeError("device status after FP16 steps")
+    del qh, rh
+    return {"step_ms": float(sum(a.elapsed_time(b) for a, b in ev)), "kernel_ms": kt.value / max(kn.value, 1),
+            "steps": steps, "launches": int(launches), "clocks": clocks.summary(),
+            "nn_idx": nn_idx}
 
 
 def reference_arm(args, world, rank):

@@ -130,10 +130,18 @@ SIFT_API int sift_last_status(void);
      sorted[q_n]     {d1, d2, i1, i2} as floats, FLT_MAX where absent
      nn_idx[2*q_n]   int32 nearest / second indices, -1 where absent
      nn_dist[2*q_n]  float distances under `metric`, FLT_MAX where absent
-   stream: a cudaStream_t (NULL = legacy default stream). With device inputs
-   and device outputs the call is asynchronous on `stream`; device-side
-   problems are then reported by sift_stream_status(stream). Any host input or
-   host output makes the call synchronous. */
+   Float and half values must be integers in [0, 255] times one common power
+   of two 2^-s, s <= 24 (raw SIFT components, or the reference benchmark's
+   components / 512, src/test.cu:99-103); distances are then in the caller's
+   units (the integer results times 2^-2s), else SIFT_ERR_NOT_INTEGER.
+   SIFT_HALF_DEVICE rows are searched in place by the FP16 tensor-core kernel
+   (kind::f16, f32 accumulation, exact for such values); float rows are packed
+   to u8 for the u8 kernel.
+   stream: a cudaStream_t (NULL = legacy default stream). With u8 device
+   inputs and device outputs the call is asynchronous on `stream`; device-side
+   problems are then reported by sift_stream_status(stream). Float / half
+   inputs synchronise once (value check); any host input or host output makes
+   the call synchronous. */
 SIFT_API int sift2nn_match(const void* q, const void* r, int type, uint32_t q_n, uint32_t r_n, int metric, float threshold,
                   uint32_t* matches, sift_float4* sorted, int32_t* nn_idx, float* nn_dist, void* stream);
 
@@ -198,8 +206,9 @@ SIFT_API void sift_profile_enable(int on);
 SIFT_API int sift_profile_collect(double* total_ms, int* launches);
 
 /* Selects the exact-search kernel for subsequent calls in this process:
-   0 (default) the CTA-pair kernel (tcgen05 cta_group::2), 1 the single-CTA
-   kernel. Both return identical results. */
+   0 (default) the CTA-pair kernels (tcgen05 cta_group::2; half inputs go to
+   the FP16 kernel), 1 the single-CTA u8 kernel, 2 the CTA-pair u8 kernel for
+   every input type (half inputs packed to u8). All return identical results. */
 SIFT_API int sift_set_kernel_variant(int variant);
 
 #ifdef __cplusplus

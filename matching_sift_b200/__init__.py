@@ -84,17 +84,22 @@ def stream_status(stream=None) -> int:
 # -------------------------------------------------------- native interface --
 
 def match(q, r, threshold: float = 0.8, metric: int = METRIC_L2, stream=None, outputs=("matches", "nn_idx", "nn_dist")):
-    """Exact 2-NN of torch uint8 CUDA tensors q [n, 128] and r [m, 128].
+    """Exact 2-NN of CUDA tensors q [n, 128] and r [m, 128].
 
+    uint8 rows are searched by the u8 tensor-core kernel; float16 rows by the
+    FP16 kernel in place; float32 rows are packed to u8 first. Float values
+    must be integers in [0, 255] times one common power of two.
     Returns a dict with the requested outputs as CUDA tensors: ``matches``
     (int64 view of uint32; UINT32_MAX where the ratio test fails), ``nn_idx``
     [n, 2] int32 (-1 absent), ``nn_dist`` [n, 2] float32, ``sorted`` [n, 4].
-    Asynchronous on ``stream`` (a torch.cuda.Stream or None for the current one).
+    Asynchronous on ``stream`` (a torch.cuda.Stream or None for the current one)
+    for uint8 inputs; float inputs synchronise once to validate the values.
     """
     import torch
 
-    if q.dtype != torch.uint8 or r.dtype != torch.uint8 or not q.is_cuda or not r.is_cuda:
-        raise TypeError("match() expects uint8 CUDA tensors")
+    types = {torch.uint8: U8_DEVICE, torch.float16: HALF_DEVICE, torch.float32: FLOAT_DEVICE}
+    if q.dtype != r.dtype or q.dtype not in types or not q.is_cuda or not r.is_cuda:
+        raise TypeError("match() expects two CUDA tensors of one dtype: uint8, float16 or float32")
     if q.dim() != 2 or q.shape[1] != 128 or r.dim() != 2 or r.shape[1] != 128:
         raise ValueError("descriptors must be [n, 128]")
     q = q.contiguous()
@@ -112,7 +117,7 @@ def match(q, r, threshold: float = 0.8, metric: int = METRIC_L2, stream=None, ou
         out["sorted"] = torch.empty((n, 4), dtype=torch.float32, device=dev)
     s = stream if stream is not None else torch.cuda.current_stream(dev)
     with torch.cuda.device(dev):
-        rc = lib().sift2nn_match(q.data_ptr(), r.data_ptr(), U8_DEVICE, n, r.shape[0], metric, threshold,
+        rc = lib().sift2nn_match(q.data_ptr(), r.data_ptr(), types[q.dtype], n, r.shape[0], metric, threshold,
                                  _ptr(out.get("matches")), _ptr(out.get("sorted")), _ptr(out.get("nn_idx")),
                                  _ptr(out.get("nn_dist")), s.cuda_stream)
     check(rc, "sift2nn_match")

@@ -2,6 +2,7 @@
 // input staging, TMA descriptor construction and the launch sequence
 //   [pack f32/f16 -> u8] -> row norms -> exact2nn (tcgen05) -> merge.
 #include <cfloat>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <atomic>
@@ -22,6 +23,8 @@ namespace sift {
 namespace {
 
 constexpr int kMaxDevices = 64;
+// Largest power-of-two scale 2^-s of descriptor values the exact kernels take.
+constexpr int kMaxShift = 24;
 
 struct DeviceCtx {
     std::mutex mu;
@@ -29,7 +32,7 @@ struct DeviceCtx {
     int num_sms = 0;
     char* arena = nullptr;
     size_t arena_bytes = 0;
-    int* d_status = nullptr;  // [0] device error code, [1] pack flag
+    int* d_status = nullptr;  // [0] device error code, [1] pack flag / value stats [1..3]
     int* h_status = nullptr;  // pinned mirror of d_status
 };
 
@@ -38,7 +41,9 @@ std::mutex g_init_mu;
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 thread_local int t_last_status = SIFT_OK;
 std::atomic<long long> g_launches{0};
-std::atomic<int> g_variant{0};  // 0: CTA-pair kernel, 1: single-CTA kernel
+// 0: CTA-pair kernels (half inputs searched by the FP16 kernel),
+// 1: single-CTA u8 kernel, 2: CTA-pair u8 kernel for every input type.
+std::atomic<int> g_variant{0};
 std::atomic<bool> g_profile{false};
 std::mutex g_prof_mu;
 std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_prof_events;
@@ -126,6 +131,19 @@ int encode_u8_rows(CUtensorMap* m, const void* base, uint64_t rows, uint32_t box
     return r == CUDA_SUCCESS ? SIFT_OK : SIFT_ERR_CUDA;
 }
 
+// FP16 rows of 128 halves (256 B): dims {128, rows}, box {64, box_rows} (one
+// 128-byte K block per load, the widest SWIZZLE_128B box).
+int encode_f16_rows(CUtensorMap* m, const void* base, uint64_t rows, uint32_t box_rows) {
+    cuuint64_t dims[2] = {static_cast<cuuint64_t>(kDim), static_cast<cuuint64_t>(rows)};
+    cuuint64_t strides[1] = {static_cast<cuuint64_t>(kDim) * 2};
+    cuuint32_t box[2] = {static_cast<cuuint32_t>(kDim / 2), box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? SIFT_OK : SIFT_ERR_CUDA;
+}
+
 int map_cuda(cudaError_t e) {
     if (e == cudaSuccess) return SIFT_OK;
     if (e == cudaErrorMemoryAllocation) return SIFT_ERR_ALLOC;
@@ -154,6 +172,23 @@ int collect_device_status(DeviceCtx& c, cudaStream_t st) {
 
 }  // namespace
 
+// Largest power-of-two shift needed to make every q and r value (float or
+// half, device-readable) an integer, checked to keep them in [0, 255].
+int common_shift(DeviceCtx& c, const void* q, const void* r, bool half, int q_n, int r_n, cudaStream_t st,
+                 int& shift) {
+    SIFT_CUDA(cudaMemsetAsync(c.d_status + 1, 0, 3 * sizeof(int), st));
+    SIFT_CUDA(launch_value_stats(q, half, q_n, c.d_status + 1, c.num_sms, st));
+    SIFT_CUDA(launch_value_stats(r, half, r_n, c.d_status + 1, c.num_sms, st));
+    SIFT_CUDA(cudaMemcpyAsync(c.h_status + 1, c.d_status + 1, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    SIFT_CUDA(cudaStreamSynchronize(st));
+    const int bad = c.h_status[1], s = c.h_status[2];
+    float mx = 0.0f;
+    std::memcpy(&mx, &c.h_status[3], sizeof(float));
+    if (bad || s > kMaxShift || ldexpf(mx, s) > 255.0f) return SIFT_ERR_NOT_INTEGER;
+    shift = s;
+    return SIFT_OK;
+}
+
 // Where the u8 descriptors a kernel reads come from, for every memory type.
 struct InputPlan {
     const void* q_src = nullptr;
@@ -164,9 +199,13 @@ struct InputPlan {
     size_t o_qu8 = 0, o_ru8 = 0, o_qf = 0, o_rf = 0;
 };
 
+// type -1: FP16 device rows read in place by the FP16 kernel (checked only).
 int plan_inputs(const void* q, const void* r, int type, int q_n, int r_n, Layout& L, InputPlan& ip) {
     if (q_n > 0 && !q) return SIFT_ERR_INVALID_ARG;
     if (r_n > 0 && !r) return SIFT_ERR_INVALID_ARG;
+    if (type == -1)
+        return ((reinterpret_cast<uintptr_t>(q) & 15) || (reinterpret_cast<uintptr_t>(r) & 15)) ? SIFT_ERR_INVALID_ARG
+                                                                                                : SIFT_OK;
     if (type < SIFT_FLOAT_HOST || type > SIFT_U8_HOST) return SIFT_ERR_INVALID_ARG;
     ip.q_src = q;
     ip.r_src = r;
@@ -206,8 +245,11 @@ int plan_inputs(const void* q, const void* r, int type, int q_n, int r_n, Layout
 }
 
 // Produces 16-byte aligned device u8 rows for both sides (arena A laid out by plan_inputs).
+// shift: the inputs were integers times 2^-shift (0 for integer inputs); the
+// u8 rows hold the integers, so distances scale by 2^(-2 shift).
 int stage_inputs(DeviceCtx& c, char* A, const InputPlan& ip, int type, const void* q, const void* r, int q_n,
-                 int r_n, cudaStream_t st, const uint8_t*& qd, const uint8_t*& rd) {
+                 int r_n, cudaStream_t st, const uint8_t*& qd, const uint8_t*& rd, int& shift) {
+    shift = 0;
     if (type == SIFT_U8_DEVICE && !ip.stage_u8) {
         qd = static_cast<const uint8_t*>(q);
         rd = static_cast<const uint8_t*>(r);
@@ -234,16 +276,28 @@ int stage_inputs(DeviceCtx& c, char* A, const InputPlan& ip, int type, const voi
     uint8_t* qo = reinterpret_cast<uint8_t*>(A + ip.o_qu8);
     uint8_t* ro = reinterpret_cast<uint8_t*>(A + ip.o_ru8);
     g_launches += r_n > 0 ? 2 : 1;
-    if (type == SIFT_HALF_DEVICE) {
-        SIFT_CUDA(launch_pack_f16_u8(q_src, q_n, qo, c.d_status + 1, c.num_sms, st));
-        SIFT_CUDA(launch_pack_f16_u8(r_src, r_n, ro, c.d_status + 1, c.num_sms, st));
-    } else {
-        SIFT_CUDA(launch_pack_f32_u8(static_cast<const float*>(q_src), q_n, qo, c.d_status + 1, c.num_sms, st));
-        SIFT_CUDA(launch_pack_f32_u8(static_cast<const float*>(r_src), r_n, ro, c.d_status + 1, c.num_sms, st));
+    const bool half = type == SIFT_HALF_DEVICE;
+    auto pack = [&](float mul) -> int {
+        SIFT_CUDA(cudaMemsetAsync(c.d_status + 1, 0, sizeof(int), st));
+        if (half) {
+            SIFT_CUDA(launch_pack_f16_u8(q_src, q_n, mul, qo, c.d_status + 1, c.num_sms, st));
+            SIFT_CUDA(launch_pack_f16_u8(r_src, r_n, mul, ro, c.d_status + 1, c.num_sms, st));
+        } else {
+            SIFT_CUDA(launch_pack_f32_u8(static_cast<const float*>(q_src), q_n, mul, qo, c.d_status + 1, c.num_sms, st));
+            SIFT_CUDA(launch_pack_f32_u8(static_cast<const float*>(r_src), r_n, mul, ro, c.d_status + 1, c.num_sms, st));
+        }
+        SIFT_CUDA(cudaMemcpyAsync(c.h_status + 1, c.d_status + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+        SIFT_CUDA(cudaStreamSynchronize(st));
+        return c.h_status[1] != 0 ? SIFT_ERR_NOT_INTEGER : SIFT_OK;
+    };
+    if (pack(1.0f) != SIFT_OK) {
+        // Not plain integers: look for one power-of-two scale of all values.
+        int s = 0;
+        SIFT_TRY(common_shift(c, q_src, r_src, half, q_n, r_n, st, s));
+        g_launches += 2;
+        SIFT_TRY(pack(ldexpf(1.0f, s)));
+        shift = s;
     }
-    SIFT_CUDA(cudaMemcpyAsync(c.h_status + 1, c.d_status + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-    SIFT_CUDA(cudaStreamSynchronize(st));
-    if (c.h_status[1] != 0) return SIFT_ERR_NOT_INTEGER;
     qd = qo;
     rd = ro;
     return SIFT_OK;
@@ -265,7 +319,10 @@ int exact_match(const MatchArgs& a) {
     const int q_n = static_cast<int>(a.q_n), r_n = static_cast<int>(a.r_n);
     if (q_n == 0) return SIFT_OK;
 
-    const bool use_pair = g_variant.load() == 0;
+    const int variant = g_variant.load();
+    const bool use_pair = variant != 1;
+    // Half inputs are searched as FP16 by the FP16 tensor-core kernel in place.
+    const bool use_f16 = variant == 0 && a.type == SIFT_HALF_DEVICE;
     const ExactPlan plan = use_pair ? make_exact_plan(q_n, r_n, c.num_sms / 2, 2) : make_exact_plan(q_n, r_n, c.num_sms, 1);
 
     // Output placement: direct when the device can write the pointer, else staged.
@@ -277,7 +334,7 @@ int exact_match(const MatchArgs& a) {
 
     Layout L;
     InputPlan ip;
-    SIFT_TRY(plan_inputs(a.q, a.r, a.type, q_n, r_n, L, ip));
+    SIFT_TRY(plan_inputs(a.q, a.r, use_f16 ? -1 : a.type, q_n, r_n, L, ip));
     const size_t o_brec = L.take(static_cast<size_t>(plan.base_tiles) * kRecInts * 4 + 16);
     const size_t o_qnorm = L.take(static_cast<size_t>(plan.q_pad) * 4);
     const size_t o_thr = L.take(static_cast<size_t>(plan.q_pad) * 4);
@@ -289,25 +346,43 @@ int exact_match(const MatchArgs& a) {
     SIFT_TRY(ensure_arena(c, L.off));
     char* A = c.arena;
 
-    // ---- inputs
+    // ---- inputs: u8 rows (packed from float / half when needed), or the
+    // caller's FP16 rows for the FP16 kernel.
     const uint8_t* qd = nullptr;
     const uint8_t* rd = nullptr;
-    SIFT_TRY(stage_inputs(c, A, ip, a.type, a.q, a.r, q_n, r_n, st, qd, rd));
+    int shift = 0;
+    if (use_f16) {
+        SIFT_TRY(common_shift(c, a.q, a.r, true, q_n, r_n, st, shift));
+        g_launches += r_n > 0 ? 2 : 1;
+    } else {
+        SIFT_TRY(stage_inputs(c, A, ip, a.type, a.q, a.r, q_n, r_n, st, qd, rd, shift));
+    }
 
     // ---- norms
     int32_t* brec = reinterpret_cast<int32_t*>(A + o_brec);
     int32_t* qnorm = reinterpret_cast<int32_t*>(A + o_qnorm);
     int32_t* thresh = reinterpret_cast<int32_t*>(A + o_thr);
-    SIFT_CUDA(launch_row_norms_u8(rd, r_n, plan.r_pad, a.metric, nullptr, brec, nullptr, st));
-    SIFT_CUDA(launch_row_norms_u8(qd, q_n, plan.q_pad, kMetricL2, qnorm, nullptr, thresh, st));
+    if (use_f16) {
+        const float mul = ldexpf(1.0f, shift);
+        SIFT_CUDA(launch_row_norms_f16(a.r, r_n, plan.r_pad, mul, a.metric, nullptr, brec, nullptr, st));
+        SIFT_CUDA(launch_row_norms_f16(a.q, q_n, plan.q_pad, mul, kMetricL2, qnorm, nullptr, thresh, st));
+    } else {
+        SIFT_CUDA(launch_row_norms_u8(rd, r_n, plan.r_pad, a.metric, nullptr, brec, nullptr, st));
+        SIFT_CUDA(launch_row_norms_u8(qd, q_n, plan.q_pad, kMetricL2, qnorm, nullptr, thresh, st));
+    }
     g_launches += (plan.r_pad > 0 ? 1 : 0) + 1;
 
     // ---- fused GEMM + top-2
     int4* partial = reinterpret_cast<int4*>(A + o_part);
     if (r_n > 0) {
         CUtensorMap qmap, bmap;
-        SIFT_TRY(encode_u8_rows(&qmap, qd, q_n, kBM));
-        SIFT_TRY(encode_u8_rows(&bmap, rd, r_n, use_pair ? kBN / 2 : kBN));
+        if (use_f16) {
+            SIFT_TRY(encode_f16_rows(&qmap, a.q, q_n, kBM));
+            SIFT_TRY(encode_f16_rows(&bmap, a.r, r_n, kBN / 2));
+        } else {
+            SIFT_TRY(encode_u8_rows(&qmap, qd, q_n, kBM));
+            SIFT_TRY(encode_u8_rows(&bmap, rd, r_n, use_pair ? kBN / 2 : kBN));
+        }
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         const bool prof = g_profile.load();
         if (prof) {
@@ -315,7 +390,10 @@ int exact_match(const MatchArgs& a) {
             SIFT_CUDA(cudaEventCreate(&e1));
             SIFT_CUDA(cudaEventRecord(e0, st));
         }
-        if (use_pair)
+        if (use_f16)
+            SIFT_CUDA(launch_exact2nn_f16_pair(qmap, bmap, brec, plan, partial, thresh, c.d_status,
+                                               ldexpf(1.0f, 2 * shift), st));
+        else if (use_pair)
             SIFT_CUDA(launch_exact2nn_u8_pair(qmap, bmap, brec, plan, partial, thresh, c.d_status, st));
         else
             SIFT_CUDA(launch_exact2nn_u8(qmap, bmap, brec, plan, partial, thresh, c.d_status, st));
@@ -332,7 +410,8 @@ int exact_match(const MatchArgs& a) {
     float4* s_out = (a.sorted && !s_dev) ? reinterpret_cast<float4*>(A + o_s) : reinterpret_cast<float4*>(a.sorted);
     int32_t* i_out = (a.nn_idx && !i_dev) ? reinterpret_cast<int32_t*>(A + o_i) : a.nn_idx;
     float* d_out = (a.nn_dist && !d_dev) ? reinterpret_cast<float*>(A + o_d) : a.nn_dist;
-    SIFT_CUDA(launch_merge2nn(partial, plan, qnorm, a.metric, a.threshold, m_out, s_out, i_out, d_out, st));
+    SIFT_CUDA(launch_merge2nn(partial, plan, qnorm, a.metric, a.threshold, ldexpf(1.0f, -2 * shift), m_out, s_out,
+                              i_out, d_out, st));
     ++g_launches;
     if (a.matches && !m_dev)
         SIFT_CUDA(cudaMemcpyAsync(a.matches, m_out, static_cast<size_t>(q_n) * 4, cudaMemcpyDeviceToHost, st));
@@ -399,7 +478,8 @@ int lsh_match(const LshArgs& a) {
 
     const uint8_t* qd = nullptr;
     const uint8_t* rd = nullptr;
-    SIFT_TRY(stage_inputs(c, A, ip, a.type, a.q, a.r, q_n, r_n, st, qd, rd));
+    int vshift = 0;  // inputs were integers times 2^-vshift
+    SIFT_TRY(stage_inputs(c, A, ip, a.type, a.q, a.r, q_n, r_n, st, qd, rd, vshift));
     const int8_t* pl = a.planes;
     if (!planes_dev) {
         SIFT_CUDA(cudaMemcpyAsync(A + o_pl, a.planes, static_cast<size_t>(L_) * k * kDim, cudaMemcpyDefault, st));
@@ -431,7 +511,7 @@ int lsh_match(const LshArgs& a) {
     int32_t* i_out = (a.nn_idx && !i_dev) ? reinterpret_cast<int32_t*>(A + o_i) : a.nn_idx;
     float* d_out = (a.nn_dist && !d_dev) ? reinterpret_cast<float*>(A + o_d) : a.nn_dist;
     SIFT_CUDA(launch_lsh_scan(qd, rd, q_n, r_n, L_, shift, nbins, codes_q, start, order, ocode, qnorm, rnorm,
-                              a.threshold, a.ratio ? 1 : 0, m_out, i_out, d_out, st));
+                              a.threshold, a.ratio ? 1 : 0, ldexpf(1.0f, -2 * vshift), m_out, i_out, d_out, st));
     g_launches += 1 + (r_n > 0 ? 3 : 0) + 1;
     if (a.matches && !m_dev)
         SIFT_CUDA(cudaMemcpyAsync(a.matches, m_out, static_cast<size_t>(q_n) * 4, cudaMemcpyDeviceToHost, st));
@@ -512,7 +592,7 @@ int profile_collect(double* total_ms, int* launches) {
 
 long long launch_count() { return g_launches.load(); }
 int set_variant(int v) {
-    if (v != 0 && v != 1) return SIFT_ERR_INVALID_ARG;
+    if (v < 0 || v > 2) return SIFT_ERR_INVALID_ARG;
     g_variant.store(v);
     return SIFT_OK;
 }

@@ -15,6 +15,13 @@ __device__ __forceinline__ int max8(const uint32_t* v) {
     return max(m, static_cast<int>(v[7]));
 }
 
+// f32 accumulators holding integer multiples of 1/dscale (dscale a power of
+// two; exact, see the FP16 kernel) -> the integer dot products, in place.
+__device__ __forceinline__ void f32_to_dot(uint32_t (&v)[32], float dscale) {
+    #pragma unroll
+    for (int c = 0; c < 32; ++c) v[c] = static_cast<uint32_t>(__float2int_rn(__uint_as_float(v[c]) * dscale));
+}
+
 // Per-thread running top-2 of one query row over base rows visited in
 // increasing index order (strict '<' keeps the lower index on ties).
 struct Top2 {

@@ -40,6 +40,7 @@
 #include <cfloat>
 #include <climits>
 #include <algorithm>
+#include <cuda_fp16.h>
 #include "exact2nn.cuh"
 #include "ptx.cuh"
 #include "epilogue.cuh"
@@ -67,16 +68,40 @@ struct __align__(8) SmemCtl {
 constexpr size_t kSmemBytes =
     1024 + kQT * kQTileBytes + kStages * kBTileBytes + kStages * kRecBytes + sizeof(SmemCtl);
 
-__global__ void __launch_bounds__(256) row_norms_u8_kernel(const uint8_t* __restrict__ x, int n, int n_pad,
-                                                           int metric, int32_t* __restrict__ norm,
-                                                           int32_t* __restrict__ rec,
-                                                           int32_t* __restrict__ thresh) {
-    // 32 rows per block, 8 threads per row, 16 bytes per thread.
+// 16 consecutive elements of a row as u8 (FP16: value * mul, exact by contract).
+__device__ __forceinline__ uint4 load16_u8(const uint8_t* x, int row, int sub, float) {
+    return reinterpret_cast<const uint4*>(x + static_cast<size_t>(row) * kDim)[sub];
+}
+__device__ __forceinline__ uint4 load16_u8(const __half* x, int row, int sub, float mul) {
+    const uint4* p = reinterpret_cast<const uint4*>(x + static_cast<size_t>(row) * kDim) + 2 * sub;
+    uint32_t w[4];
+    #pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const uint4 v = p[h];
+        const __half2* hv = reinterpret_cast<const __half2*>(&v);
+        #pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const float2 a = __half22float2(hv[2 * k]), b = __half22float2(hv[2 * k + 1]);
+            w[2 * h + k] = static_cast<uint32_t>(__float2int_rn(a.x * mul)) |
+                           (static_cast<uint32_t>(__float2int_rn(a.y * mul)) << 8) |
+                           (static_cast<uint32_t>(__float2int_rn(b.x * mul)) << 16) |
+                           (static_cast<uint32_t>(__float2int_rn(b.y * mul)) << 24);
+        }
+    }
+    return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) row_norms_kernel(const T* __restrict__ x, int n, int n_pad, float mul,
+                                                        int metric, int32_t* __restrict__ norm,
+                                                        int32_t* __restrict__ rec,
+                                                        int32_t* __restrict__ thresh) {
+    // 32 rows per block, 8 threads per row, 16 elements per thread.
     const int row = blockIdx.x * 32 + (threadIdx.x >> 3);
     const int sub = threadIdx.x & 7;
     uint32_t s = 0;
     if (row < n) {
-        const uint4 w = reinterpret_cast<const uint4*>(x + static_cast<size_t>(row) * kDim)[sub];
+        const uint4 w = load16_u8(x, row, sub, mul);
         s = __dp4a(w.x, w.x, 0u);
         s = __dp4a(w.y, w.y, s);
         s = __dp4a(w.z, w.z, s);
@@ -343,6 +368,7 @@ __device__ __forceinline__ bool lex_less(int ka, int ia, int kb, int ib) {
 
 __global__ void __launch_bounds__(256) merge2nn_kernel(const int4* __restrict__ partial, const ExactPlan plan,
                                                        const int32_t* __restrict__ qnorm, int metric, float thr,
+                                                       float dscale,
                                                        uint32_t* __restrict__ matches, float4* __restrict__ sorted,
                                                        int32_t* __restrict__ nn_idx, float* __restrict__ nn_dist) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -371,8 +397,8 @@ __global__ void __launch_bounds__(256) merge2nn_kernel(const int4* __restrict__ 
     const bool v1 = j1 >= 0 && a1 < kKeyPad;
     const bool v2 = j2 >= 0 && a2 < kKeyPad;
     const int qn = metric == kMetricL2 ? qnorm[q] : 0;
-    const float d1 = v1 ? static_cast<float>(a1 + qn) : FLT_MAX;
-    const float d2 = v2 ? static_cast<float>(a2 + qn) : FLT_MAX;
+    const float d1 = v1 ? static_cast<float>(a1 + qn) * dscale : FLT_MAX;
+    const float d2 = v2 ? static_cast<float>(a2 + qn) * dscale : FLT_MAX;
     if (matches) {
         bool pass = false;
         if (v1) {
@@ -432,7 +458,15 @@ size_t exact2nn_smem_bytes() { return kSmemBytes; }
 cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* norm, int32_t* rec,
                                 int32_t* thresh, cudaStream_t stream) {
     if (n_pad <= 0) return cudaSuccess;
-    row_norms_u8_kernel<<<n_pad / 32, 256, 0, stream>>>(x, n, n_pad, metric, norm, rec, thresh);
+    row_norms_kernel<uint8_t><<<n_pad / 32, 256, 0, stream>>>(x, n, n_pad, 1.0f, metric, norm, rec, thresh);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_row_norms_f16(const void* x, int n, int n_pad, float mul, int metric, int32_t* norm, int32_t* rec,
+                                 int32_t* thresh, cudaStream_t stream) {
+    if (n_pad <= 0) return cudaSuccess;
+    row_norms_kernel<__half><<<n_pad / 32, 256, 0, stream>>>(static_cast<const __half*>(x), n, n_pad, mul, metric,
+                                                             norm, rec, thresh);
     return cudaGetLastError();
 }
 
@@ -455,11 +489,11 @@ cudaError_t launch_exact2nn_u8(const CUtensorMap& qmap, const CUtensorMap& bmap,
 }
 
 cudaError_t launch_merge2nn(const int4* partial, const ExactPlan& plan, const int32_t* qnorm, int metric,
-                            float threshold, uint32_t* matches, float4* sorted, int32_t* nn_idx, float* nn_dist,
-                            cudaStream_t stream) {
+                            float threshold, float dist_scale, uint32_t* matches, float4* sorted, int32_t* nn_idx,
+                            float* nn_dist, cudaStream_t stream) {
     if (plan.q_n <= 0) return cudaSuccess;
-    merge2nn_kernel<<<(plan.q_n + 255) / 256, 256, 0, stream>>>(partial, plan, qnorm, metric, threshold, matches,
-                                                               sorted, nn_idx, nn_dist);
+    merge2nn_kernel<<<(plan.q_n + 255) / 256, 256, 0, stream>>>(partial, plan, qnorm, metric, threshold, dist_scale,
+                                                               matches, sorted, nn_idx, nn_dist);
     return cudaGetLastError();
 }
 

@@ -68,6 +68,10 @@ ExactPlan make_exact_plan(int q_n, int r_n, int num_workers, int parts);
 //                                     pruning bound of the search kernel)
 cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* norm, int32_t* rec,
                                 int32_t* thresh, cudaStream_t stream);
+// The same for FP16 rows whose values times mul (a power of two) are
+// integers in [0, 255].
+cudaError_t launch_row_norms_f16(const void* x, int n, int n_pad, float mul, int metric, int32_t* norm, int32_t* rec,
+                                 int32_t* thresh, cudaStream_t stream);
 
 // The fused GEMM + top-2 kernel. partial: [max_splits][parts][q_pad] int4
 // {key1, idx1, key2, idx2} with key = norm(b) - 2 q.b. brec: base records
@@ -81,6 +85,12 @@ cudaError_t launch_exact2nn_u8(const CUtensorMap& qmap, const CUtensorMap& bmap,
 cudaError_t launch_exact2nn_u8_pair(const CUtensorMap& qmap, const CUtensorMap& bmap_half, const int32_t* brec,
                                     const ExactPlan& plan, int4* partial, int32_t* thresh, int* err,
                                     cudaStream_t stream);
+// FP16 rows (bmap_half / qmap: half tensor maps with boxes of 64 elements):
+// values are integers times 2^-s and dscale = 2^(2s) turns the f32 dot
+// products back into integers (brec built from the same integers).
+cudaError_t launch_exact2nn_f16_pair(const CUtensorMap& qmap, const CUtensorMap& bmap_half, const int32_t* brec,
+                                     const ExactPlan& plan, int4* partial, int32_t* thresh, int* err, float dscale,
+                                     cudaStream_t stream);
 size_t exact2nn_pair_smem_bytes();
 
 // Merge of the per-CTA partial top-2 lists, distances, ratio test and output.
@@ -89,9 +99,11 @@ size_t exact2nn_pair_smem_bytes();
 //   sorted[q]    {d1, d2, i1, i2} as floats (FLT_MAX where absent)
 //   nn_idx[2q..] int32 indices (-1 where absent)
 //   nn_dist[2q..] float distances (FLT_MAX where absent)
+// dist_scale multiplies every distance (2^-2s for inputs that were integers
+// times 2^-s; 1 otherwise) before the ratio test and the outputs.
 cudaError_t launch_merge2nn(const int4* partial, const ExactPlan& plan, const int32_t* qnorm, int metric,
-                            float threshold, uint32_t* matches, float4* sorted, int32_t* nn_idx, float* nn_dist,
-                            cudaStream_t stream);
+                            float threshold, float dist_scale, uint32_t* matches, float4* sorted, int32_t* nn_idx,
+                            float* nn_dist, cudaStream_t stream);
 
 size_t exact2nn_smem_bytes();
 

@@ -42,6 +42,22 @@
 //   tempty[b]  (L) the 8 warps of buffer b in each CTA read it      remote arrive
 // Every wait is bounded (2 s); an expired wait raises the CTA's abort flag
 // and records an error code, and every role still reaches the teardown.
+//
+// Two instantiations of one body:
+//   exact2nn_u8_pair_kernel   u8 rows (128 B), kind::i8, s32 accumulators,
+//                             4 MMAs of K = 32 per 128 x 128 tile product
+//   exact2nn_f16_pair_kernel  FP16 rows (256 B = two 128-byte K blocks, each
+//                             loaded by its own TMA box of 64 halves), kind::f16
+//                             with f32 accumulators, 8 MMAs of K = 16. This is
+//                             the counterpart of the reference's half GEMM
+//                             (cublasHgemm, src/knn_brute.cu:262-266). Values
+//                             are integers times 2^-s (|integer| <= 255), so
+//                             every product and partial sum is an integer
+//                             multiple of 2^-2s below 2^24 * 2^-2s and the f32
+//                             accumulators are exact; the epilogue turns them
+//                             into the same integer dot products as the u8
+//                             kernel (times dscale = 2^2s, rounded) and the
+//                             rest is shared.
 #include <climits>
 #include "exact2nn.cuh"
 #include "ptx.cuh"
@@ -53,10 +69,7 @@ namespace {
 
 constexpr int kPQT = 2;                          // query tiles per CTA
 constexpr int kPHalf = kBN / 2;                  // base rows loaded per CTA per unit
-constexpr int kPQTileBytes = kBM * kDim;         // 16 KB
-constexpr int kPBHalfBytes = kPHalf * kDim;      // 8 KB
 constexpr int kPRecBytes = kRecInts * 4;         // 640 B
-constexpr int kPStages = 12;
 constexpr int kPSlots = 2 * kPQT;                // (query tile, buffer)
 constexpr int kPEpiWarps = 16;
 constexpr int kPThreads = 64 + 32 * kPEpiWarps;
@@ -65,25 +78,50 @@ constexpr uint16_t kPairMask = 0x3;
 static_assert(kPEpiWarps == 4 * kPSlots, "one epilogue warp per (slot, lane quarter)");
 static_assert(kPQT * 2 * kBM == kQT * kBM, "a pair covers one query group");
 
-struct __align__(8) PairCtl {
-    uint64_t full[kPStages];
-    uint64_t rfull[kPStages];
-    uint64_t sfree[kPStages];
-    uint64_t qfull, qempty;
-    uint64_t tfull[2], tempty[2];
-    uint64_t drain;
-    uint32_t tmem_base;
-    int abort_flag;
-    int no_abort;
+// Shapes of one element type. A row of 128 elements is kKBlocks blocks of
+// 128 bytes; each block of a tile is stored as its own SW128 K-major tile
+// (rows x 128 B), and every MMA consumes 32 bytes of K.
+template <bool F16>
+struct PairCfg {
+    static constexpr int kElemBytes = F16 ? 2 : 1;
+    static constexpr int kKBlocks = F16 ? 2 : 1;
+    static constexpr int kBoxElems = 128 / kElemBytes;       // TMA box width of one K block
+    static constexpr int kQKBlock = kBM * 128;               // bytes of one K block of a query tile
+    static constexpr int kBKBlock = kPHalf * 128;            // bytes of one K block of a base half
+    static constexpr int kQTileBytes = kKBlocks * kQKBlock;  // 16 / 32 KB
+    static constexpr int kBHalfBytes = kKBlocks * kBKBlock;  // 8 / 16 KB
+    static constexpr int kStages = F16 ? 8 : 12;
+    struct __align__(8) Ctl {
+        uint64_t full[kStages];
+        uint64_t rfull[kStages];
+        uint64_t sfree[kStages];
+        uint64_t qfull, qempty;
+        uint64_t tfull[2], tempty[2];
+        uint64_t drain;
+        uint32_t tmem_base;
+        int abort_flag;
+        int no_abort;
+    };
+    static constexpr size_t kSmemBytes =
+        1024 + kPQT * kQTileBytes + kStages * kBHalfBytes + kStages * kPRecBytes + sizeof(Ctl);
+    // M = 256 (the pair), N = kBN; s32 accumulators for u8 x u8, f32 for f16 x f16.
+    static constexpr uint32_t kIdesc =
+        F16 ? ptx::idesc_make(1 /*F32*/, 0 /*F16*/, 0 /*F16*/, 2 * kBM, kBN)
+            : ptx::idesc_make(2 /*S32*/, 0 /*u8*/, 0 /*u8*/, 2 * kBM, kBN);
 };
+static_assert(PairCfg<true>::kSmemBytes <= 227 * 1024, "FP16 pair kernel shared memory");
+static_assert(PairCfg<false>::kSmemBytes <= 227 * 1024, "u8 pair kernel shared memory");
 
-constexpr size_t kPSmemBytes =
-    1024 + kPQT * kPQTileBytes + kPStages * kPBHalfBytes + kPStages * kPRecBytes + sizeof(PairCtl);
-
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
-    exact2nn_u8_pair_kernel(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap bmap,
-                            const int32_t* __restrict__ brec, const ExactPlan plan, int4* __restrict__ partial,
-                            int32_t* __restrict__ thresh, int* __restrict__ err) {
+template <bool F16>
+__device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtensorMap& bmap,
+                                          const int32_t* __restrict__ brec, const ExactPlan& plan,
+                                          int4* __restrict__ partial, int32_t* __restrict__ thresh,
+                                          int* __restrict__ err, float dscale) {
+    using Cfg = PairCfg<F16>;
+    constexpr int kPStages = Cfg::kStages;
+    constexpr int kPQTileBytes = Cfg::kQTileBytes;
+    constexpr int kPBHalfBytes = Cfg::kBHalfBytes;
+    using PairCtl = typename Cfg::Ctl;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw_u32 = ptx::smem_u32(smem_raw);
     uint8_t* smem = smem_raw + ((1024u - (raw_u32 & 1023u)) & 1023u);
@@ -163,9 +201,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
                         !ptx::mbar_wait_cluster(bar_qempty, (ngroups - 1) & 1, abort_flag, err, kErrWaitQuery))
                         break;
                     if (leader) ptx::mbar_arrive_expect_tx(bar_qfull, 2 * kPQT * kPQTileBytes);
-                    for (int t = 0; t < kPQT; ++t)
-                        ptx::tma_load_2d_pair(q_s + t * kPQTileBytes, &qmap, 0,
-                                              ((g * kPQT + t) * 2 + static_cast<int>(rank)) * kBM, lead_qfull);
+                    for (int t = 0; t < kPQT; ++t) {
+                        #pragma unroll
+                        for (int kb = 0; kb < Cfg::kKBlocks; ++kb)
+                            ptx::tma_load_2d_pair(q_s + t * kPQTileBytes + kb * Cfg::kQKBlock, &qmap,
+                                                  kb * Cfg::kBoxElems,
+                                                  ((g * kPQT + t) * 2 + static_cast<int>(rank)) * kBM, lead_qfull);
+                    }
                     cur_g = g;
                     ++ngroups;
                 }
@@ -173,8 +215,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
                 if (!ptx::mbar_wait(bar_sfree + 8 * s, ((n / kPStages) & 1) ^ 1, abort_flag, err, kErrWaitProducer))
                     break;
                 if (leader) ptx::mbar_arrive_expect_tx(bar_full + 8 * s, 2 * kPBHalfBytes);
-                ptx::tma_load_2d_pair(b_s + s * kPBHalfBytes, &bmap, 0, j * kBN + static_cast<int>(rank) * kPHalf,
-                                      lead_full + 8 * s);
+                #pragma unroll
+                for (int kb = 0; kb < Cfg::kKBlocks; ++kb)
+                    ptx::tma_load_2d_pair(b_s + s * kPBHalfBytes + kb * Cfg::kBKBlock, &bmap, kb * Cfg::kBoxElems,
+                                          j * kBN + static_cast<int>(rank) * kPHalf, lead_full + 8 * s);
                 ptx::mbar_arrive_expect_tx(bar_rfull + 8 * s, kPRecBytes);
                 ptx::bulk_load(r_s + s * kPRecBytes, brec + static_cast<size_t>(j) * kRecInts, kPRecBytes,
                                bar_rfull + 8 * s);
@@ -194,7 +238,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
     } else if (warp == 1) {
         if (lane == 0 && leader) {
             // -------------------------------------------------- MMA issuer
-            constexpr uint32_t idesc = ptx::idesc_make(2 /*S32*/, 0 /*u8*/, 0 /*u8*/, 2 * kBM, kBN);
+            constexpr uint32_t idesc = Cfg::kIdesc;
             const uint64_t a_desc0 = ptx::sdesc_sw128(q_s);
             const uint64_t b_desc0 = ptx::sdesc_sw128(b_s);
             int cur_g = -1, ngroups = 0;
@@ -221,10 +265,20 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
                 #pragma unroll
                 for (int t = 0; t < kPQT; ++t) {
                     const uint32_t d = tmem + (t * 2 + buf) * kBN;
-                    const uint64_t a_desc = a_desc0 + static_cast<uint64_t>((t * kPQTileBytes) >> 4);
                     #pragma unroll
-                    for (int kk = 0; kk < kDim / 32; ++kk)
-                        ptx::mma_i8_pair(d, a_desc + 2 * kk, b_desc + 2 * kk, idesc, kk > 0 ? 1u : 0u);
+                    for (int kb = 0; kb < Cfg::kKBlocks; ++kb) {
+                        const uint64_t a_desc =
+                            a_desc0 + static_cast<uint64_t>((t * kPQTileBytes + kb * Cfg::kQKBlock) >> 4);
+                        const uint64_t b_kb = b_desc + static_cast<uint64_t>((kb * Cfg::kBKBlock) >> 4);
+                        #pragma unroll
+                        for (int kk = 0; kk < 4; ++kk) {
+                            const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
+                            if constexpr (F16)
+                                ptx::mma_f16_pair(d, a_desc + 2 * kk, b_kb + 2 * kk, idesc, acc);
+                            else
+                                ptx::mma_i8_pair(d, a_desc + 2 * kk, b_kb + 2 * kk, idesc, acc);
+                        }
+                    }
                 }
                 ptx::tc_commit_pair_mc(bar_tfull + 8 * buf, kPairMask);
                 const bool last_of_group = (n + 1 == n_units) || (j + 1 == BT);
@@ -289,15 +343,19 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
                     uint32_t va[32];
                     ptx::tmem_ld32(taddr, va);
                     ptx::tmem_ld_wait(va);
+                    if constexpr (F16) f32_to_dot(va, dscale);
                     scan_group(va, row0, gm.x, rec, rec + 128, st);
                     ptx::tmem_ld32(taddr + 32, va);
                     ptx::tmem_ld_wait(va);
+                    if constexpr (F16) f32_to_dot(va, dscale);
                     scan_group(va, row0 + 32, gm.y, rec + 32, rec + 132, st);
                     ptx::tmem_ld32(taddr + 64, va);
                     ptx::tmem_ld_wait(va);
+                    if constexpr (F16) f32_to_dot(va, dscale);
                     scan_group(va, row0 + 64, gm.z, rec + 64, rec + 136, st);
                     ptx::tmem_ld32(taddr + 96, va);
                     ptx::tmem_ld_wait(va);
+                    if constexpr (F16) f32_to_dot(va, dscale);
                     ptx::tc_fence_before();
                     __syncwarp();
                     if (lane == 0) ptx::mbar_arrive_cluster_relaxed(lead_tempty);
@@ -331,26 +389,58 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
     }
 }
 
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
+    exact2nn_u8_pair_kernel(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap bmap,
+                            const int32_t* __restrict__ brec, const ExactPlan plan, int4* __restrict__ partial,
+                            int32_t* __restrict__ thresh, int* __restrict__ err) {
+    pair_body<false>(qmap, bmap, brec, plan, partial, thresh, err, 1.0f);
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
+    exact2nn_f16_pair_kernel(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap bmap,
+                             const int32_t* __restrict__ brec, const ExactPlan plan, int4* __restrict__ partial,
+                             int32_t* __restrict__ thresh, int* __restrict__ err, float dscale) {
+    pair_body<true>(qmap, bmap, brec, plan, partial, thresh, err, dscale);
+}
+
+template <typename K>
+cudaError_t set_smem_once(K kernel, size_t bytes, bool (&done)[64]) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64 || !done[dev]) {
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+        if (e != cudaSuccess) return e;
+        if (dev >= 0 && dev < 64) done[dev] = true;
+    }
+    return cudaSuccess;
+}
+
 }  // namespace
 
-size_t exact2nn_pair_smem_bytes() { return kPSmemBytes; }
+size_t exact2nn_pair_smem_bytes() { return PairCfg<false>::kSmemBytes; }
 
 cudaError_t launch_exact2nn_u8_pair(const CUtensorMap& qmap, const CUtensorMap& bmap_half, const int32_t* brec,
                                     const ExactPlan& plan, int4* partial, int32_t* thresh, int* err,
                                     cudaStream_t stream) {
     static bool attr_set[64] = {};
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    cudaError_t e = set_smem_once(exact2nn_u8_pair_kernel, PairCfg<false>::kSmemBytes, attr_set);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
-        e = cudaFuncSetAttribute(exact2nn_u8_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(kPSmemBytes));
-        if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < 64) attr_set[dev] = true;
-    }
     if (plan.grid <= 0) return cudaSuccess;
-    exact2nn_u8_pair_kernel<<<2 * plan.grid, kPThreads, kPSmemBytes, stream>>>(qmap, bmap_half, brec, plan, partial,
-                                                                               thresh, err);
+    exact2nn_u8_pair_kernel<<<2 * plan.grid, kPThreads, PairCfg<false>::kSmemBytes, stream>>>(
+        qmap, bmap_half, brec, plan, partial, thresh, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_exact2nn_f16_pair(const CUtensorMap& qmap, const CUtensorMap& bmap_half, const int32_t* brec,
+                                     const ExactPlan& plan, int4* partial, int32_t* thresh, int* err, float dscale,
+                                     cudaStream_t stream) {
+    static bool attr_set[64] = {};
+    cudaError_t e = set_smem_once(exact2nn_f16_pair_kernel, PairCfg<true>::kSmemBytes, attr_set);
+    if (e != cudaSuccess) return e;
+    if (plan.grid <= 0) return cudaSuccess;
+    exact2nn_f16_pair_kernel<<<2 * plan.grid, kPThreads, PairCfg<true>::kSmemBytes, stream>>>(
+        qmap, bmap_half, brec, plan, partial, thresh, err, dscale);
     return cudaGetLastError();
 }
 

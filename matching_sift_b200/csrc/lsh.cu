@@ -281,7 +281,8 @@ __global__ void __launch_bounds__(256) lsh_scan_kernel(const uint8_t* __restrict
                                                        const uint32_t* __restrict__ ocode,
                                                        const int32_t* __restrict__ qnorm,
                                                        const int32_t* __restrict__ rnorm, float thr, int ratio,
-                                                       uint32_t* __restrict__ matches, int32_t* __restrict__ nn_idx,
+                                                       float dscale, uint32_t* __restrict__ matches,
+                                                       int32_t* __restrict__ nn_idx,
                                                        float* __restrict__ nn_dist) {
     const int wq = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -329,8 +330,8 @@ __global__ void __launch_bounds__(256) lsh_scan_kernel(const uint8_t* __restrict
     }
     if (lane == 0) {
         const bool v1 = i1 >= 0, v2 = i2 >= 0;
-        const float f1 = v1 ? static_cast<float>(d1) : FLT_MAX;
-        const float f2 = v2 ? static_cast<float>(d2) : FLT_MAX;
+        const float f1 = v1 ? static_cast<float>(d1) * dscale : FLT_MAX;
+        const float f2 = v2 ? static_cast<float>(d2) * dscale : FLT_MAX;
         if (matches) {
             bool pass = v1;
             if (v1 && ratio) pass = (sqrtf(f1) / (v2 ? sqrtf(f2) : INFINITY)) < thr;
@@ -385,12 +386,12 @@ cudaError_t launch_lsh_buckets(const uint32_t* codes, int n, int L, int shift, i
 
 cudaError_t launch_lsh_scan(const uint8_t* q, const uint8_t* r, int q_n, int r_n, int L, int shift, int nbins,
                             const uint32_t* qcodes, const int* start, const int* order, const uint32_t* ocode,
-                            const int32_t* qnorm, const int32_t* rnorm, float thr, int ratio, uint32_t* matches,
-                            int32_t* nn_idx, float* nn_dist, cudaStream_t stream) {
+                            const int32_t* qnorm, const int32_t* rnorm, float thr, int ratio, float dist_scale,
+                            uint32_t* matches, int32_t* nn_idx, float* nn_dist, cudaStream_t stream) {
     if (q_n <= 0) return cudaSuccess;
     const int blocks = (q_n * 32 + 255) / 256;
     lsh_scan_kernel<<<blocks, 256, 0, stream>>>(q, r, q_n, r_n, L, shift, nbins, qcodes, start, order, ocode, qnorm,
-                                                rnorm, thr, ratio, matches, nn_idx, nn_dist);
+                                                rnorm, thr, ratio, dist_scale, matches, nn_idx, nn_dist);
     return cudaGetLastError();
 }
 

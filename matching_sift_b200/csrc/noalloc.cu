@@ -142,7 +142,7 @@ extern "C" SIFT_API int sift2nn_match_noalloc(const uint8_t* q, const uint8_t* r
         if (launch_exact2nn_u8_pair(qmap, bmap, rec, plan, partial, thresh, err, st) != cudaSuccess)
             return SIFT_ERR_CUDA;
     }
-    if (launch_merge2nn(partial, plan, qnorm, kMetricL2, threshold, matches, nullptr, nn_idx, nn_dist, st) !=
+    if (launch_merge2nn(partial, plan, qnorm, kMetricL2, threshold, 1.0f, matches, nullptr, nn_idx, nn_dist, st) !=
         cudaSuccess)
         return SIFT_ERR_CUDA;
     return SIFT_OK;
