@@ -179,6 +179,46 @@ SIFT_API int sift_lsh_match(const void* q, const void* r, int type, uint32_t q_n
 SIFT_API int sift2nn_match_noalloc(const uint8_t* q, const uint8_t* r, uint32_t q_n, uint32_t r_n, float threshold,
                                    uint32_t* matches, int32_t* nn_idx, float* nn_dist, void* stream);
 
+/* Batched exact 2-NN of many independent (query set, base set) problems,
+   e.g. the keypoint descriptors of many image pairs of uneven sizes, in one
+   persistent launch driven by a device work list (no counterpart in the
+   reference, which matches one pair per call). q: the query sets of all
+   problems concatenated in problem order (sum of n_q rows); r: r_rows base
+   rows, problem p using rows [r_off, r_off + n_r) (problems may share rows).
+   Both uint8 [rows][128], 16-byte aligned device memory. Outputs are per
+   query row of q (device memory; any may be NULL), indices local to the
+   problem's base set: matches (ratio test at `threshold`, else UINT32_MAX),
+   nn_idx[2*row] (-1 absent), nn_dist[2*row] (squared L2, FLT_MAX absent).
+   Asynchronous on `stream`; the kernel shape is the one last tuned for a
+   batch of the same sizes, else the default. */
+typedef struct sift_pair {
+    uint32_t n_q;   /* query rows of the problem (consecutive in q) */
+    uint32_t n_r;   /* base rows of the problem */
+    uint32_t r_off; /* first base row of the problem in r */
+} sift_pair;
+SIFT_API int sift2nn_match_batch(const uint8_t* q, const uint8_t* r, uint32_t r_rows, const sift_pair* pairs,
+                                 int n_pairs, float threshold, uint32_t* matches, int32_t* nn_idx, float* nn_dist,
+                                 void* stream);
+
+/* A batch bound to fixed buffers, replayed as one CUDA graph: create times
+   the kernel shapes on this batch when flags has SIFT_BATCH_TUNE (the choice
+   is remembered for batches of the same sizes), or takes shape k with
+   SIFT_BATCH_SHAPE(k), k in 0..2 (0: 512-query groups, one query buffer;
+   1: 512-query groups, two buffers; 2: 256-query groups, two buffers). The
+   plan owns its scratch memory; run launches the graph on `stream` (the
+   results follow the current contents of q and r). Create synchronises. */
+typedef struct sift_batch_plan sift_batch_plan;
+#define SIFT_BATCH_TUNE 1
+#define SIFT_BATCH_SHAPE(k) (((k) + 1) << 4)
+SIFT_API int sift_batch_plan_create(const uint8_t* q, const uint8_t* r, uint32_t r_rows, const sift_pair* pairs,
+                                    int n_pairs, float threshold, uint32_t* matches, int32_t* nn_idx, float* nn_dist,
+                                    int flags, sift_batch_plan** plan);
+SIFT_API int sift_batch_plan_run(sift_batch_plan* plan, void* stream);
+/* Chosen shape (query tiles per CTA, query buffers) and, after tuning, the
+   measured milliseconds of each shape (tuned_ms[3], -1 when not timed). */
+SIFT_API int sift_batch_plan_info(const sift_batch_plan* plan, int* qpt, int* qbuf, float* tuned_ms);
+SIFT_API void sift_batch_plan_destroy(sift_batch_plan* plan);
+
 /* Synchronises `stream` and returns the device status of the calls issued on
    the current device since the last check (SIFT_OK, SIFT_ERR_DEVICE_TIMEOUT
    when a bounded wait inside a kernel expired, SIFT_ERR_CUDA). */
@@ -193,6 +233,13 @@ SIFT_API const char* sift_version(void);
 /* ---------------------------------------------------------------------
  * Part 3: instrumentation (used by the benchmark)
  * ------------------------------------------------------------------- */
+
+/* Host-side work decomposition of a batch (no GPU needed): out[0..5] =
+   units, base-tile records, query rows, max CTA pairs sharing one query
+   group, CTA pairs launched, queries per group; for `workers` CTA pairs and
+   qpt query tiles per CTA (1 or 2). */
+SIFT_API int sift_batch_describe(const sift_pair* pairs, int n_pairs, uint32_t r_rows, int qpt, int workers,
+                                 long long* out);
 
 /* Number of kernels this library has launched in the process so far. */
 SIFT_API long long sift_launch_count(void);

@@ -13,14 +13,15 @@ from __future__ import annotations
 
 import ctypes
 
-from ._native import (FLOAT_DEVICE, FLOAT_HOST, HALF_DEVICE, METRIC_DOT, METRIC_L2, SIFT_ERR_ALLOC,
+from ._native import (SIFT_BATCH_SHAPE, SIFT_BATCH_TUNE,
+                      FLOAT_DEVICE, FLOAT_HOST, HALF_DEVICE, METRIC_DOT, METRIC_L2, SIFT_ERR_ALLOC,
                       SIFT_ERR_CUDA, SIFT_ERR_DEVICE_TIMEOUT, SIFT_ERR_INVALID_ARG, SIFT_ERR_NO_DEVICE,
                       SIFT_ERR_NOT_INTEGER, SIFT_ERR_UNSUPPORTED, SIFT_OK, U8_DEVICE, U8_HOST, LIB_PATH,
                       SiftError, check, lib, status_string)
 
 __all__ = [
     "cublas_2nn_sift", "cublas_2nn_f", "device_brute", "host_brute", "lsh_gpu", "match", "lsh_match", "lsh_hash",
-    "stream_status", "version",
+    "stream_status", "version", "match_batch", "BatchPlan", "batch_describe",
     "SiftError", "FLOAT_HOST", "FLOAT_DEVICE", "HALF_DEVICE", "U8_DEVICE", "U8_HOST", "METRIC_L2", "METRIC_DOT",
 ]
 
@@ -159,3 +160,95 @@ def lsh_match(q, r, planes, threshold: float = 0.0, stream=None):
                                threshold, out["matches"].data_ptr(), out["nn_idx"].data_ptr(),
                                out["nn_dist"].data_ptr(), s.cuda_stream), "sift_lsh_match")
     return out
+
+
+# ------------------------------------------------------------------ batches --
+
+def _pairs_array(pairs):
+    """(n, 3) uint32 rows {n_q, n_r, r_off} as a contiguous array (sift_pair[])."""
+    import numpy as np
+
+    a = np.ascontiguousarray(np.asarray(pairs, dtype=np.uint32).reshape(-1, 3))
+    return a
+
+
+def _batch_outputs(total_q, dev):
+    import torch
+
+    return {"matches": torch.empty(total_q, dtype=torch.int32, device=dev),
+            "nn_idx": torch.empty((total_q, 2), dtype=torch.int32, device=dev),
+            "nn_dist": torch.empty((total_q, 2), dtype=torch.float32, device=dev)}
+
+
+def match_batch(q, r, pairs, threshold: float = 0.8, stream=None):
+    """Exact 2-NN of many problems in one launch.
+
+    q: uint8 CUDA tensor, the query sets of all problems concatenated in
+    order; r: uint8 CUDA tensor of base rows; pairs: rows {n_q, n_r, r_off}.
+    Returns {"matches", "nn_idx", "nn_dist"} per query row (indices local to
+    the problem's base rows).
+    """
+    import torch
+
+    pa = _pairs_array(pairs)
+    total_q = int(pa[:, 0].sum()) if len(pa) else 0
+    if q.shape[0] != total_q:
+        raise ValueError(f"q has {q.shape[0]} rows, the pairs {total_q}")
+    out = _batch_outputs(total_q, q.device)
+    s = stream if stream is not None else torch.cuda.current_stream(q.device)
+    check(lib().sift2nn_match_batch(_ptr(q), _ptr(r), r.shape[0], pa.ctypes.data, len(pa), threshold,
+                                    _ptr(out["matches"]), _ptr(out["nn_idx"]), _ptr(out["nn_dist"]), s.cuda_stream),
+          "sift2nn_match_batch")
+    return out
+
+
+class BatchPlan:
+    """A batch bound to (q, r, outputs) and replayed as one CUDA graph."""
+
+    def __init__(self, q, r, pairs, threshold: float = 0.8, tune: bool = True, shape=None):
+        self._pa = _pairs_array(pairs)
+        total_q = int(self._pa[:, 0].sum()) if len(self._pa) else 0
+        if q.shape[0] != total_q:
+            raise ValueError(f"q has {q.shape[0]} rows, the pairs {total_q}")
+        self.q, self.r = q, r
+        self.out = _batch_outputs(total_q, q.device)
+        flags = (SIFT_BATCH_TUNE if tune else 0) | (SIFT_BATCH_SHAPE(shape) if shape is not None else 0)
+        h = ctypes.c_void_p()
+        check(lib().sift_batch_plan_create(_ptr(q), _ptr(r), r.shape[0], self._pa.ctypes.data, len(self._pa),
+                                           threshold, _ptr(self.out["matches"]), _ptr(self.out["nn_idx"]),
+                                           _ptr(self.out["nn_dist"]), flags, ctypes.byref(h)), "sift_batch_plan_create")
+        self._h = h
+
+    def run(self, stream=None):
+        import torch
+
+        s = stream if stream is not None else torch.cuda.current_stream(self.q.device)
+        check(lib().sift_batch_plan_run(self._h, s.cuda_stream), "sift_batch_plan_run")
+        return self.out
+
+    def info(self):
+        qpt, qbuf = ctypes.c_int(), ctypes.c_int()
+        ms = (ctypes.c_float * 3)()
+        check(lib().sift_batch_plan_info(self._h, ctypes.byref(qpt), ctypes.byref(qbuf), ms), "sift_batch_plan_info")
+        return {"qpt": qpt.value, "qbuf": qbuf.value, "tuned_ms": list(ms)}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sift_batch_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_describe(pairs, r_rows: int, qpt: int = 2, workers: int = 74):
+    """Host-side decomposition of a batch (no GPU): units, records, queries,
+    max_splits, grid, group_rows."""
+    pa = _pairs_array(pairs)
+    out = (ctypes.c_longlong * 6)()
+    check(lib().sift_batch_describe(pa.ctypes.data if len(pa) else None, len(pa), r_rows, qpt, workers, out),
+          "sift_batch_describe")
+    return dict(zip(("units", "tiles", "queries", "max_splits", "grid", "group_rows"), list(out)))

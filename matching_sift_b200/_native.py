@@ -47,7 +47,23 @@ _PROTOS = {
                                       ctypes.c_int, ctypes.c_float, _vp, _vp, _vp, _vp]),
     "sift2nn_match_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, _vp, _vp,
                                              _vp, _vp]),
+    "sift2nn_match_batch": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_int, ctypes.c_float, _vp, _vp,
+                                           _vp, _vp]),
+    "sift_batch_plan_create": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_int, ctypes.c_float, _vp, _vp,
+                                              _vp, ctypes.c_int, ctypes.POINTER(_vp)]),
+    "sift_batch_plan_run": (ctypes.c_int, [_vp, _vp]),
+    "sift_batch_plan_info": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_float)]),
+    "sift_batch_plan_destroy": (None, [_vp]),
+    "sift_batch_describe": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_longlong)]),
 }
+
+SIFT_BATCH_TUNE = 1
+
+
+def SIFT_BATCH_SHAPE(k: int) -> int:
+    return (k + 1) << 4
 
 _lib = None
 

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 #include "sift2nn.h"
 #include "api_internal.h"
+#include "context.h"
 #include "exact2nn.cuh"
 #include "pack.cuh"
 #include "lsh.cuh"
@@ -20,27 +21,15 @@
 
 namespace sift {
 
-namespace {
+namespace detail {
 
-constexpr int kMaxDevices = 64;
-// Largest power-of-two scale 2^-s of descriptor values the exact kernels take.
-constexpr int kMaxShift = 24;
 
-struct DeviceCtx {
-    std::mutex mu;
-    bool ready = false;
-    int num_sms = 0;
-    char* arena = nullptr;
-    size_t arena_bytes = 0;
-    int* d_status = nullptr;  // [0] device error code, [1] pack flag / value stats [1..3]
-    int* h_status = nullptr;  // pinned mirror of d_status
-};
 
 DeviceCtx g_ctx[kMaxDevices];
 std::mutex g_init_mu;
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 thread_local int t_last_status = SIFT_OK;
-std::atomic<long long> g_launches{0};
+std::atomic<long long> g_launches{0};  // kernels launched by this library
 // 0: CTA-pair kernels (half inputs searched by the FP16 kernel),
 // 1: single-CTA u8 kernel, 2: CTA-pair u8 kernel for every input type.
 std::atomic<int> g_variant{0};
@@ -48,16 +37,6 @@ std::atomic<bool> g_profile{false};
 std::mutex g_prof_mu;
 std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_prof_events;
 
-// 256-byte aligned bump layout over the arena.
-struct Layout {
-    size_t off = 0;
-    size_t take(size_t bytes) {
-        off = (off + 255) & ~static_cast<size_t>(255);
-        const size_t o = off;
-        off += bytes;
-        return o;
-    }
-};
 
 int ensure_ready(DeviceCtx*& out, int& dev) {
     int n = 0;
@@ -150,12 +129,6 @@ int map_cuda(cudaError_t e) {
     return SIFT_ERR_CUDA;
 }
 
-#define SIFT_TRY(expr)                 \
-    do {                               \
-        int _rc = (expr);              \
-        if (_rc != SIFT_OK) return _rc; \
-    } while (0)
-#define SIFT_CUDA(expr) SIFT_TRY(map_cuda(expr))
 
 // Reads and clears the device status words. Caller has synchronised `st`.
 int collect_device_status(DeviceCtx& c, cudaStream_t st) {
@@ -170,7 +143,9 @@ int collect_device_status(DeviceCtx& c, cudaStream_t st) {
     return SIFT_OK;
 }
 
-}  // namespace
+}  // namespace detail
+
+using namespace detail;
 
 // Largest power-of-two shift needed to make every q and r value (float or
 // half, device-readable) an integer, checked to keep them in [0, 255].

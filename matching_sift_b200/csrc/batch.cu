@@ -1,0 +1,366 @@
+// Batched exact 2-NN: many (query set, base set) problems -- e.g. the two
+// keypoint sets of many image pairs, of uneven sizes -- in ONE persistent
+// launch of the CTA-pair kernel driven by a device work list (WorkItem per
+// problem). The reference matches one image pair per call (cublas_2nn_sift,
+// src/knn_brute.cu:24; its benchmark loops over calls, src/test.cu:194-216);
+// this has no counterpart there.
+//
+// Sequence per batch (one stream): query norms + bounds, base-tile records of
+// every problem, the search kernel over all units, the merge. A plan
+// (sift_batch_plan) owns its device memory, picks the kernel shape with a
+// small autotuner (times each shape on the batch itself) and captures the
+// sequence in a CUDA graph, so a repeated batch of the same sizes (new
+// descriptor values in the same buffers) costs one graph launch.
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <vector>
+#include "api_internal.h"
+#include "context.h"
+#include "exact2nn.cuh"
+
+struct sift_batch_plan {
+    int dev = 0;
+    sift::detail::DeviceCtx* ctx = nullptr;
+    int shape = 0;
+    float tuned_ms[3] = {-1.f, -1.f, -1.f};
+    sift::WorkItem* d_items = nullptr;
+    char* mem = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace sift {
+namespace {
+
+using detail::DeviceCtx;
+
+struct Shape {
+    int qpt, qbuf;
+};
+// Kernel shapes the autotuner chooses from: query tiles per CTA (groups of
+// 512 or 256 queries) and query buffers (2: next group's queries load during
+// the current group's MMAs).
+constexpr Shape kShapes[3] = {{2, 1}, {2, 2}, {1, 2}};
+constexpr int kNumShapes = 3;
+constexpr int kDefaultShape = 1;
+
+std::mutex g_tune_mu;
+std::map<std::array<long long, 4>, int> g_tune_cache;
+
+struct Built {
+    std::vector<WorkItem> items;
+    long long units = 0;
+    int total_tiles = 0, total_q = 0, group_rows = 0;
+    ExactPlan plan{};
+};
+
+int build(const sift_pair* pairs, int n_pairs, uint32_t r_rows, int qpt, int workers, Built& b) {
+    if (n_pairs < 0 || (n_pairs > 0 && !pairs)) return SIFT_ERR_INVALID_ARG;
+    std::vector<int> na(n_pairs), nb(n_pairs), off(n_pairs);
+    long long tq = 0;
+    for (int p = 0; p < n_pairs; ++p) {
+        const sift_pair& s = pairs[p];
+        if (static_cast<uint64_t>(s.r_off) + s.n_r > r_rows) return SIFT_ERR_INVALID_ARG;
+        tq += s.n_q;
+        if (tq > 0x7fffffffLL - 1024 || s.n_r > 0x7fffffffu - 1024) return SIFT_ERR_INVALID_ARG;
+        na[p] = static_cast<int>(s.n_q);
+        nb[p] = static_cast<int>(s.n_r);
+        off[p] = static_cast<int>(s.r_off);
+    }
+    if (r_rows > 0x7fffffffu - 1024) return SIFT_ERR_INVALID_ARG;
+    b.group_rows = 2 * qpt * kBM;
+    b.items.resize(n_pairs);
+    b.units = make_batch_items(n_pairs, na.data(), nb.data(), off.data(), b.group_rows, b.items.data(),
+                               &b.total_tiles, &b.total_q);
+    b.plan = make_batch_plan(b.items.data(), n_pairs, b.units, b.total_q, workers, 2);
+    return SIFT_OK;
+}
+
+std::array<long long, 4> signature(const Built& b) {
+    return {static_cast<long long>(b.items.size()), b.total_q, b.units, b.total_tiles};
+}
+
+struct Buffers {
+    WorkItem* items = nullptr;
+    int32_t* rec = nullptr;
+    int32_t* qnorm = nullptr;
+    int32_t* thresh = nullptr;
+    int4* partial = nullptr;
+};
+
+size_t partial_bytes(const Built& b) {
+    return static_cast<size_t>(b.plan.max_splits) * b.plan.parts * b.plan.q_pad * sizeof(int4);
+}
+
+// Layout of a batch's scratch for the largest of `builds`.
+struct BatchLayout {
+    size_t o_items, o_rec, o_qn, o_thr, o_part, bytes;
+};
+BatchLayout layout_for(const Built* builds, int n) {
+    size_t part = 0;
+    for (int k = 0; k < n; ++k) part = std::max(part, partial_bytes(builds[k]));
+    const Built& b = builds[0];
+    detail::Layout L;
+    BatchLayout o{};
+    o.o_items = L.take(sizeof(WorkItem) * (b.items.size() + 1));
+    o.o_rec = L.take(static_cast<size_t>(b.total_tiles) * kRecInts * 4 + 16);
+    o.o_qn = L.take(static_cast<size_t>(b.plan.q_pad) * 4 + 16);
+    o.o_thr = L.take(static_cast<size_t>(b.plan.q_pad) * 4 + 16);
+    o.o_part = L.take(part + 16);
+    o.bytes = L.off;
+    return o;
+}
+Buffers buffers_at(char* base, const BatchLayout& o) {
+    Buffers m;
+    m.items = reinterpret_cast<WorkItem*>(base + o.o_items);
+    m.rec = reinterpret_cast<int32_t*>(base + o.o_rec);
+    m.qnorm = reinterpret_cast<int32_t*>(base + o.o_qn);
+    m.thresh = reinterpret_cast<int32_t*>(base + o.o_thr);
+    m.partial = reinterpret_cast<int4*>(base + o.o_part);
+    return m;
+}
+
+int enqueue(DeviceCtx& c, const uint8_t* q, const uint8_t* r, uint32_t r_rows, const Built& b, const Buffers& m,
+            Shape sh, float thr, uint32_t* matches, int32_t* nn_idx, float* nn_dist, cudaStream_t st) {
+    if (b.total_q == 0) return SIFT_OK;
+    BatchPlan bp{b.plan, m.items, static_cast<int>(b.items.size()), b.total_tiles, b.group_rows};
+    SIFT_CUDA(launch_row_norms_u8(q, b.total_q, b.plan.q_pad, kMetricL2, m.qnorm, nullptr, m.thresh, st));
+    int launches = 2;
+    if (b.units > 0) {
+        SIFT_CUDA(launch_batch_records(r, static_cast<int>(r_rows), bp, kMetricL2, m.rec, st));
+        CUtensorMap qmap, rmap;
+        SIFT_TRY(detail::encode_u8_rows(&qmap, q, static_cast<uint64_t>(b.total_q), kBM));
+        SIFT_TRY(detail::encode_u8_rows(&rmap, r, r_rows, kBN / 2));
+        SIFT_CUDA(launch_exact2nn_u8_pair_batch(qmap, rmap, m.rec, bp, m.partial, m.thresh, c.d_status, sh.qpt,
+                                                sh.qbuf, st));
+        launches += 2;
+    }
+    SIFT_CUDA(launch_merge2nn_batch(m.partial, bp, b.total_q, m.qnorm, kMetricL2, thr, 1.0f, matches, nullptr, nn_idx,
+                                    nn_dist, st));
+    detail::g_launches += launches;
+    return SIFT_OK;
+}
+
+int check_io(const uint8_t* q, const uint8_t* r, uint32_t r_rows, long long total_q, uint32_t* matches,
+             int32_t* nn_idx, float* nn_dist) {
+    if (total_q > 0 && (!q || (reinterpret_cast<uintptr_t>(q) & 15) || !detail::is_device_accessible(q)))
+        return SIFT_ERR_INVALID_ARG;
+    if (r_rows > 0 && (!r || (reinterpret_cast<uintptr_t>(r) & 15) || !detail::is_device_accessible(r)))
+        return SIFT_ERR_INVALID_ARG;
+    for (const void* o : {static_cast<const void*>(matches), static_cast<const void*>(nn_idx),
+                          static_cast<const void*>(nn_dist)})
+        if (o && total_q > 0 && !detail::is_device_accessible(o)) return SIFT_ERR_INVALID_ARG;
+    return SIFT_OK;
+}
+
+int cached_shape(const Built& b) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(signature(b));
+    return it == g_tune_cache.end() ? kDefaultShape : it->second;
+}
+
+}  // namespace
+
+int match_batch(const uint8_t* q, const uint8_t* r, uint32_t r_rows, const sift_pair* pairs, int n_pairs,
+                float threshold, uint32_t* matches, int32_t* nn_idx, float* nn_dist, void* stream) {
+    DeviceCtx* cp = nullptr;
+    int dev = 0;
+    SIFT_TRY(detail::ensure_ready(cp, dev));
+    DeviceCtx& c = *cp;
+    Built probe;
+    SIFT_TRY(build(pairs, n_pairs, r_rows, 2, c.num_sms / 2, probe));
+    const int shape = cached_shape(probe);
+    Built b;
+    SIFT_TRY(build(pairs, n_pairs, r_rows, kShapes[shape].qpt, c.num_sms / 2, b));
+    SIFT_TRY(check_io(q, r, r_rows, b.total_q, matches, nn_idx, nn_dist));
+    if (b.total_q == 0) return SIFT_OK;
+    std::lock_guard<std::mutex> lk(c.mu);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const BatchLayout o = layout_for(&b, 1);
+    SIFT_TRY(detail::ensure_arena(c, o.bytes));
+    const Buffers m = buffers_at(c.arena, o);
+    if (!b.items.empty())
+        SIFT_CUDA(cudaMemcpyAsync(m.items, b.items.data(), sizeof(WorkItem) * b.items.size(), cudaMemcpyHostToDevice,
+                                  st));
+    return enqueue(c, q, r, r_rows, b, m, kShapes[shape], threshold, matches, nn_idx, nn_dist, st);
+}
+
+int batch_plan_create(const uint8_t* q, const uint8_t* r, uint32_t r_rows, const sift_pair* pairs, int n_pairs,
+                      float threshold, uint32_t* matches, int32_t* nn_idx, float* nn_dist, int flags,
+                      sift_batch_plan** out) {
+    if (!out) return SIFT_ERR_INVALID_ARG;
+    *out = nullptr;
+    DeviceCtx* cp = nullptr;
+    int dev = 0;
+    SIFT_TRY(detail::ensure_ready(cp, dev));
+    DeviceCtx& c = *cp;
+    Built builds[kNumShapes];
+    for (int k = 0; k < kNumShapes; ++k)
+        SIFT_TRY(build(pairs, n_pairs, r_rows, kShapes[k].qpt, c.num_sms / 2, builds[k]));
+    SIFT_TRY(check_io(q, r, r_rows, builds[0].total_q, matches, nn_idx, nn_dist));
+    const int forced = (flags >> 4) & 0xf;  // SIFT_BATCH_SHAPE(k) = (k + 1) << 4
+    if (forced > kNumShapes) return SIFT_ERR_INVALID_ARG;
+
+    sift_batch_plan* P = new (std::nothrow) sift_batch_plan();
+    if (!P) return SIFT_ERR_ALLOC;
+    P->dev = dev;
+    P->ctx = cp;
+    auto fail = [&](int rc) {
+        if (P->exec) cudaGraphExecDestroy(P->exec);
+        if (P->graph) cudaGraphDestroy(P->graph);
+        if (P->mem) cudaFree(P->mem);
+        delete P;
+        return rc;
+    };
+    const BatchLayout o = layout_for(builds, kNumShapes);
+    if (cudaMalloc(&P->mem, o.bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(SIFT_ERR_ALLOC);
+    }
+    const Buffers m = buffers_at(P->mem, o);
+    cudaStream_t cs = nullptr;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return fail(SIFT_ERR_CUDA);
+    auto run_shape = [&](int k) -> int {
+        const Built& b = builds[k];
+        if (!b.items.empty())
+            SIFT_CUDA(cudaMemcpyAsync(m.items, b.items.data(), sizeof(WorkItem) * b.items.size(),
+                                      cudaMemcpyHostToDevice, cs));
+        return enqueue(c, q, r, r_rows, b, m, kShapes[k], threshold, matches, nn_idx, nn_dist, cs);
+    };
+    int rc = SIFT_OK;
+    int shape = forced > 0 ? forced - 1 : cached_shape(builds[0]);
+    if ((flags & SIFT_BATCH_TUNE) && forced == 0 && builds[0].units > 0) {
+        // Autotune: each shape once to warm up, then the best of three timed runs.
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = SIFT_ERR_CUDA;
+        float best = 0.f;
+        for (int k = 0; k < kNumShapes && rc == SIFT_OK; ++k) {
+            rc = run_shape(k);
+            float t_min = 1e30f;
+            for (int rep = 0; rep < 3 && rc == SIFT_OK; ++rep) {
+                if (cudaEventRecord(e0, cs) != cudaSuccess) rc = SIFT_ERR_CUDA;
+                if (rc == SIFT_OK) rc = run_shape(k);
+                float ms = 0.f;
+                if (rc == SIFT_OK && (cudaEventRecord(e1, cs) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                                      cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+                    rc = SIFT_ERR_CUDA;
+                t_min = std::min(t_min, ms);
+            }
+            if (rc == SIFT_OK) {
+                P->tuned_ms[k] = t_min;
+                if (k == 0 || t_min < best) {
+                    best = t_min;
+                    shape = k;
+                }
+            }
+        }
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (rc == SIFT_OK) {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            g_tune_cache[signature(builds[0])] = shape;
+        }
+    }
+    // One plain run of the chosen shape (sets kernel attributes, checks the
+    // device status), then the capture.
+    if (rc == SIFT_OK) rc = run_shape(shape);
+    if (rc == SIFT_OK && cudaStreamSynchronize(cs) != cudaSuccess) rc = SIFT_ERR_CUDA;
+    if (rc == SIFT_OK) {
+        std::lock_guard<std::mutex> lk(c.mu);
+        rc = detail::collect_device_status(c, cs);
+    }
+    if (rc == SIFT_OK) {
+        if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            rc = SIFT_ERR_CUDA;
+        } else {
+            const int erc = enqueue(c, q, r, r_rows, builds[shape], m, kShapes[shape], threshold, matches, nn_idx,
+                                    nn_dist, cs);
+            const cudaError_t ce = cudaStreamEndCapture(cs, &P->graph);
+            rc = erc != SIFT_OK ? erc : detail::map_cuda(ce);
+        }
+    }
+    if (rc == SIFT_OK && cudaGraphInstantiate(&P->exec, P->graph, 0) != cudaSuccess) rc = SIFT_ERR_CUDA;
+    cudaStreamDestroy(cs);
+    if (rc != SIFT_OK) {
+        cudaGetLastError();
+        return fail(rc);
+    }
+    P->shape = shape;
+    *out = P;
+    return SIFT_OK;
+}
+
+int batch_plan_run(sift_batch_plan* P, void* stream) {
+    if (!P || !P->exec) return SIFT_ERR_INVALID_ARG;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev != P->dev) return SIFT_ERR_INVALID_ARG;
+    SIFT_CUDA(cudaGraphLaunch(P->exec, static_cast<cudaStream_t>(stream)));
+    return SIFT_OK;
+}
+
+int batch_plan_info(const sift_batch_plan* P, int* qpt, int* qbuf, float* tuned_ms) {
+    if (!P) return SIFT_ERR_INVALID_ARG;
+    if (qpt) *qpt = kShapes[P->shape].qpt;
+    if (qbuf) *qbuf = kShapes[P->shape].qbuf;
+    if (tuned_ms) std::memcpy(tuned_ms, P->tuned_ms, sizeof(P->tuned_ms));
+    return SIFT_OK;
+}
+
+void batch_plan_destroy(sift_batch_plan* P) {
+    if (!P) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(P->dev);
+    cudaDeviceSynchronize();
+    if (P->exec) cudaGraphExecDestroy(P->exec);
+    if (P->graph) cudaGraphDestroy(P->graph);
+    if (P->mem) cudaFree(P->mem);
+    cudaSetDevice(cur);
+    delete P;
+}
+
+int batch_describe(const sift_pair* pairs, int n_pairs, uint32_t r_rows, int qpt, int workers, long long* out) {
+    if (!out || workers < 1 || (qpt != 1 && qpt != 2)) return SIFT_ERR_INVALID_ARG;
+    Built b;
+    SIFT_TRY(build(pairs, n_pairs, r_rows, qpt, workers, b));
+    out[0] = b.units;
+    out[1] = b.total_tiles;
+    out[2] = b.total_q;
+    out[3] = b.plan.max_splits;
+    out[4] = b.plan.grid;
+    out[5] = b.group_rows;
+    return SIFT_OK;
+}
+
+}  // namespace sift
+
+extern "C" {
+
+int sift2nn_match_batch(const uint8_t* q, const uint8_t* r, uint32_t r_rows, const sift_pair* pairs, int n_pairs,
+                        float threshold, uint32_t* matches, int32_t* nn_idx, float* nn_dist, void* stream) {
+    return sift::match_batch(q, r, r_rows, pairs, n_pairs, threshold, matches, nn_idx, nn_dist, stream);
+}
+
+int sift_batch_plan_create(const uint8_t* q, const uint8_t* r, uint32_t r_rows, const sift_pair* pairs, int n_pairs,
+                           float threshold, uint32_t* matches, int32_t* nn_idx, float* nn_dist, int flags,
+                           sift_batch_plan** plan) {
+    return sift::batch_plan_create(q, r, r_rows, pairs, n_pairs, threshold, matches, nn_idx, nn_dist, flags, plan);
+}
+
+int sift_batch_plan_run(sift_batch_plan* plan, void* stream) { return sift::batch_plan_run(plan, stream); }
+
+int sift_batch_plan_info(const sift_batch_plan* plan, int* qpt, int* qbuf, float* tuned_ms) {
+    return sift::batch_plan_info(plan, qpt, qbuf, tuned_ms);
+}
+
+void sift_batch_plan_destroy(sift_batch_plan* plan) { sift::batch_plan_destroy(plan); }
+
+int sift_batch_describe(const sift_pair* pairs, int n_pairs, uint32_t r_rows, int qpt, int workers, long long* out) {
+    return sift::batch_describe(pairs, n_pairs, r_rows, qpt, workers, out);
+}
+
+}  // extern "C"

@@ -1,0 +1,62 @@
+// Per-device runtime state shared by the host entry points (api.cu,
+// batch.cu): readiness, scratch arena, status words, tensor-map encoding.
+#pragma once
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+#include "sift2nn.h"
+
+namespace sift {
+namespace detail {
+
+constexpr int kMaxDevices = 64;
+// Largest power-of-two scale 2^-s of descriptor values the exact kernels take.
+constexpr int kMaxShift = 24;
+
+struct DeviceCtx {
+    std::mutex mu;            // serialises the calls that use the arena
+    bool ready = false;
+    int num_sms = 0;
+    char* arena = nullptr;    // scratch, grown on demand, reused across calls
+    size_t arena_bytes = 0;
+    int* d_status = nullptr;  // [0] device error code, [1] pack flag / value stats [1..3]
+    int* h_status = nullptr;  // pinned mirror of d_status
+};
+
+// 256-byte aligned bump layout over the arena.
+struct Layout {
+    size_t off = 0;
+    size_t take(size_t bytes) {
+        off = (off + 255) & ~static_cast<size_t>(255);
+        const size_t o = off;
+        off += bytes;
+        return o;
+    }
+};
+
+extern std::atomic<long long> g_launches;
+
+// Context of the current device (initialised on first use; sm_100 only).
+int ensure_ready(DeviceCtx*& out, int& dev);
+// Grows c's arena to at least `bytes` (synchronises the device when it grows).
+int ensure_arena(DeviceCtx& c, size_t bytes);
+bool is_device_accessible(const void* p);
+// u8 rows of 128 bytes: dims {128, rows}, box {128, box_rows}, SWIZZLE_128B.
+int encode_u8_rows(CUtensorMap* m, const void* base, uint64_t rows, uint32_t box_rows);
+int map_cuda(cudaError_t e);
+// Reads and clears the device status words. Caller has synchronised `st`.
+int collect_device_status(DeviceCtx& c, cudaStream_t st);
+
+}  // namespace detail
+}  // namespace sift
+
+#define SIFT_TRY(expr)                  \
+    do {                                \
+        int _rc = (expr);               \
+        if (_rc != SIFT_OK) return _rc; \
+    } while (0)
+#define SIFT_CUDA(expr) SIFT_TRY(::sift::detail::map_cuda(expr))

@@ -137,6 +137,63 @@ __global__ void __launch_bounds__(256) row_norms_kernel(const T* __restrict__ x,
     }
 }
 
+// Largest k with key(items[k]) <= v over a non-decreasing key; empty
+// problems share the key of the problem after them, so the match is the
+// problem that owns v.
+template <typename F>
+__device__ __forceinline__ int find_item(int n_items, long long v, F key) {
+    int lo = 0, hi = n_items - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (key(mid) <= v) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Base-tile records of a batch: block b fills quarter b % 4 of record b / 4;
+// the record belongs to the problem whose record range holds it, and rows of
+// its base set past n_b are padding (norm kKeyPad).
+__global__ void __launch_bounds__(256) batch_records_kernel(const uint8_t* __restrict__ x,
+                                                            const WorkItem* __restrict__ items, int n_items,
+                                                            int metric, int32_t* __restrict__ rec) {
+    const int T = blockIdx.x >> 2, part = blockIdx.x & 3;
+    const int p = find_item(n_items, T, [&](int k) { return static_cast<long long>(items[k].rec_off); });
+    const WorkItem it = items[p];
+    const int local = (T - it.rec_off) * kBN + part * 32 + (threadIdx.x >> 3);
+    const int sub = threadIdx.x & 7;
+    uint32_t s = 0;
+    if (local < it.n_b) {
+        const uint4 w = reinterpret_cast<const uint4*>(x + static_cast<size_t>(it.b_off + local) * kDim)[sub];
+        s = __dp4a(w.x, w.x, 0u);
+        s = __dp4a(w.y, w.y, s);
+        s = __dp4a(w.z, w.z, s);
+        s = __dp4a(w.w, w.w, s);
+    }
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    s += __shfl_xor_sync(0xffffffffu, s, 4);
+    const int32_t v = local < it.n_b ? (metric == kMetricL2 ? static_cast<int32_t>(s) : 0) : kKeyPad;
+    __shared__ int32_t nrm[32];
+    int32_t* r = rec + static_cast<size_t>(T) * kRecInts;
+    if (sub == 0) {
+        nrm[threadIdx.x >> 3] = v;
+        r[part * 32 + (threadIdx.x >> 3)] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        int m = nrm[8 * threadIdx.x];
+        #pragma unroll
+        for (int i = 1; i < 8; ++i) m = min(m, nrm[8 * threadIdx.x + i]);
+        r[128 + part * 4 + threadIdx.x] = m;
+    }
+    if (threadIdx.x == 32) {
+        int m = nrm[0];
+        #pragma unroll
+        for (int i = 1; i < 32; ++i) m = min(m, nrm[i]);
+        r[144 + part] = m;
+    }
+}
+
 __global__ void __launch_bounds__(kThreads, 1)
     exact2nn_u8_kernel(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap bmap,
                        const int32_t* __restrict__ brec, const ExactPlan plan, int4* __restrict__ partial,
@@ -367,18 +424,17 @@ __device__ __forceinline__ bool lex_less(int ka, int ia, int kb, int ib) {
 }
 
 __global__ void __launch_bounds__(256) merge2nn_kernel(const int4* __restrict__ partial, const ExactPlan plan,
+                                                       const WorkItem* __restrict__ items, int n_items,
+                                                       const WorkItem single, int group_rows, int total_q,
                                                        const int32_t* __restrict__ qnorm, int metric, float thr,
                                                        float dscale,
                                                        uint32_t* __restrict__ matches, float4* __restrict__ sorted,
                                                        int32_t* __restrict__ nn_idx, float* __restrict__ nn_dist) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= plan.q_n) return;
+    if (q >= total_q) return;
     const long long W = plan.units, G = plan.grid;
-    const long long BT = plan.base_tiles;
-    const int g = q / (kQT * kBM);
-    // No base rows: no CTA ran and every neighbour is absent.
-    const int c0 = W > 0 ? plan_cta_of(g * BT, W, G) : 0;
-    const int c1 = W > 0 ? plan_cta_of((g + 1) * BT - 1, W, G) : -1;
+    const WorkItem it =
+        items ? items[find_item(n_items, q, [&](int k) { return static_cast<long long>(items[k].a_off); })] : single;
     int a1 = INT_MAX, j1 = -1, a2 = INT_MAX, j2 = -1;
     auto push = [&](int k, int i) {
         if (i < 0) return;
@@ -389,13 +445,21 @@ __global__ void __launch_bounds__(256) merge2nn_kernel(const int4* __restrict__ 
             a2 = k; j2 = i;
         }
     };
-    for (int s = 0; s < (c1 - c0 + 1) * plan.parts; ++s) {
-        const int4 p = partial[static_cast<size_t>(s) * plan.q_pad + q];
-        push(p.x, p.y);
-        push(p.z, p.w);
+    // No base rows: no CTA scanned this query and every neighbour is absent.
+    if (W > 0 && it.tiles > 0) {
+        const long long first = it.u_begin + static_cast<long long>((q - it.a_off) / group_rows) * it.tiles;
+        const int c0 = plan_cta_of(first, W, G);
+        const int c1 = plan_cta_of(first + it.tiles - 1, W, G);
+        for (int s = 0; s < (c1 - c0 + 1) * plan.parts; ++s) {
+            const int4 p = partial[static_cast<size_t>(s) * plan.q_pad + q];
+            push(p.x, p.y);
+            push(p.z, p.w);
+        }
     }
-    const bool v1 = j1 >= 0 && a1 < kKeyPad;
-    const bool v2 = j2 >= 0 && a2 < kKeyPad;
+    // Rows past the problem's base set are padding (they may hold another
+    // problem's rows, but only enter a top-2 when fewer real rows exist).
+    const bool v1 = j1 >= 0 && j1 < it.n_b && a1 < kKeyPad;
+    const bool v2 = j2 >= 0 && j2 < it.n_b && a2 < kKeyPad;
     const int qn = metric == kMetricL2 ? qnorm[q] : 0;
     const float d1 = v1 ? static_cast<float>(a1 + qn) * dscale : FLT_MAX;
     const float d2 = v2 ? static_cast<float>(a2 + qn) * dscale : FLT_MAX;
@@ -492,9 +556,82 @@ cudaError_t launch_merge2nn(const int4* partial, const ExactPlan& plan, const in
                             float threshold, float dist_scale, uint32_t* matches, float4* sorted, int32_t* nn_idx,
                             float* nn_dist, cudaStream_t stream) {
     if (plan.q_n <= 0) return cudaSuccess;
-    merge2nn_kernel<<<(plan.q_n + 255) / 256, 256, 0, stream>>>(partial, plan, qnorm, metric, threshold, dist_scale,
-                                                               matches, sorted, nn_idx, nn_dist);
+    WorkItem single{};
+    single.n_a = plan.q_n;
+    single.n_b = plan.r_n;
+    single.groups = plan.q_groups;
+    single.tiles = plan.base_tiles;
+    merge2nn_kernel<<<(plan.q_n + 255) / 256, 256, 0, stream>>>(partial, plan, nullptr, 1, single, kQT * kBM, plan.q_n,
+                                                               qnorm, metric, threshold, dist_scale, matches, sorted,
+                                                               nn_idx, nn_dist);
     return cudaGetLastError();
+}
+
+cudaError_t launch_merge2nn_batch(const int4* partial, const BatchPlan& bp, int total_queries, const int32_t* qnorm,
+                                  int metric, float threshold, float dist_scale, uint32_t* matches, float4* sorted,
+                                  int32_t* nn_idx, float* nn_dist, cudaStream_t stream) {
+    if (total_queries <= 0) return cudaSuccess;
+    merge2nn_kernel<<<(total_queries + 255) / 256, 256, 0, stream>>>(
+        partial, bp.plan, bp.items, bp.n_items, WorkItem{}, bp.group_rows, total_queries, qnorm, metric, threshold,
+        dist_scale, matches, sorted, nn_idx, nn_dist);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_records(const uint8_t* base, int, const BatchPlan& bp, int metric, int32_t* rec,
+                                 cudaStream_t stream) {
+    if (bp.total_tiles <= 0) return cudaSuccess;
+    batch_records_kernel<<<bp.total_tiles * 4, 256, 0, stream>>>(base, bp.items, bp.n_items, metric, rec);
+    return cudaGetLastError();
+}
+
+long long make_batch_items(int n_items, const int* n_a, const int* n_b, const int* b_off, int group_rows,
+                           WorkItem* items, int* total_tiles, int* total_queries) {
+    long long u = 0;
+    int a = 0, rec = 0;
+    for (int p = 0; p < n_items; ++p) {
+        WorkItem& it = items[p];
+        it = WorkItem{};
+        it.a_off = a;
+        it.n_a = n_a[p];
+        it.b_off = b_off[p];
+        it.n_b = n_b[p];
+        it.groups = (n_a[p] + group_rows - 1) / group_rows;
+        it.tiles = (n_b[p] + kBN - 1) / kBN;
+        it.u_begin = u;
+        it.rec_off = rec;
+        u += static_cast<long long>(it.groups) * it.tiles;
+        rec += it.tiles;
+        a += n_a[p];
+    }
+    if (total_tiles) *total_tiles = rec;
+    if (total_queries) *total_queries = a;
+    return u;
+}
+
+ExactPlan make_batch_plan(const WorkItem* items, int n_items, long long units, int total_queries, int num_workers,
+                          int parts) {
+    ExactPlan p{};
+    p.parts = parts;
+    p.q_n = total_queries;
+    p.r_n = 0;
+    p.q_tiles = (total_queries + kBM - 1) / kBM;
+    p.q_pad = p.q_tiles * kBM;
+    p.units = units;
+    p.grid = static_cast<int>(std::min<long long>(num_workers, units));
+    int ms = 1;
+    if (p.grid > 0) {
+        for (int k = 0; k < n_items; ++k) {
+            const WorkItem& it = items[k];
+            for (int g = 0; g < it.groups && it.tiles > 0; ++g) {
+                const long long first = it.u_begin + static_cast<long long>(g) * it.tiles;
+                const int c0 = plan_cta_of(first, units, p.grid);
+                const int c1 = plan_cta_of(first + it.tiles - 1, units, p.grid);
+                ms = std::max(ms, c1 - c0 + 1);
+            }
+        }
+    }
+    p.max_splits = ms;
+    return p;
 }
 
 }  // namespace sift

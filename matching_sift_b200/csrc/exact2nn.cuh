@@ -54,6 +54,43 @@ __host__ __device__ inline int plan_cta_of(long long w, long long W, long long G
     return static_cast<int>(((w + 1) * G - 1) / W);
 }
 
+// One (query set, base set) problem of a batch searched by one launch of the
+// CTA-pair kernels. Query sets are consecutive row ranges of one query tensor
+// (a_off = rows of the problems before it); base sets are any row ranges of
+// one base tensor. Units of problem p: groups x tiles, numbered from u_begin;
+// its base-tile records start at rec_off. A single search is the batch of one
+// problem {0, q_n, 0, r_n, 0, q_groups, base_tiles, 0}.
+struct WorkItem {
+    int a_off, n_a;
+    int b_off, n_b;
+    long long u_begin;
+    int groups, tiles;
+    int rec_off;
+    int pad_;
+};
+static_assert(sizeof(WorkItem) == 40, "WorkItem layout");
+
+// Batch plan: items[] in device memory, plan.units = sum of all units,
+// plan.q_pad = query capacity (>= total query rows, multiple of kBM),
+// plan.max_splits over every query group of every problem.
+struct BatchPlan {
+    ExactPlan plan;
+    const WorkItem* items;   // device
+    int n_items;
+    int total_tiles;         // records
+    int group_rows;          // queries per query group
+};
+
+// Builds the work items of a batch on the host. n_a[p], n_b[p], b_off[p]:
+// sizes and base-row offsets of the problems (a_off is the sum of the n_a
+// before p); group_rows: queries per group (512 or 256). Returns total units.
+long long make_batch_items(int n_items, const int* n_a, const int* n_b, const int* b_off, int group_rows,
+                           WorkItem* items, int* total_tiles, int* total_queries);
+// The plan of a batch: units, grid, q_pad (query capacity) and max_splits over
+// every query group of every problem.
+ExactPlan make_batch_plan(const WorkItem* items, int n_items, long long units, int total_queries, int num_workers,
+                          int parts);
+
 // num_workers: persistent CTAs (or CTA pairs); parts: partial top-2 lists
 // each worker writes per query (one per disjoint column slice it scans).
 ExactPlan make_exact_plan(int q_n, int r_n, int num_workers, int parts);
@@ -85,6 +122,22 @@ cudaError_t launch_exact2nn_u8(const CUtensorMap& qmap, const CUtensorMap& bmap,
 cudaError_t launch_exact2nn_u8_pair(const CUtensorMap& qmap, const CUtensorMap& bmap_half, const int32_t* brec,
                                     const ExactPlan& plan, int4* partial, int32_t* thresh, int* err,
                                     cudaStream_t stream);
+// The same kernel over a batch (items in device memory). qpt: query tiles per
+// CTA (2: query groups of 512 rows, 1: groups of 256 rows; the items must be
+// made with the same group size); qbuf: query buffers (1 or 2). Shapes built:
+// (2, 1), (2, 2), (1, 2).
+cudaError_t launch_exact2nn_u8_pair_batch(const CUtensorMap& qmap, const CUtensorMap& bmap_half, const int32_t* brec,
+                                          const BatchPlan& bp, int4* partial, int32_t* thresh, int* err, int qpt,
+                                          int qbuf, cudaStream_t stream);
+// Base-tile records of every problem of a batch (rows of base set p past
+// n_b[p] are padding), total_tiles records.
+cudaError_t launch_batch_records(const uint8_t* base, int base_rows, const BatchPlan& bp, int metric, int32_t* rec,
+                                 cudaStream_t stream);
+// Merge for a batch: query row q belongs to the problem whose range holds it;
+// indices are local to the problem's base set.
+cudaError_t launch_merge2nn_batch(const int4* partial, const BatchPlan& bp, int total_queries, const int32_t* qnorm,
+                                  int metric, float threshold, float dist_scale, uint32_t* matches, float4* sorted,
+                                  int32_t* nn_idx, float* nn_dist, cudaStream_t stream);
 // FP16 rows (bmap_half / qmap: half tensor maps with boxes of 64 elements):
 // values are integers times 2^-s and dscale = 2^(2s) turns the f32 dot
 // products back into integers (brec built from the same integers).

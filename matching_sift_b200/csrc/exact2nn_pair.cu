@@ -11,16 +11,23 @@
 // accumulator buffers per query tile, so the MMA of the next base tile runs
 // while the epilogue is still scanning the previous one.
 //
-// Per CTA: 2 query tiles x 128 rows (a work group of the pair = 512 queries,
-// the same grouping as the single-CTA kernel), TMEM 4 slots x 128 columns =
-// (query tile, buffer); unit n uses buffer n % 2.
+// Per CTA: QPT query tiles x 128 rows (a work group of the pair = 2 * QPT
+// * 128 queries; QPT = 2 gives the single-CTA kernel's groups of 512), TMEM
+// 2 * QPT slots x 128 columns = (query tile, buffer); unit n uses buffer n % 2.
+// QB query buffers: with 2 the next group's queries load while the current
+// group's MMAs run (batches of small problems change groups often).
 //
-// Warp roles (kPThreads = 576 per CTA):
+// Work: a list of problems (WorkItem: query rows, base rows, unit range); a
+// single search is a list of one. Units (problem, query group, base tile) are
+// numbered problem by problem and every CTA pair owns a contiguous range; all
+// roles walk the same range with a Cursor.
+//
+// Warp roles (64 + 32 * 8 * QPT threads per CTA):
 //   warp 0       TMA producer (both CTAs): its own query rows, its half of
 //                each base tile (completion counted on the leader's barrier)
 //                and the full norms record of the tile (local barrier)
 //   warp 1       TMEM allocator (both CTAs); MMA issuer (leader CTA only)
-//   warps 2..17  epilogue (both CTAs): warp w owns query tile (w - 2) / 8,
+//   warps 2..    epilogue (both CTAs): warp w owns query tile (w - 2) / 8,
 //                buffer ((w - 2) / 4) % 2 (so it scans every other unit, all
 //                128 columns) and TMEM lane quarter w % 4
 //
@@ -36,14 +43,14 @@
 //   sfree[s]   the 8 epilogue warps that scanned stage s's unit are
 //              done: its MMAs completed (they waited on tfull) and its
 //              record is no longer read (per CTA)                  arrive
-//   qfull      (L) query tiles of both CTAs landed                  TMA tx
-//   qempty     MMAs of the current query group done (both CTAs)     commit, multicast
+//   qfull[b]   (L) query tiles of both CTAs landed in buffer b      TMA tx
+//   qempty[b]  MMAs of the group in query buffer b done (both CTAs) commit, multicast
 //   tfull[b]   both query tiles' accumulators of buffer b done      commit, multicast
 //   tempty[b]  (L) the 8 warps of buffer b in each CTA read it      remote arrive
 // Every wait is bounded (2 s); an expired wait raises the CTA's abort flag
 // and records an error code, and every role still reaches the teardown.
 //
-// Two instantiations of one body:
+// Instantiations of one body:
 //   exact2nn_u8_pair_kernel   u8 rows (128 B), kind::i8, s32 accumulators,
 //                             4 MMAs of K = 32 per 128 x 128 tile product
 //   exact2nn_f16_pair_kernel  FP16 rows (256 B = two 128-byte K blocks, each
@@ -58,6 +65,8 @@
 //                             into the same integer dot products as the u8
 //                             kernel (times dscale = 2^2s, rounded) and the
 //                             rest is shared.
+//   exact2nn_u8_pair_batch_kernel<QPT, QB>  u8 batches with the shapes the
+//                             batch autotuner chooses from.
 #include <climits>
 #include "exact2nn.cuh"
 #include "ptx.cuh"
@@ -67,21 +76,15 @@ namespace sift {
 
 namespace {
 
-constexpr int kPQT = 2;                          // query tiles per CTA
 constexpr int kPHalf = kBN / 2;                  // base rows loaded per CTA per unit
 constexpr int kPRecBytes = kRecInts * 4;         // 640 B
-constexpr int kPSlots = 2 * kPQT;                // (query tile, buffer)
-constexpr int kPEpiWarps = 16;
-constexpr int kPThreads = 64 + 32 * kPEpiWarps;
-constexpr int kPTmemCols = kPSlots * kBN;        // 512
 constexpr uint16_t kPairMask = 0x3;
-static_assert(kPEpiWarps == 4 * kPSlots, "one epilogue warp per (slot, lane quarter)");
-static_assert(kPQT * 2 * kBM == kQT * kBM, "a pair covers one query group");
+constexpr size_t kPSmemBudget = 225 * 1024;
 
-// Shapes of one element type. A row of 128 elements is kKBlocks blocks of
+// Shapes of one instantiation. A row of 128 elements is kKBlocks blocks of
 // 128 bytes; each block of a tile is stored as its own SW128 K-major tile
 // (rows x 128 B), and every MMA consumes 32 bytes of K.
-template <bool F16>
+template <bool F16, int QPT, int QB>
 struct PairCfg {
     static constexpr int kElemBytes = F16 ? 2 : 1;
     static constexpr int kKBlocks = F16 ? 2 : 1;
@@ -89,13 +92,20 @@ struct PairCfg {
     static constexpr int kQKBlock = kBM * 128;               // bytes of one K block of a query tile
     static constexpr int kBKBlock = kPHalf * 128;            // bytes of one K block of a base half
     static constexpr int kQTileBytes = kKBlocks * kQKBlock;  // 16 / 32 KB
+    static constexpr int kQBufBytes = QPT * kQTileBytes;
     static constexpr int kBHalfBytes = kKBlocks * kBKBlock;  // 8 / 16 KB
-    static constexpr int kStages = F16 ? 8 : 12;
+    static constexpr int kSlots = 2 * QPT;                   // (query tile, buffer)
+    static constexpr int kEpiWarps = 4 * kSlots;             // one per (slot, lane quarter)
+    static constexpr int kThreads = 64 + 32 * kEpiWarps;
+    static constexpr int kTmemCols = kSlots * kBN;
+    static constexpr int kStagesFit =
+        static_cast<int>((kPSmemBudget - 1024 - 512 - QB * kQBufBytes) / (kBHalfBytes + kPRecBytes));
+    static constexpr int kStages = kStagesFit < 12 ? kStagesFit : 12;
     struct __align__(8) Ctl {
         uint64_t full[kStages];
         uint64_t rfull[kStages];
         uint64_t sfree[kStages];
-        uint64_t qfull, qempty;
+        uint64_t qfull[QB], qempty[QB];
         uint64_t tfull[2], tempty[2];
         uint64_t drain;
         uint32_t tmem_base;
@@ -103,30 +113,79 @@ struct PairCfg {
         int no_abort;
     };
     static constexpr size_t kSmemBytes =
-        1024 + kPQT * kQTileBytes + kStages * kBHalfBytes + kStages * kPRecBytes + sizeof(Ctl);
+        1024 + QB * kQBufBytes + kStages * kBHalfBytes + kStages * kPRecBytes + sizeof(Ctl);
     // M = 256 (the pair), N = kBN; s32 accumulators for u8 x u8, f32 for f16 x f16.
     static constexpr uint32_t kIdesc =
         F16 ? ptx::idesc_make(1 /*F32*/, 0 /*F16*/, 0 /*F16*/, 2 * kBM, kBN)
             : ptx::idesc_make(2 /*S32*/, 0 /*u8*/, 0 /*u8*/, 2 * kBM, kBN);
+    static_assert(kStages >= 4, "base ring too shallow");
+    static_assert(kSmemBytes <= 227 * 1024, "shared memory");
+    static_assert(kSmemBytes <= kPSmemBudget + 1024, "shared memory budget");
 };
-static_assert(PairCfg<true>::kSmemBytes <= 227 * 1024, "FP16 pair kernel shared memory");
-static_assert(PairCfg<false>::kSmemBytes <= 227 * 1024, "u8 pair kernel shared memory");
 
-template <bool F16>
+// Walks a CTA pair's contiguous unit range over the work items.
+struct Cursor {
+    const WorkItem* items;  // device list, or null for the single item `it`
+    int n_items;
+    WorkItem it;            // current problem
+    int p, g, j;            // problem, query group, base tile
+
+    __device__ __forceinline__ void init(const WorkItem* list, int n, const WorkItem& single, long long w) {
+        items = list;
+        n_items = n;
+        p = 0;
+        if (list) {
+            int lo = 0, hi = n - 1;  // largest p with u_begin <= w (empty items share the next one's u_begin)
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (list[mid].u_begin <= w) lo = mid; else hi = mid - 1;
+            }
+            p = lo;
+            it = list[p];
+        } else {
+            it = single;
+        }
+        const long long r = w - it.u_begin;
+        g = it.tiles > 0 ? static_cast<int>(r / it.tiles) : 0;
+        j = static_cast<int>(r - static_cast<long long>(g) * it.tiles);
+    }
+    __device__ __forceinline__ bool last_of_group() const { return j + 1 == it.tiles; }
+    // One unit forward; true when the next unit opens a query group.
+    __device__ __forceinline__ bool next() {
+        if (++j < it.tiles) return false;
+        j = 0;
+        if (++g < it.groups) return true;
+        g = 0;
+        if (items) {
+            while (++p < n_items) {
+                it = items[p];
+                if (it.groups > 0 && it.tiles > 0) break;
+            }
+        }
+        return true;
+    }
+    __device__ __forceinline__ long long group_first_unit() const {
+        return it.u_begin + static_cast<long long>(g) * it.tiles;
+    }
+};
+
+template <bool F16, int QPT, int QB>
 __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtensorMap& bmap,
                                           const int32_t* __restrict__ brec, const ExactPlan& plan,
+                                          const WorkItem* __restrict__ items, int n_items, const WorkItem& single,
                                           int4* __restrict__ partial, int32_t* __restrict__ thresh,
                                           int* __restrict__ err, float dscale) {
-    using Cfg = PairCfg<F16>;
+    using Cfg = PairCfg<F16, QPT, QB>;
     constexpr int kPStages = Cfg::kStages;
     constexpr int kPQTileBytes = Cfg::kQTileBytes;
     constexpr int kPBHalfBytes = Cfg::kBHalfBytes;
+    constexpr int kPEpiWarps = Cfg::kEpiWarps;
     using PairCtl = typename Cfg::Ctl;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw_u32 = ptx::smem_u32(smem_raw);
     uint8_t* smem = smem_raw + ((1024u - (raw_u32 & 1023u)) & 1023u);
     uint8_t* q_smem = smem;
-    uint8_t* b_smem = smem + kPQT * kPQTileBytes;
+    uint8_t* b_smem = smem + QB * Cfg::kQBufBytes;
     int32_t* r_smem = reinterpret_cast<int32_t*>(b_smem + kPStages * kPBHalfBytes);
     PairCtl* ctl = reinterpret_cast<PairCtl*>(r_smem + kPStages * kRecInts);
     const uint32_t q_s = ptx::smem_u32(q_smem);
@@ -142,15 +201,12 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
     const long long G = plan.grid;  // pairs
     const long long w_begin = plan_w0(pair, W, G);
     const int n_units = static_cast<int>(plan_w0(pair + 1, W, G) - w_begin);
-    const int BT = plan.base_tiles;
-    const int g_begin = static_cast<int>(w_begin / BT);
-    const int j_begin = static_cast<int>(w_begin - static_cast<long long>(g_begin) * BT);
 
     const uint32_t bar_full = ptx::smem_u32(&ctl->full[0]);
     const uint32_t bar_rfull = ptx::smem_u32(&ctl->rfull[0]);
     const uint32_t bar_sfree = ptx::smem_u32(&ctl->sfree[0]);
-    const uint32_t bar_qfull = ptx::smem_u32(&ctl->qfull);
-    const uint32_t bar_qempty = ptx::smem_u32(&ctl->qempty);
+    const uint32_t bar_qfull = ptx::smem_u32(&ctl->qfull[0]);
+    const uint32_t bar_qempty = ptx::smem_u32(&ctl->qempty[0]);
     const uint32_t bar_tfull = ptx::smem_u32(&ctl->tfull[0]);
     const uint32_t bar_tempty = ptx::smem_u32(&ctl->tempty[0]);
     const uint32_t bar_drain = ptx::smem_u32(&ctl->drain);
@@ -161,11 +217,13 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
             ptx::mbar_init(bar_rfull + 8 * s, 1);
             ptx::mbar_init(bar_sfree + 8 * s, kPEpiWarps / 2);
         }
-        ptx::mbar_init(bar_qfull, 1);
-        ptx::mbar_init(bar_qempty, 1);
+        for (int b = 0; b < QB; ++b) {
+            ptx::mbar_init(bar_qfull + 8 * b, 1);
+            ptx::mbar_init(bar_qempty + 8 * b, 1);
+        }
         for (int b = 0; b < 2; ++b) {
             ptx::mbar_init(bar_tfull + 8 * b, 1);
-            ptx::mbar_init(bar_tempty + 8 * b, 2 * kPEpiWarps / 2);  // 8 warps of buffer b in each CTA
+            ptx::mbar_init(bar_tempty + 8 * b, 2 * kPEpiWarps / 2);  // the warps of buffer b in each CTA
         }
         ptx::mbar_init(bar_drain, 1);
         ctl->abort_flag = 0;
@@ -173,7 +231,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
         ptx::fence_mbar_init();
     }
     if (warp == 1) {
-        ptx::tmem_alloc_pair(ptx::smem_u32(&ctl->tmem_base), kPTmemCols);
+        ptx::tmem_alloc_pair(ptx::smem_u32(&ctl->tmem_base), Cfg::kTmemCols);
         ptx::tmem_relinquish_pair();
     }
     ptx::tc_fence_before();
@@ -185,6 +243,9 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
     volatile int* abort_flag = &ctl->abort_flag;
     volatile int* never = &ctl->no_abort;
 
+    Cursor cur;
+    if (n_units > 0) cur.init(items, n_items, single, w_begin);
+
     if (warp == 0) {
         if (lane == 0) {
             // ------------------------------------------------ TMA producer
@@ -192,64 +253,68 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
             ptx::tma_prefetch_desc(&bmap);
             const uint32_t lead_qfull = ptx::mapa(bar_qfull, 0);
             const uint32_t lead_full = ptx::mapa(bar_full, 0);
-            int cur_g = -1, ngroups = 0;
-            int g = g_begin, j = j_begin;
+            int ngroups = 0;
+            bool new_group = true;
             int n = 0;
             for (; n < n_units; ++n) {
-                if (g != cur_g) {
-                    if (ngroups > 0 &&
-                        !ptx::mbar_wait_cluster(bar_qempty, (ngroups - 1) & 1, abort_flag, err, kErrWaitQuery))
+                if (new_group) {
+                    const int qb = ngroups % QB;
+                    if (ngroups >= QB && !ptx::mbar_wait_cluster(bar_qempty + 8 * qb, ((ngroups / QB) - 1) & 1,
+                                                                 abort_flag, err, kErrWaitQuery))
                         break;
-                    if (leader) ptx::mbar_arrive_expect_tx(bar_qfull, 2 * kPQT * kPQTileBytes);
-                    for (int t = 0; t < kPQT; ++t) {
+                    if (leader) ptx::mbar_arrive_expect_tx(bar_qfull + 8 * qb, 2 * Cfg::kQBufBytes);
+                    for (int t = 0; t < QPT; ++t) {
+                        const int row = cur.it.a_off + ((cur.g * QPT + t) * 2 + static_cast<int>(rank)) * kBM;
                         #pragma unroll
                         for (int kb = 0; kb < Cfg::kKBlocks; ++kb)
-                            ptx::tma_load_2d_pair(q_s + t * kPQTileBytes + kb * Cfg::kQKBlock, &qmap,
-                                                  kb * Cfg::kBoxElems,
-                                                  ((g * kPQT + t) * 2 + static_cast<int>(rank)) * kBM, lead_qfull);
+                            ptx::tma_load_2d_pair(q_s + qb * Cfg::kQBufBytes + t * kPQTileBytes + kb * Cfg::kQKBlock,
+                                                  &qmap, kb * Cfg::kBoxElems, row, lead_qfull + 8 * qb);
                     }
-                    cur_g = g;
                     ++ngroups;
                 }
                 const int s = n % kPStages;
                 if (!ptx::mbar_wait(bar_sfree + 8 * s, ((n / kPStages) & 1) ^ 1, abort_flag, err, kErrWaitProducer))
                     break;
                 if (leader) ptx::mbar_arrive_expect_tx(bar_full + 8 * s, 2 * kPBHalfBytes);
+                const int brow = cur.it.b_off + cur.j * kBN + static_cast<int>(rank) * kPHalf;
                 #pragma unroll
                 for (int kb = 0; kb < Cfg::kKBlocks; ++kb)
                     ptx::tma_load_2d_pair(b_s + s * kPBHalfBytes + kb * Cfg::kBKBlock, &bmap, kb * Cfg::kBoxElems,
-                                          j * kBN + static_cast<int>(rank) * kPHalf, lead_full + 8 * s);
+                                          brow, lead_full + 8 * s);
                 ptx::mbar_arrive_expect_tx(bar_rfull + 8 * s, kPRecBytes);
-                ptx::bulk_load(r_s + s * kPRecBytes, brec + static_cast<size_t>(j) * kRecInts, kPRecBytes,
-                               bar_rfull + 8 * s);
-                if (++j == BT) { j = 0; ++g; }
+                ptx::bulk_load(r_s + s * kPRecBytes, brec + static_cast<size_t>(cur.it.rec_off + cur.j) * kRecInts,
+                               kPRecBytes, bar_rfull + 8 * s);
+                new_group = cur.next();
             }
             // Drain: this CTA's copies land before it may exit. Records are
             // counted locally; base halves are consumed once the epilogue
-            // has released the stage.
+            // has released the stage; query buffers once their MMAs are done.
             for (int k = (n > kPStages ? n - kPStages : 0); k < n; ++k) {
                 ptx::mbar_wait(bar_rfull + 8 * (k % kPStages), (k / kPStages) & 1, never, err, kErrWaitDrain);
                 ptx::mbar_wait(bar_sfree + 8 * (k % kPStages), (k / kPStages) & 1, never, err, kErrWaitDrain);
             }
-            if (ngroups > 0)
-                ptx::mbar_wait_cluster(bar_qempty, (ngroups - 1) & 1, never, err, kErrWaitDrain);
+            for (int k = (ngroups > QB ? ngroups - QB : 0); k < ngroups; ++k)
+                ptx::mbar_wait_cluster(bar_qempty + 8 * (k % QB), (k / QB) & 1, never, err, kErrWaitDrain);
         }
         __syncwarp();
     } else if (warp == 1) {
         if (lane == 0 && leader) {
             // -------------------------------------------------- MMA issuer
             constexpr uint32_t idesc = Cfg::kIdesc;
-            const uint64_t a_desc0 = ptx::sdesc_sw128(q_s);
             const uint64_t b_desc0 = ptx::sdesc_sw128(b_s);
-            int cur_g = -1, ngroups = 0;
-            int g = g_begin, j = j_begin;
+            int ngroups = 0;
+            bool new_group = true;
+            uint64_t a_desc0 = ptx::sdesc_sw128(q_s);
+            int qb = 0;
             // Barrier tests of unit n issued while unit n - 1's MMAs are issued.
             bool pre_full = ptx::mbar_try_wait(bar_full, 0);
             bool pre_tempty = ptx::mbar_try_wait(bar_tempty, 1);
             for (int n = 0; n < n_units; ++n) {
-                if (g != cur_g) {
-                    if (!ptx::mbar_wait_cluster(bar_qfull, ngroups & 1, abort_flag, err, kErrWaitQuery)) break;
-                    cur_g = g;
+                if (new_group) {
+                    qb = ngroups % QB;
+                    if (!ptx::mbar_wait_cluster(bar_qfull + 8 * qb, (ngroups / QB) & 1, abort_flag, err, kErrWaitQuery))
+                        break;
+                    a_desc0 = ptx::sdesc_sw128(q_s + qb * Cfg::kQBufBytes);
                     ++ngroups;
                 }
                 const int s = n % kPStages;
@@ -263,7 +328,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                 ptx::tc_fence_after();
                 const uint64_t b_desc = b_desc0 + static_cast<uint64_t>((s * kPBHalfBytes) >> 4);
                 #pragma unroll
-                for (int t = 0; t < kPQT; ++t) {
+                for (int t = 0; t < QPT; ++t) {
                     const uint32_t d = tmem + (t * 2 + buf) * kBN;
                     #pragma unroll
                     for (int kb = 0; kb < Cfg::kKBlocks; ++kb) {
@@ -281,14 +346,13 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                     }
                 }
                 ptx::tc_commit_pair_mc(bar_tfull + 8 * buf, kPairMask);
-                const bool last_of_group = (n + 1 == n_units) || (j + 1 == BT);
-                if (last_of_group) ptx::tc_commit_pair_mc(bar_qempty, kPairMask);
+                if (n + 1 == n_units || cur.last_of_group()) ptx::tc_commit_pair_mc(bar_qempty + 8 * qb, kPairMask);
                 // Test the barriers of unit n + 1 now, behind this unit's queued MMAs.
                 if (n + 1 < n_units) {
                     pre_full = ptx::mbar_try_wait(bar_full + 8 * ((n + 1) % kPStages), ((n + 1) / kPStages) & 1);
                     pre_tempty = ptx::mbar_try_wait(bar_tempty + 8 * (buf ^ 1), (((n + 1) >> 1) & 1) ^ 1);
                 }
-                if (++j == BT) { j = 0; ++g; }
+                new_group = cur.next();
             }
             // Drain: all issued MMAs complete before TMEM is released.
             ptx::tc_commit_pair(bar_drain);
@@ -305,25 +369,27 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
         const uint32_t lead_tempty = ptx::mapa(bar_tempty + 8 * buf, 0);
         Top2 st{INT_MAX, -1, INT_MAX, -1, INT_MAX};
         int published = INT_MAX;
-        int cur_g = -1, split = 0, q = 0;
-        bool active = false;
-        int g = g_begin, j = j_begin;
+        int split = 0, q = 0;
+        bool active = false, valid = false, open = false;
+        bool new_group = true;
 
         for (int n = 0; n < n_units; ++n) {
-            if (g != cur_g) {
-                if (cur_g >= 0 && active)
+            if (new_group) {
+                if (open && valid)
                     partial[(static_cast<size_t>(split) * 2 + buf) * plan.q_pad + q] =
                         make_int4(st.k1, st.i1, st.k2, st.i2);
                 st = Top2{INT_MAX, -1, INT_MAX, -1, INT_MAX};
                 published = INT_MAX;
-                cur_g = g;
-                const int tile = (g * kPQT + t) * 2 + static_cast<int>(rank);
-                active = tile < plan.q_tiles;
-                split = pair - plan_cta_of(static_cast<long long>(g) * BT, W, G);
-                q = tile * kBM + quarter * 32 + lane;
+                open = true;
+                const int q_local = ((cur.g * QPT + t) * 2 + static_cast<int>(rank)) * kBM + quarter * 32 + lane;
+                valid = q_local < cur.it.n_a;
+                active = __any_sync(0xffffffffu, valid);
+                split = pair - plan_cta_of(cur.group_first_unit(), W, G);
+                q = cur.it.a_off + q_local;
             }
+            const int j = cur.j;
             if ((n & 1) == buf) {
-                const int shared_thr = active ? __ldcg(thresh + q) : INT_MAX;
+                const int shared_thr = valid ? __ldcg(thresh + q) : INT_MAX;
                 const int s = n % kPStages;
                 const uint32_t rpar = (n / kPStages) & 1, tpar = (static_cast<uint32_t>(n) >> 1) & 1;
                 // Both tests are issued back to back so their latencies overlap.
@@ -360,7 +426,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                     __syncwarp();
                     if (lane == 0) ptx::mbar_arrive_cluster_relaxed(lead_tempty);
                     scan_group(va, row0 + 96, gm.w, rec + 96, rec + 140, st);
-                    if (st.k2 < published) {
+                    if (valid && st.k2 < published) {
                         atomicMin(thresh + q, st.k2);
                         published = st.k2;
                     }
@@ -372,9 +438,9 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                 __syncwarp();
                 if (lane == 0) ptx::mbar_arrive(bar_sfree + 8 * s);
             }
-            if (++j == BT) { j = 0; ++g; }
+            new_group = cur.next();
         }
-        if (cur_g >= 0 && active)
+        if (open && valid)
             partial[(static_cast<size_t>(split) * 2 + buf) * plan.q_pad + q] = make_int4(st.k1, st.i1, st.k2, st.i2);
     }
 
@@ -385,22 +451,35 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
     ptx::cluster_sync();
     if (warp == 1) {
         ptx::tc_fence_after();
-        ptx::tmem_dealloc_pair(tmem, kPTmemCols);
+        ptx::tmem_dealloc_pair(tmem, Cfg::kTmemCols);
     }
 }
 
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
+using CfgU8 = PairCfg<false, 2, 1>;
+using CfgF16 = PairCfg<true, 2, 1>;
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CfgU8::kThreads, 1)
     exact2nn_u8_pair_kernel(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap bmap,
-                            const int32_t* __restrict__ brec, const ExactPlan plan, int4* __restrict__ partial,
-                            int32_t* __restrict__ thresh, int* __restrict__ err) {
-    pair_body<false>(qmap, bmap, brec, plan, partial, thresh, err, 1.0f);
+                            const int32_t* __restrict__ brec, const ExactPlan plan, const WorkItem single,
+                            int4* __restrict__ partial, int32_t* __restrict__ thresh, int* __restrict__ err) {
+    pair_body<false, 2, 1>(qmap, bmap, brec, plan, nullptr, 1, single, partial, thresh, err, 1.0f);
 }
 
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kPThreads, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CfgF16::kThreads, 1)
     exact2nn_f16_pair_kernel(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap bmap,
-                             const int32_t* __restrict__ brec, const ExactPlan plan, int4* __restrict__ partial,
-                             int32_t* __restrict__ thresh, int* __restrict__ err, float dscale) {
-    pair_body<true>(qmap, bmap, brec, plan, partial, thresh, err, dscale);
+                             const int32_t* __restrict__ brec, const ExactPlan plan, const WorkItem single,
+                             int4* __restrict__ partial, int32_t* __restrict__ thresh, int* __restrict__ err,
+                             float dscale) {
+    pair_body<true, 2, 1>(qmap, bmap, brec, plan, nullptr, 1, single, partial, thresh, err, dscale);
+}
+
+template <int QPT, int QB>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairCfg<false, QPT, QB>::kThreads, 1)
+    exact2nn_u8_pair_batch_kernel(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap bmap,
+                                  const int32_t* __restrict__ brec, const ExactPlan plan,
+                                  const WorkItem* __restrict__ items, int n_items, int4* __restrict__ partial,
+                                  int32_t* __restrict__ thresh, int* __restrict__ err) {
+    pair_body<false, QPT, QB>(qmap, bmap, brec, plan, items, n_items, WorkItem{}, partial, thresh, err, 1.0f);
 }
 
 template <typename K>
@@ -416,19 +495,45 @@ cudaError_t set_smem_once(K kernel, size_t bytes, bool (&done)[64]) {
     return cudaSuccess;
 }
 
+WorkItem single_item(const ExactPlan& plan) {
+    WorkItem w{};
+    w.a_off = 0;
+    w.n_a = plan.q_n;
+    w.b_off = 0;
+    w.n_b = plan.r_n;
+    w.u_begin = 0;
+    w.groups = plan.q_groups;
+    w.tiles = plan.base_tiles;
+    w.rec_off = 0;
+    return w;
+}
+
+template <int QPT, int QB>
+cudaError_t launch_batch_variant(const CUtensorMap& qmap, const CUtensorMap& bmap, const int32_t* brec,
+                                 const BatchPlan& bp, int4* partial, int32_t* thresh, int* err, cudaStream_t stream) {
+    using Cfg = PairCfg<false, QPT, QB>;
+    static bool attr_set[64] = {};
+    cudaError_t e = set_smem_once(exact2nn_u8_pair_batch_kernel<QPT, QB>, Cfg::kSmemBytes, attr_set);
+    if (e != cudaSuccess) return e;
+    if (bp.plan.grid <= 0) return cudaSuccess;
+    exact2nn_u8_pair_batch_kernel<QPT, QB><<<2 * bp.plan.grid, Cfg::kThreads, Cfg::kSmemBytes, stream>>>(
+        qmap, bmap, brec, bp.plan, bp.items, bp.n_items, partial, thresh, err);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
-size_t exact2nn_pair_smem_bytes() { return PairCfg<false>::kSmemBytes; }
+size_t exact2nn_pair_smem_bytes() { return CfgU8::kSmemBytes; }
 
 cudaError_t launch_exact2nn_u8_pair(const CUtensorMap& qmap, const CUtensorMap& bmap_half, const int32_t* brec,
                                     const ExactPlan& plan, int4* partial, int32_t* thresh, int* err,
                                     cudaStream_t stream) {
     static bool attr_set[64] = {};
-    cudaError_t e = set_smem_once(exact2nn_u8_pair_kernel, PairCfg<false>::kSmemBytes, attr_set);
+    cudaError_t e = set_smem_once(exact2nn_u8_pair_kernel, CfgU8::kSmemBytes, attr_set);
     if (e != cudaSuccess) return e;
     if (plan.grid <= 0) return cudaSuccess;
-    exact2nn_u8_pair_kernel<<<2 * plan.grid, kPThreads, PairCfg<false>::kSmemBytes, stream>>>(
-        qmap, bmap_half, brec, plan, partial, thresh, err);
+    exact2nn_u8_pair_kernel<<<2 * plan.grid, CfgU8::kThreads, CfgU8::kSmemBytes, stream>>>(
+        qmap, bmap_half, brec, plan, single_item(plan), partial, thresh, err);
     return cudaGetLastError();
 }
 
@@ -436,12 +541,21 @@ cudaError_t launch_exact2nn_f16_pair(const CUtensorMap& qmap, const CUtensorMap&
                                      const ExactPlan& plan, int4* partial, int32_t* thresh, int* err, float dscale,
                                      cudaStream_t stream) {
     static bool attr_set[64] = {};
-    cudaError_t e = set_smem_once(exact2nn_f16_pair_kernel, PairCfg<true>::kSmemBytes, attr_set);
+    cudaError_t e = set_smem_once(exact2nn_f16_pair_kernel, CfgF16::kSmemBytes, attr_set);
     if (e != cudaSuccess) return e;
     if (plan.grid <= 0) return cudaSuccess;
-    exact2nn_f16_pair_kernel<<<2 * plan.grid, kPThreads, PairCfg<true>::kSmemBytes, stream>>>(
-        qmap, bmap_half, brec, plan, partial, thresh, err, dscale);
+    exact2nn_f16_pair_kernel<<<2 * plan.grid, CfgF16::kThreads, CfgF16::kSmemBytes, stream>>>(
+        qmap, bmap_half, brec, plan, single_item(plan), partial, thresh, err, dscale);
     return cudaGetLastError();
+}
+
+cudaError_t launch_exact2nn_u8_pair_batch(const CUtensorMap& qmap, const CUtensorMap& bmap_half, const int32_t* brec,
+                                          const BatchPlan& bp, int4* partial, int32_t* thresh, int* err, int qpt,
+                                          int qbuf, cudaStream_t stream) {
+    if (qpt == 2 && qbuf == 1) return launch_batch_variant<2, 1>(qmap, bmap_half, brec, bp, partial, thresh, err, stream);
+    if (qpt == 2 && qbuf == 2) return launch_batch_variant<2, 2>(qmap, bmap_half, brec, bp, partial, thresh, err, stream);
+    if (qpt == 1 && qbuf == 2) return launch_batch_variant<1, 2>(qmap, bmap_half, brec, bp, partial, thresh, err, stream);
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace sift
