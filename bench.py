@@ -245,6 +245,7 @@ def main():
         variants["fp16"] = fp16_leg(args, lib, ms, torch, qd, rd, flush, stream, q_n)
         if not torch.equal(variants["fp16"].pop("nn_idx"), nn_idx):
             raise RuntimeError("FP16 and u8 kernels disagree")
+        variants["pairs"] = pairs_leg(args, ms, torch, dev, stream)
 
     # ---- end to end through the C ABI with host buffers
     e2e_ms = float("nan")
@@ -275,7 +276,8 @@ def main():
 
     # ---- max over ranks
     vkeys = sorted(variants)
-    t = torch.tensor([step_ms, e2e_ms, kernel_ms] + [variants[k][f] for k in vkeys for f in ("step_ms", "kernel_ms")],
+    t = torch.tensor([step_ms, e2e_ms, kernel_ms] +
+                     [variants[k].get(f, 0.0) for k in vkeys for f in ("step_ms", "kernel_ms")],
                      dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -325,11 +327,28 @@ def main():
                          "frac_of_2x_bf16_" + peak_src: round(achieved / bf16x2, 4)},
             "clocks": clocks.summary(),
         }
+        if "pairs" in variants:
+            v = variants["pairs"]
+            pk_ms = v["step_ms"] / v["steps"]
+            ach = v["ops"] / (pk_ms * 1e-3) / 1e12
+            line.setdefault("variants", {})["pairs512"] = {
+                "value": round(world * v["queries"] / (pk_ms * 1e-3), 1), "unit": "queries/s",
+                "ms_per_step": round(pk_ms, 4), "steps": v["steps"], "dtype": "u8",
+                "workload": f"{v['pairs']} image pairs, 500..8000 keypoints per side (log-uniform, seed 0), "
+                            f"{v['queries']:,} query rows vs their pair's base rows, ratio test 0.8",
+                "call": "sift_batch_plan_run: one CUDA graph (norms, records, one persistent "
+                        "exact2nn_u8_pair_batch_kernel launch over the device work list, merge)",
+                "inputs": "q + r = %.0f MB device-resident (> L2)" % (v["bytes"] / 1e6),
+                "shape": v["shape"], "tuned_ms": v["tuned_ms"],
+                "roofline": {"bound": "tensor", "achieved": round(ach, 1), "peak": round(peak_int8, 1),
+                             "unit": "TFLOP/s", "frac": round(ach / peak_int8, 4), "ops_per_step": v["ops"],
+                             "note": "whole graph time (4 launches), 2 ops per MAC"},
+                "gpu_launches": v["launches"]}
         if "fp16" in variants:
             v = variants["fp16"]
             f16_peak = peaks["bf16_tflops"]
             ach = ops / (v["kernel_ms"] * 1e-3) / 1e12
-            line["variants"] = {"fp16": {
+            line.setdefault("variants", {})["fp16"] = {
                 "value": round(world * q_n * v["steps"] / (v["step_ms"] * 1e-3), 1), "unit": "queries/s",
                 "ms_per_step": round(v["step_ms"] / v["steps"], 4), "steps": v["steps"], "dtype": "f16",
                 "call": "sift2nn_match(type=SIFT_HALF_DEVICE): FP16 rows searched in place by "
@@ -338,7 +357,7 @@ def main():
                              "peak": round(f16_peak, 1), "unit": "TFLOP/s", "frac": round(ach / f16_peak, 4),
                              "kernel_ms": round(v["kernel_ms"], 4),
                              "peak_note": f"dense bf16 cuBLAS ({peak_src}), the same tensor rate as f16"},
-                "gpu_launches": v["launches"], "clocks": v["clocks"]}}
+                "gpu_launches": v["launches"], "clocks": v["clocks"]}
         if not args.no_cpu_baseline:
             rate, sample, threads, kind = cpu_reference_rate(queries, base, 15.0)
             line["cpu_baseline"] = {"value": round(rate, 2), "unit": "queries/s", "cores": threads, "kind": kind,
@@ -389,6 +408,43 @@ def fp16_leg(args, lib, ms, torch, qd, rd, flush, stream, q_n):
     return {"step_ms": float(sum(a.elapsed_time(b) for a, b in ev)), "kernel_ms": kt.value / max(kn.value, 1),
             "steps": steps, "launches": int(launches), "clocks": clocks.summary(),
             "nn_idx": nn_idx}
+
+
+def pairs_leg(args, ms, torch, dev, stream):
+    """512 uneven image pairs (the batched workload) through a tuned batch plan."""
+    from matching_sift_b200 import datagen
+
+    data = datagen.make_pairs(512, seed=0)
+    q = np.concatenate([a for a, _ in data])
+    r = np.concatenate([b for _, b in data])
+    pairs, off, ops = [], 0, 0
+    for a, b in data:
+        pairs.append([a.shape[0], b.shape[0], off])
+        off += b.shape[0]
+        ops += 2 * a.shape[0] * b.shape[0] * DIM
+    qd, rd = torch.from_numpy(q).to(dev), torch.from_numpy(r).to(dev)
+    plan = ms.BatchPlan(qd, rd, pairs, threshold=THRESHOLD, tune=True)
+    info = plan.info()
+    for _ in range(args.warmup):
+        plan.run(stream)
+    torch.cuda.synchronize()
+    steps = max(3, args.steps)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = ms.lib().sift_launch_count()
+    a.record(stream)
+    for _ in range(steps):
+        plan.run(stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    if ms.stream_status(stream.cuda_stream) != 0:
+        raise RuntimeError("device status after the batched steps")
+    plan.close()
+    return {"step_ms": a.elapsed_time(b), "steps": steps, "queries": int(q.shape[0]), "pairs": len(pairs),
+            "ops": float(ops), "bytes": float(q.nbytes + r.nbytes),
+            "shape": {"qpt": info["qpt"], "qbuf": info["qbuf"]},
+            "tuned_ms": [round(x, 4) for x in info["tuned_ms"]],
+            # graph replays are not counted by the library's launch counter; 4 kernels per replay
+            "launches": int(ms.lib().sift_launch_count() - launches0) + 4 * steps}
 
 
 def reference_arm(args, world, rank):
