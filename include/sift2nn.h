@@ -234,6 +234,65 @@ SIFT_API const char* sift_version(void);
  * Part 3: instrumentation (used by the benchmark)
  * ------------------------------------------------------------------- */
 
+/* ---------------------------------------------------------------------
+ * Learned hash (no counterpart in the reference, whose only hash is the
+ * random-hyperplane family of src/lsh_h.cu:88-100): an MLP 128 -> 256 -> k,
+ * z = W2 h + b2, h = bf16(relu(W1 (x / 64) + b1)), BF16 weights, FP32
+ * accumulation; bit j of a descriptor's bucket code is set when z_j > 0.
+ * ------------------------------------------------------------------- */
+typedef struct sift_mlp {
+    const void* w1;  /* bf16 [256][128], device, 16-byte aligned */
+    const float* b1; /* [256] */
+    const void* w2;  /* bf16 [k][256] */
+    const float* b2; /* [k] */
+    int k;           /* code bits, 1..32 */
+} sift_mlp;
+
+/* Trains a model on neighbour pairs labelled by the exact search: each of
+   `steps` Adam steps (learning rate lr) draws `batch` (multiple of 32)
+   training queries from train_q, their exact nearest base rows and `batch`
+   random base rows, and minimises
+     mean(1 - s(q, nn)) + neg_weight * mean(s(q, random)^2)
+       + balance_weight * sum_j mean(t_j)^2,
+   t = tanh(z), s(a, b) = mean_j t_aj t_bj. base, train_q: uint8 [n][128]
+   device rows. Outputs: the model (w1, b1, w2, b2 as in sift_mlp, device),
+   optionally the FP32 parameters (params_out, device, SIFT_MLP_PARAMS
+   floats: W1, b1, W2 padded to 32 rows, b2 padded to 32) and the loss of
+   every step (loss_curve, host). Deterministic for a given seed.
+   Synchronises. */
+#define SIFT_MLP_PARAMS (256 * 128 + 256 + 32 * 256 + 32)
+SIFT_API int sift_mlp_train(const uint8_t* base, uint32_t r_n, const uint8_t* train_q, uint32_t t_n, int k, int steps,
+                            int batch, float lr, float neg_weight, float balance_weight, unsigned long long seed,
+                            void* w1, float* b1, void* w2, float* b2, float* params_out, float* loss_curve);
+
+/* Bucket codes of n uint8 rows (device) on the tensor cores; z (optional,
+   device [n][k]) receives the outputs. Asynchronous on `stream`. */
+SIFT_API int sift_mlp_hash(const uint8_t* x, uint32_t n, const sift_mlp* model, uint32_t* codes, float* z,
+                           void* stream);
+
+/* Approximate 2-NN with the learned hash: base rows are bucketed by code;
+   each query scans n_probes buckets (its code, then codes with its
+   smallest-|z| bits flipped, lightest flips first; n_probes <= 64) with
+   exact distances; queries whose buckets held fewer than min_candidates rows
+   are searched exactly (the exact kernel) instead. Outputs as sift2nn_match
+   for uint8 device rows (matches: ratio test when threshold > 0, else the
+   nearest candidate); candidates (device [q_n], optional) receives the number
+   of base rows each query compared in its buckets; fallback_count (host,
+   optional) the number of queries searched exactly. Synchronises when
+   min_candidates > 0. */
+SIFT_API int sift_mlp_match(const uint8_t* q, const uint8_t* r, uint32_t q_n, uint32_t r_n, const sift_mlp* model,
+                            int n_probes, int min_candidates, float threshold, uint32_t* matches, int32_t* nn_idx,
+                            float* nn_dist, uint32_t* candidates, uint32_t* fallback_count, void* stream);
+
+/* Loss and gradients of one training step, for checking the training
+   kernels: x = [3 * batch][128] uint8 device rows (queries, their
+   neighbours, random rows), params / grads = SIFT_MLP_PARAMS device floats
+   (weights are rounded to BF16 for the forward pass; gradients pass straight
+   through the roundings), loss (host [4]) = total, positive, negative,
+   balance terms. Synchronises. */
+SIFT_API int sift_mlp_loss_grad(const uint8_t* x, int batch, int k, const float* params, float neg_weight,
+                                float balance_weight, float* grads, float* loss);
+
 /* Host-side work decomposition of a batch (no GPU needed): out[0..5] =
    units, base-tile records, query rows, max CTA pairs sharing one query
    group, CTA pairs launched, queries per group; for `workers` CTA pairs and

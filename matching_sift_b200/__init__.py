@@ -13,7 +13,7 @@ from __future__ import annotations
 
 import ctypes
 
-from ._native import (SIFT_BATCH_SHAPE, SIFT_BATCH_TUNE,
+from ._native import (SIFT_BATCH_SHAPE, SIFT_BATCH_TUNE, SIFT_MLP_PARAMS, sift_mlp,
                       FLOAT_DEVICE, FLOAT_HOST, HALF_DEVICE, METRIC_DOT, METRIC_L2, SIFT_ERR_ALLOC,
                       SIFT_ERR_CUDA, SIFT_ERR_DEVICE_TIMEOUT, SIFT_ERR_INVALID_ARG, SIFT_ERR_NO_DEVICE,
                       SIFT_ERR_NOT_INTEGER, SIFT_ERR_UNSUPPORTED, SIFT_OK, U8_DEVICE, U8_HOST, LIB_PATH,
@@ -21,7 +21,7 @@ from ._native import (SIFT_BATCH_SHAPE, SIFT_BATCH_TUNE,
 
 __all__ = [
     "cublas_2nn_sift", "cublas_2nn_f", "device_brute", "host_brute", "lsh_gpu", "match", "lsh_match", "lsh_hash",
-    "stream_status", "version", "match_batch", "BatchPlan", "batch_describe",
+    "stream_status", "version", "match_batch", "BatchPlan", "batch_describe", "MlpHash", "mlp_loss_grad",
     "SiftError", "FLOAT_HOST", "FLOAT_DEVICE", "HALF_DEVICE", "U8_DEVICE", "U8_HOST", "METRIC_L2", "METRIC_DOT",
 ]
 
@@ -252,3 +252,93 @@ def batch_describe(pairs, r_rows: int, qpt: int = 2, workers: int = 74):
     check(lib().sift_batch_describe(pa.ctypes.data if len(pa) else None, len(pa), r_rows, qpt, workers, out),
           "sift_batch_describe")
     return dict(zip(("units", "tiles", "queries", "max_splits", "grid", "group_rows"), list(out)))
+
+
+# ------------------------------------------------------------- learned hash --
+
+class MlpHash:
+    """A learned hash model (MLP 128 -> 256 -> k, BF16 weights) on the GPU.
+
+    Build it with :meth:`train` (neighbour pairs labelled by the exact search)
+    or from explicit FP32 parameters (:meth:`from_params`, the flat layout of
+    SIFT_MLP_PARAMS floats).
+    """
+
+    def __init__(self, w1, b1, w2, b2, k: int, params=None, loss_curve=None):
+        self.w1, self.b1, self.w2, self.b2, self.k = w1, b1, w2, b2, k
+        self.params = params
+        self.loss_curve = loss_curve
+        self._c = sift_mlp(w1.data_ptr(), b1.data_ptr(), w2.data_ptr(), b2.data_ptr(), k)
+
+    @staticmethod
+    def _empty(k, dev):
+        import torch
+
+        return (torch.empty((256, 128), dtype=torch.bfloat16, device=dev), torch.empty(256, device=dev),
+                torch.empty((k, 256), dtype=torch.bfloat16, device=dev), torch.empty(k, device=dev))
+
+    @classmethod
+    def train(cls, base, train_q, k: int = 16, steps: int = 1000, batch: int = 2048, lr: float = 2e-3,
+              neg_weight: float = 1.0, balance_weight: float = 1.0, seed: int = 0):
+        import numpy as np
+        import torch
+
+        w1, b1, w2, b2 = cls._empty(k, base.device)
+        params = torch.empty(SIFT_MLP_PARAMS, device=base.device)
+        curve = np.zeros(max(steps, 1), np.float32)
+        check(lib().sift_mlp_train(_ptr(base), base.shape[0], _ptr(train_q), train_q.shape[0], k, steps, batch, lr,
+                                   neg_weight, balance_weight, seed, _ptr(w1), _ptr(b1), _ptr(w2), _ptr(b2),
+                                   _ptr(params), curve.ctypes.data), "sift_mlp_train")
+        return cls(w1, b1, w2, b2, k, params=params, loss_curve=curve[:steps])
+
+    @classmethod
+    def from_params(cls, params, k: int):
+        """Model from flat FP32 parameters (torch CUDA tensor), weights rounded to BF16."""
+        import torch
+
+        p = params.float()
+        w1 = p[:256 * 128].view(256, 128).to(torch.bfloat16).contiguous()
+        b1 = p[256 * 128:256 * 128 + 256].contiguous()
+        o = 256 * 128 + 256
+        w2 = p[o:o + 32 * 256].view(32, 256)[:k].to(torch.bfloat16).contiguous()
+        b2 = p[o + 32 * 256:o + 32 * 256 + k].contiguous()
+        return cls(w1, b1, w2, b2, k, params=params)
+
+    def hash(self, x, with_z: bool = False, stream=None):
+        import torch
+
+        codes = torch.empty(x.shape[0], dtype=torch.int32, device=x.device)
+        z = torch.empty((x.shape[0], self.k), device=x.device) if with_z else None
+        s = stream if stream is not None else torch.cuda.current_stream(x.device)
+        check(lib().sift_mlp_hash(_ptr(x), x.shape[0], ctypes.byref(self._c), _ptr(codes), _ptr(z), s.cuda_stream),
+              "sift_mlp_hash")
+        return (codes, z) if with_z else codes
+
+    def match(self, q, r, n_probes: int = 1, min_candidates: int = 0, threshold: float = 0.0, stream=None):
+        """{"matches", "nn_idx", "nn_dist", "candidates", "fallback"}: learned-hash 2-NN (see sift_mlp_match)."""
+        import torch
+
+        n = q.shape[0]
+        out = {"matches": torch.empty(n, dtype=torch.int32, device=q.device),
+               "nn_idx": torch.empty((n, 2), dtype=torch.int32, device=q.device),
+               "nn_dist": torch.empty((n, 2), dtype=torch.float32, device=q.device),
+               "candidates": torch.empty(n, dtype=torch.int32, device=q.device)}
+        fb = ctypes.c_uint32(0)
+        s = stream if stream is not None else torch.cuda.current_stream(q.device)
+        check(lib().sift_mlp_match(_ptr(q), _ptr(r), n, r.shape[0], ctypes.byref(self._c), n_probes, min_candidates,
+                                   threshold, _ptr(out["matches"]), _ptr(out["nn_idx"]), _ptr(out["nn_dist"]),
+                                   _ptr(out["candidates"]), ctypes.byref(fb), s.cuda_stream), "sift_mlp_match")
+        out["fallback"] = fb.value
+        return out
+
+
+def mlp_loss_grad(x, batch: int, k: int, params, neg_weight: float = 1.0, balance_weight: float = 1.0):
+    """(loss[4], grads) of one training step on rows x [3 * batch, 128] (device)."""
+    import numpy as np
+    import torch
+
+    grads = torch.empty(SIFT_MLP_PARAMS, device=x.device)
+    loss = (ctypes.c_float * 4)()
+    check(lib().sift_mlp_loss_grad(_ptr(x), batch, k, _ptr(params), neg_weight, balance_weight, _ptr(grads), loss),
+          "sift_mlp_loss_grad")
+    return np.array(list(loss), np.float64), grads

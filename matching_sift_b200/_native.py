@@ -57,7 +57,24 @@ _PROTOS = {
     "sift_batch_plan_destroy": (None, [_vp]),
     "sift_batch_describe": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
                                            ctypes.POINTER(ctypes.c_longlong)]),
+    "sift_mlp_train": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                      ctypes.c_ulonglong, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "sift_mlp_hash": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, _vp, _vp, _vp]),
+    "sift_mlp_match": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, _vp, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_float, _vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_uint32), _vp]),
+    "sift_mlp_loss_grad": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_float, ctypes.c_float, _vp,
+                                          ctypes.POINTER(ctypes.c_float)]),
 }
+
+
+class sift_mlp(ctypes.Structure):
+    """C layout of `sift_mlp` (include/sift2nn.h)."""
+    _fields_ = [("w1", ctypes.c_void_p), ("b1", ctypes.c_void_p), ("w2", ctypes.c_void_p),
+                ("b2", ctypes.c_void_p), ("k", ctypes.c_int)]
+
+
+SIFT_MLP_PARAMS = 256 * 128 + 256 + 32 * 256 + 32
 
 SIFT_BATCH_TUNE = 1
 

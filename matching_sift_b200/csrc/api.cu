@@ -110,6 +110,18 @@ int encode_u8_rows(CUtensorMap* m, const void* base, uint64_t rows, uint32_t box
     return r == CUDA_SUCCESS ? SIFT_OK : SIFT_ERR_CUDA;
 }
 
+int encode_bf16_2d(CUtensorMap* m, const void* base, uint64_t inner, uint64_t rows, uint32_t box_inner,
+                   uint32_t box_rows) {
+    cuuint64_t dims[2] = {static_cast<cuuint64_t>(inner), static_cast<cuuint64_t>(rows)};
+    cuuint64_t strides[1] = {static_cast<cuuint64_t>(inner) * 2};
+    cuuint32_t box[2] = {box_inner, box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? SIFT_OK : SIFT_ERR_CUDA;
+}
+
 // FP16 rows of 128 halves (256 B): dims {128, rows}, box {64, box_rows} (one
 // 128-byte K block per load, the widest SWIZZLE_128B box).
 int encode_f16_rows(CUtensorMap* m, const void* base, uint64_t rows, uint32_t box_rows) {
@@ -485,8 +497,9 @@ int lsh_match(const LshArgs& a) {
     uint32_t* m_out = (a.matches && !m_dev) ? reinterpret_cast<uint32_t*>(A + o_m) : a.matches;
     int32_t* i_out = (a.nn_idx && !i_dev) ? reinterpret_cast<int32_t*>(A + o_i) : a.nn_idx;
     float* d_out = (a.nn_dist && !d_dev) ? reinterpret_cast<float*>(A + o_d) : a.nn_dist;
-    SIFT_CUDA(launch_lsh_scan(qd, rd, q_n, r_n, L_, shift, nbins, codes_q, start, order, ocode, qnorm, rnorm,
-                              a.threshold, a.ratio ? 1 : 0, ldexpf(1.0f, -2 * vshift), m_out, i_out, d_out, st));
+    SIFT_CUDA(launch_lsh_scan(qd, rd, q_n, r_n, L_, 1, shift, nbins, codes_q, start, order, ocode, qnorm, rnorm,
+                              a.threshold, a.ratio ? 1 : 0, ldexpf(1.0f, -2 * vshift), m_out, nullptr, i_out, d_out,
+                              st));
     g_launches += 1 + (r_n > 0 ? 3 : 0) + 1;
     if (a.matches && !m_dev)
         SIFT_CUDA(cudaMemcpyAsync(a.matches, m_out, static_cast<size_t>(q_n) * 4, cudaMemcpyDeviceToHost, st));

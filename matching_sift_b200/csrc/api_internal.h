@@ -38,6 +38,9 @@ struct LshArgs {
     bool sync = false;
 };
 int lsh_match(const LshArgs& a);
+int mlp_train(const uint8_t* base, uint32_t r_n, const uint8_t* tq, uint32_t t_n, int k, int steps, int batch,
+              float lr, float neg_w, float bal_w, unsigned long long seed, void* w1_out, float* b1_out, void* w2_out,
+              float* b2_out, float* params_out, float* loss_curve);
 int lsh_hash(const uint8_t* x, uint32_t n, const int8_t* planes, int L, int k, uint32_t* codes, void* stream);
 void reference_planes(int L, int nbits, int8_t* out);
 int stream_status(void* stream);

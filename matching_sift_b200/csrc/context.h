@@ -47,6 +47,10 @@ int ensure_arena(DeviceCtx& c, size_t bytes);
 bool is_device_accessible(const void* p);
 // u8 rows of 128 bytes: dims {128, rows}, box {128, box_rows}, SWIZZLE_128B.
 int encode_u8_rows(CUtensorMap* m, const void* base, uint64_t rows, uint32_t box_rows);
+// BF16 matrix [rows][inner] (row pitch inner * 2 bytes): box {box_inner, box_rows},
+// SWIZZLE_128B (box_inner * 2 <= 128), rows past the end read as zeros.
+int encode_bf16_2d(CUtensorMap* m, const void* base, uint64_t inner, uint64_t rows, uint32_t box_inner,
+                   uint32_t box_rows);
 int map_cuda(cudaError_t e);
 // Reads and clears the device status words. Caller has synchronised `st`.
 int collect_device_status(DeviceCtx& c, cudaStream_t st);

@@ -20,8 +20,8 @@
 // query's code (the reference scans sorted positions starting at a point id
 // instead, src/lsh_h.cu:599,617 vs :469,482, which is not the bucket).
 //
-// Candidate scan. One warp per query over its L buckets; each lane takes one
-// candidate at a time and forms |q - b|^2 = |q|^2 + |b|^2 - 2 q.b with dp4a;
+// Candidate scan. One warp per query over its L buckets (L x P with P probe
+// codes per table: multi-probe); each lane takes one candidate at a time and forms |q - b|^2 = |q|^2 + |b|^2 - 2 q.b with dp4a;
 // the per-query top-2 is lexicographic in (distance, index) and counts a base
 // point found in several tables once.
 #include <climits>
@@ -275,13 +275,14 @@ __device__ __forceinline__ void push_dedup(int d, int i, int& d1, int& i1, int& 
 // One warp per query. Each lane holds the query row (32 words) and scans one
 // candidate at a time; lanes' top-2 lists are merged at the end.
 __global__ void __launch_bounds__(256) lsh_scan_kernel(const uint8_t* __restrict__ q, const uint8_t* __restrict__ r,
-                                                       int q_n, int r_n, int L, int shift, int nbins,
+                                                       int q_n, int r_n, int L, int probes, int shift, int nbins,
                                                        const uint32_t* __restrict__ qcodes,
                                                        const int* __restrict__ start, const int* __restrict__ order,
                                                        const uint32_t* __restrict__ ocode,
                                                        const int32_t* __restrict__ qnorm,
                                                        const int32_t* __restrict__ rnorm, float thr, int ratio,
                                                        float dscale, uint32_t* __restrict__ matches,
+                                                       uint32_t* __restrict__ counts,
                                                        int32_t* __restrict__ nn_idx,
                                                        float* __restrict__ nn_dist) {
     const int wq = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -296,8 +297,14 @@ __global__ void __launch_bounds__(256) lsh_scan_kernel(const uint8_t* __restrict
     }
     const int nq = qnorm[wq];
     int d1 = INT_MAX, i1 = -1, d2 = INT_MAX, i2 = -1;
-    for (int t = 0; t < L; ++t) {
-        const uint32_t code = qcodes[static_cast<size_t>(t) * q_n + wq];
+    uint32_t seen = 0;  // candidates this lane compared (bucket members)
+    for (int c = 0; c < L * probes; ++c) {
+        const int t = c / probes;  // probe c of the query searches table t
+        const uint32_t code = qcodes[static_cast<size_t>(c) * q_n + wq];
+        // A repeated probe code (fewer distinct probes than requested) is skipped.
+        bool dup = false;
+        for (int c2 = t * probes; c2 < c; ++c2) dup |= qcodes[static_cast<size_t>(c2) * q_n + wq] == code;
+        if (dup) continue;
         const int* st = start + static_cast<size_t>(t) * (nbins + 1);
         const int bin = static_cast<int>(code >> shift);
         const int s = st[bin], e = st[bin + 1];
@@ -305,6 +312,7 @@ __global__ void __launch_bounds__(256) lsh_scan_kernel(const uint8_t* __restrict
         const uint32_t* oc = ocode + static_cast<size_t>(t) * r_n;
         for (int p = s + lane; p < e; p += 32) {
             if (oc[p] != code) continue;
+            ++seen;
             const int id = ord[p];
             const uint4* rrow = reinterpret_cast<const uint4*>(r + static_cast<size_t>(id) * 128);
             uint32_t dot = 0;
@@ -328,7 +336,10 @@ __global__ void __launch_bounds__(256) lsh_scan_kernel(const uint8_t* __restrict
         push_dedup(od1, oi1, d1, i1, d2, i2);
         push_dedup(od2, oi2, d1, i1, d2, i2);
     }
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) seen += __shfl_xor_sync(0xffffffffu, seen, o);
     if (lane == 0) {
+        if (counts) counts[wq] = seen;
         const bool v1 = i1 >= 0, v2 = i2 >= 0;
         const float f1 = v1 ? static_cast<float>(d1) * dscale : FLT_MAX;
         const float f2 = v2 ? static_cast<float>(d2) * dscale : FLT_MAX;
@@ -384,14 +395,17 @@ cudaError_t launch_lsh_buckets(const uint32_t* codes, int n, int L, int shift, i
     return cudaGetLastError();
 }
 
-cudaError_t launch_lsh_scan(const uint8_t* q, const uint8_t* r, int q_n, int r_n, int L, int shift, int nbins,
-                            const uint32_t* qcodes, const int* start, const int* order, const uint32_t* ocode,
-                            const int32_t* qnorm, const int32_t* rnorm, float thr, int ratio, float dist_scale,
-                            uint32_t* matches, int32_t* nn_idx, float* nn_dist, cudaStream_t stream) {
+cudaError_t launch_lsh_scan(const uint8_t* q, const uint8_t* r, int q_n, int r_n, int L, int probes, int shift,
+                            int nbins, const uint32_t* qcodes, const int* start, const int* order,
+                            const uint32_t* ocode, const int32_t* qnorm, const int32_t* rnorm, float thr, int ratio,
+                            float dist_scale, uint32_t* matches, uint32_t* counts, int32_t* nn_idx, float* nn_dist,
+                            cudaStream_t stream) {
     if (q_n <= 0) return cudaSuccess;
-    const int blocks = (q_n * 32 + 255) / 256;
-    lsh_scan_kernel<<<blocks, 256, 0, stream>>>(q, r, q_n, r_n, L, shift, nbins, qcodes, start, order, ocode, qnorm,
-                                                rnorm, thr, ratio, dist_scale, matches, nn_idx, nn_dist);
+    const long long blocks = (static_cast<long long>(q_n) * 32 + 255) / 256;
+    lsh_scan_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(q, r, q_n, r_n, L, probes, shift, nbins,
+                                                                      qcodes, start, order, ocode, qnorm, rnorm, thr,
+                                                                      ratio, dist_scale, matches, counts, nn_idx,
+                                                                      nn_dist);
     return cudaGetLastError();
 }
 

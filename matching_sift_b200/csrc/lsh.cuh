@@ -26,12 +26,15 @@ cudaError_t launch_lsh_hash(const CUtensorMap& xmap, const CUtensorMap& pmap, in
 cudaError_t launch_lsh_buckets(const uint32_t* codes, int n, int L, int shift, int nbins, int* hist, int* start,
                                int* order, uint32_t* ocode, int num_sms, cudaStream_t stream);
 
-// Exact 2-NN of every query over the union of its L buckets. ratio != 0
-// applies the Lowe test with `thr` to `matches`; otherwise matches = nearest.
-// dist_scale multiplies the distances (2^-2s for inputs scaled by 2^-s).
-cudaError_t launch_lsh_scan(const uint8_t* q, const uint8_t* r, int q_n, int r_n, int L, int shift, int nbins,
-                            const uint32_t* qcodes, const int* start, const int* order, const uint32_t* ocode,
-                            const int32_t* qnorm, const int32_t* rnorm, float thr, int ratio, float dist_scale,
-                            uint32_t* matches, int32_t* nn_idx, float* nn_dist, cudaStream_t stream);
+// Exact 2-NN of every query over the union of its buckets: qcodes[L * probes][q_n],
+// code c of a query searching table c / probes (probes = 1: its own code in
+// every table). ratio != 0 applies the Lowe test with `thr` to `matches`;
+// otherwise matches = nearest. dist_scale multiplies the distances (2^-2s for
+// inputs scaled by 2^-s). counts (optional): candidates compared per query.
+cudaError_t launch_lsh_scan(const uint8_t* q, const uint8_t* r, int q_n, int r_n, int L, int probes, int shift,
+                            int nbins, const uint32_t* qcodes, const int* start, const int* order,
+                            const uint32_t* ocode, const int32_t* qnorm, const int32_t* rnorm, float thr, int ratio,
+                            float dist_scale, uint32_t* matches, uint32_t* counts, int32_t* nn_idx, float* nn_dist,
+                            cudaStream_t stream);
 
 }  // namespace sift
