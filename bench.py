@@ -168,7 +168,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true", help="time only the device-resident path")
     ap.add_argument("--queries", type=int, default=Q_N, help="queries per GPU (profiling of smaller cases)")
-    ap.add_argument("--no-variants", action="store_true", help="skip the FP16 leg")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="skip the FP16, batched-pairs, learned-hash and LSH legs")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -246,6 +247,9 @@ def main():
         if not torch.equal(variants["fp16"].pop("nn_idx"), nn_idx):
             raise RuntimeError("FP16 and u8 kernels disagree")
         variants["pairs"] = pairs_leg(args, ms, torch, dev, stream)
+        truth = nn_idx[:, 0].cpu().numpy()
+        variants["learned"] = learned_leg(args, ms, torch, dev, stream, qd, rd, base, truth)
+        variants["lsh"] = lsh_leg(args, ms, torch, dev, stream, qd, rd, truth)
 
     # ---- end to end through the C ABI with host buffers
     e2e_ms = float("nan")
@@ -344,6 +348,12 @@ def main():
                              "unit": "TFLOP/s", "frac": round(ach / peak_int8, 4), "ops_per_step": v["ops"],
                              "note": "whole graph time (4 launches), 2 ops per MAC"},
                 "gpu_launches": v["launches"]}
+        for key in ("learned", "lsh"):
+            if key in variants:
+                v = dict(variants[key])
+                v.pop("step_ms", None)
+                v.pop("kernel_ms", None)
+                line.setdefault("variants", {})["learned_hash" if key == "learned" else "lsh"] = v
         if "fp16" in variants:
             v = variants["fp16"]
             f16_peak = peaks["bf16_tflops"]
@@ -445,6 +455,71 @@ def pairs_leg(args, ms, torch, dev, stream):
             "tuned_ms": [round(x, 4) for x in info["tuned_ms"]],
             # graph replays are not counted by the library's launch counter; 4 kernels per replay
             "launches": int(ms.lib().sift_launch_count() - launches0) + 4 * steps}
+
+
+def _time_calls(torch, stream, fn, steps):
+    """Mean device time (ms) of fn() over `steps` calls after one warm-up call."""
+    fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        out = fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps, out
+
+
+def learned_leg(args, ms, torch, dev, stream, qd, rd, base, truth):
+    """Learned hash (MLP 128 -> 256 -> 16) trained on 100,000 synthetic
+    queries labelled by the exact kernel; 2-NN of the bench queries at
+    several operating points (probes, exact-fallback criteria), each call
+    rebuilding the base's buckets; recall@1 against the exact results."""
+    from matching_sift_b200 import datagen
+
+    tq = torch.from_numpy(datagen.make_queries(100_000, base, seed=7)).to(dev)
+    t0 = time.perf_counter()
+    model = ms.MlpHash.train(rd, tq, k=16, steps=1500, batch=2048, lr=2e-3, seed=1)
+    train_s = time.perf_counter() - t0
+    q_n = qd.shape[0]
+    points = []
+    steps = max(3, args.steps // 2)
+    for probes, min_cand, max_dist in ((1, 0, 0.0), (4, 0, 0.0), (16, 0, 0.0), (1, 64, 0.0), (4, 64, 30000.0),
+                                       (1, 64, 30000.0), (1, 0, 20000.0)):
+        ms_call, out = _time_calls(torch, stream, lambda: model.match(qd, rd, n_probes=probes, min_candidates=min_cand,
+                                                                     max_dist=max_dist, stream=stream), steps)
+        got = out["nn_idx"][:, 0].cpu().numpy()
+        points.append({"probes": probes, "min_candidates": min_cand, "max_dist": max_dist,
+                       "ms_per_call": round(ms_call, 4), "value": round(q_n / (ms_call * 1e-3), 1),
+                       "recall1": round(float((got == truth).mean()), 4),
+                       "candidates_mean": round(float(out["candidates"].float().mean().item()), 1),
+                       "exact_fallback_queries": int(out["fallback"])})
+    ok = [p for p in points if p["recall1"] >= 0.8]
+    best = max(ok, key=lambda p: p["value"]) if ok else None
+    return {"value": best["value"] if best else None, "unit": "queries/s",
+            "recall1": best["recall1"] if best else None, "operating_point": best,
+            "at": "fastest point with recall@1 >= 0.8 against the exact results (null if none)",
+            "workload": "same queries and base as the exact leg; every call hashes the base on the tensor cores "
+                        "and rebuilds its buckets",
+            "model": "MLP 128->256->16, BF16 weights, trained 1500 Adam steps x 2048 pairs "
+                     f"({train_s:.2f} s incl. exact labels of 100,000 training queries)",
+            "points": points}
+
+
+def lsh_leg(args, ms, torch, dev, stream, qd, rd, truth):
+    """Random-hyperplane LSH (int8 N(0,1)*32 planes, seed 1) at two (k, L)
+    settings: recall@1 against the exact results and queries/s per call."""
+    from matching_sift_b200 import datagen
+
+    q_n = qd.shape[0]
+    points = []
+    for k, L in ((16, 8), (8, 16)):
+        planes = torch.from_numpy(datagen.quantize_planes(datagen.make_hyperplanes(k, L, seed=1))).to(dev)
+        ms_call, out = _time_calls(torch, stream, lambda: ms.lsh_match(qd, rd, planes, stream=stream), 2)
+        got = out["nn_idx"][:, 0].cpu().numpy()
+        points.append({"k": k, "L": L, "ms_per_call": round(ms_call, 3), "value": round(q_n / (ms_call * 1e-3), 1),
+                       "recall1": round(float((got == truth).mean()), 4)})
+    return {"unit": "queries/s", "call": "sift_lsh_match (hash base + buckets + scan per call)", "points": points}
 
 
 def reference_arm(args, world, rank):

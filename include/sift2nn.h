@@ -273,16 +273,19 @@ SIFT_API int sift_mlp_hash(const uint8_t* x, uint32_t n, const sift_mlp* model, 
 /* Approximate 2-NN with the learned hash: base rows are bucketed by code;
    each query scans n_probes buckets (its code, then codes with its
    smallest-|z| bits flipped, lightest flips first; n_probes <= 64) with
-   exact distances; queries whose buckets held fewer than min_candidates rows
-   are searched exactly (the exact kernel) instead. Outputs as sift2nn_match
+   exact distances; queries whose buckets held fewer than min_candidates rows,
+   or (max_dist > 0) whose nearest candidate lies farther than max_dist
+   (squared L2; none found counts as farther), are searched exactly (the
+   exact kernel) instead. Outputs as sift2nn_match
    for uint8 device rows (matches: ratio test when threshold > 0, else the
    nearest candidate); candidates (device [q_n], optional) receives the number
    of base rows each query compared in its buckets; fallback_count (host,
    optional) the number of queries searched exactly. Synchronises when
-   min_candidates > 0. */
+   min_candidates > 0 or max_dist > 0. */
 SIFT_API int sift_mlp_match(const uint8_t* q, const uint8_t* r, uint32_t q_n, uint32_t r_n, const sift_mlp* model,
-                            int n_probes, int min_candidates, float threshold, uint32_t* matches, int32_t* nn_idx,
-                            float* nn_dist, uint32_t* candidates, uint32_t* fallback_count, void* stream);
+                            int n_probes, int min_candidates, float max_dist, float threshold, uint32_t* matches,
+                            int32_t* nn_idx, float* nn_dist, uint32_t* candidates, uint32_t* fallback_count,
+                            void* stream);
 
 /* Loss and gradients of one training step, for checking the training
    kernels: x = [3 * batch][128] uint8 device rows (queries, their

@@ -314,7 +314,8 @@ class MlpHash:
               "sift_mlp_hash")
         return (codes, z) if with_z else codes
 
-    def match(self, q, r, n_probes: int = 1, min_candidates: int = 0, threshold: float = 0.0, stream=None):
+    def match(self, q, r, n_probes: int = 1, min_candidates: int = 0, max_dist: float = 0.0, threshold: float = 0.0,
+              stream=None):
         """{"matches", "nn_idx", "nn_dist", "candidates", "fallback"}: learned-hash 2-NN (see sift_mlp_match)."""
         import torch
 
@@ -326,7 +327,7 @@ class MlpHash:
         fb = ctypes.c_uint32(0)
         s = stream if stream is not None else torch.cuda.current_stream(q.device)
         check(lib().sift_mlp_match(_ptr(q), _ptr(r), n, r.shape[0], ctypes.byref(self._c), n_probes, min_candidates,
-                                   threshold, _ptr(out["matches"]), _ptr(out["nn_idx"]), _ptr(out["nn_dist"]),
+                                   max_dist, threshold, _ptr(out["matches"]), _ptr(out["nn_idx"]), _ptr(out["nn_dist"]),
                                    _ptr(out["candidates"]), ctypes.byref(fb), s.cuda_stream), "sift_mlp_match")
         out["fallback"] = fb.value
         return out

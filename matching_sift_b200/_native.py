@@ -62,7 +62,8 @@ _PROTOS = {
                                       ctypes.c_ulonglong, _vp, _vp, _vp, _vp, _vp, _vp]),
     "sift_mlp_hash": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, _vp, _vp, _vp]),
     "sift_mlp_match": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, _vp, ctypes.c_int, ctypes.c_int,
-                                      ctypes.c_float, _vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_uint32), _vp]),
+                                      ctypes.c_float, ctypes.c_float, _vp, _vp, _vp, _vp,
+                                      ctypes.POINTER(ctypes.c_uint32), _vp]),
     "sift_mlp_loss_grad": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_float, ctypes.c_float, _vp,
                                           ctypes.POINTER(ctypes.c_float)]),
 }

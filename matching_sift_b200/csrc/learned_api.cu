@@ -17,11 +17,14 @@ namespace {
 
 using detail::DeviceCtx;
 
-// Queries whose probed buckets compared fewer than min_cand candidates.
-__global__ void flag_kernel(const uint32_t* __restrict__ counts, int n, uint32_t min_cand, int* __restrict__ idx,
-                            int* __restrict__ n_out) {
+// Queries whose probed buckets compared fewer than min_cand candidates, or
+// (max_dist > 0) whose nearest candidate lies farther than max_dist.
+__global__ void flag_kernel(const uint32_t* __restrict__ counts, const float* __restrict__ dist, int n,
+                            uint32_t min_cand, float max_dist, int* __restrict__ idx, int* __restrict__ n_out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n && counts[i] < min_cand) idx[atomicAdd(n_out, 1)] = i;
+    if (i >= n) return;
+    const bool far = max_dist > 0.0f && !(dist[2 * i] <= max_dist);
+    if (counts[i] < min_cand || far) idx[atomicAdd(n_out, 1)] = i;
 }
 
 __global__ void gather_rows_kernel(const uint8_t* __restrict__ q, const int* __restrict__ idx, int n,
@@ -99,10 +102,11 @@ int mlp_hash(const uint8_t* x, uint32_t n, const sift_mlp* model, uint32_t* code
 }
 
 int mlp_match(const uint8_t* q, const uint8_t* r, uint32_t q_n_, uint32_t r_n_, const sift_mlp* model, int n_probes,
-              int min_candidates, float threshold, uint32_t* matches, int32_t* nn_idx, float* nn_dist,
-              uint32_t* candidates, uint32_t* fallback_count, void* stream) {
+              int min_candidates, float max_dist, float threshold, uint32_t* matches, int32_t* nn_idx,
+              float* nn_dist, uint32_t* candidates, uint32_t* fallback_count, void* stream) {
     SIFT_TRY(check_model(model));
-    if (q_n_ > 0x7fffffffu / 64 || r_n_ > 0x7fffffffu / 64 || n_probes < 1 || n_probes > 64 || min_candidates < 0)
+    if (q_n_ > 0x7fffffffu / 64 || r_n_ > 0x7fffffffu / 64 || n_probes < 1 || n_probes > 64 || min_candidates < 0 ||
+        !(max_dist >= 0.0f))
         return SIFT_ERR_INVALID_ARG;
     if (fallback_count) *fallback_count = 0;
     if (q_n_ == 0) return SIFT_OK;
@@ -149,11 +153,13 @@ int mlp_match(const uint8_t* q, const uint8_t* r, uint32_t q_n_, uint32_t r_n_, 
     const size_t o_fqn = L.take(static_cast<size_t>(q_pad) * 4);
     const size_t o_fthr = L.take(static_cast<size_t>(q_pad) * 4);
     const size_t o_fpart = L.take(fb_part);
+    const size_t o_dist = L.take(static_cast<size_t>(q_n) * 8);  // distances when the caller takes none
     SIFT_TRY(detail::ensure_arena(c, L.off));
     char* A = c.arena;
     auto U32 = [&](size_t o) { return reinterpret_cast<uint32_t*>(A + o); };
     auto I32 = [&](size_t o) { return reinterpret_cast<int32_t*>(A + o); };
     uint32_t* counts = candidates ? candidates : U32(o_cnt);
+    float* dist = nn_dist ? nn_dist : reinterpret_cast<float*>(A + o_dist);
 
     CUtensorMap w1map, w2map;
     SIFT_TRY(encode_model(m, &w1map, &w2map));
@@ -173,16 +179,17 @@ int mlp_match(const uint8_t* q, const uint8_t* r, uint32_t q_n_, uint32_t r_n_, 
     SIFT_CUDA(launch_probe_codes(U32(o_cq), reinterpret_cast<float*>(A + o_z), q_n, k, flip, n_probes, U32(o_pc), st));
     SIFT_CUDA(launch_lsh_scan(q, r, q_n, r_n, 1, n_probes, shift, nbins, U32(o_pc), I32(o_start), I32(o_order),
                               U32(o_ocode), I32(o_qn), I32(o_rn), threshold, threshold > 0.f ? 1 : 0, 1.0f, matches,
-                              counts, nn_idx, nn_dist, st));
+                              counts, nn_idx, dist, st));
     launches += 4;
     detail::g_launches += launches;
-    if (min_candidates <= 0 || r_n == 0) return SIFT_OK;
+    if ((min_candidates <= 0 && max_dist <= 0.0f) || r_n == 0) return SIFT_OK;
 
     // ---- exact fallback for queries with too few candidates
     int* fidx = I32(o_fidx);
     int* fcount = fidx + q_n;  // the 16 bytes past the index list
     SIFT_CUDA(cudaMemsetAsync(fcount, 0, sizeof(int), st));
-    flag_kernel<<<(q_n + 255) / 256, 256, 0, st>>>(counts, q_n, static_cast<uint32_t>(min_candidates), fidx, fcount);
+    flag_kernel<<<(q_n + 255) / 256, 256, 0, st>>>(counts, dist, q_n, static_cast<uint32_t>(min_candidates), max_dist,
+                                                    fidx, fcount);
     SIFT_CUDA(cudaGetLastError());
     SIFT_CUDA(cudaMemcpyAsync(c.h_status + 1, fcount, sizeof(int), cudaMemcpyDeviceToHost, st));
     SIFT_CUDA(cudaStreamSynchronize(st));
@@ -375,10 +382,10 @@ int sift_mlp_hash(const uint8_t* x, uint32_t n, const sift_mlp* model, uint32_t*
 }
 
 int sift_mlp_match(const uint8_t* q, const uint8_t* r, uint32_t q_n, uint32_t r_n, const sift_mlp* model,
-                   int n_probes, int min_candidates, float threshold, uint32_t* matches, int32_t* nn_idx,
-                   float* nn_dist, uint32_t* candidates, uint32_t* fallback_count, void* stream) {
-    return sift::mlp_match(q, r, q_n, r_n, model, n_probes, min_candidates, threshold, matches, nn_idx, nn_dist,
-                           candidates, fallback_count, stream);
+                   int n_probes, int min_candidates, float max_dist, float threshold, uint32_t* matches,
+                   int32_t* nn_idx, float* nn_dist, uint32_t* candidates, uint32_t* fallback_count, void* stream) {
+    return sift::mlp_match(q, r, q_n, r_n, model, n_probes, min_candidates, max_dist, threshold, matches, nn_idx,
+                           nn_dist, candidates, fallback_count, stream);
 }
 
 int sift_mlp_train(const uint8_t* base, uint32_t r_n, const uint8_t* train_q, uint32_t t_n, int k, int steps,

@@ -110,6 +110,15 @@ def test_fallback_to_exact(cuda_device):
     dd = ((q[has].astype(np.int64) - r[idx[has, 0]].astype(np.int64)) ** 2).sum(1)
     np.testing.assert_array_equal(dd, dist[has, 0])
     assert (dist[has, 0] >= d[has, 0]).all()
+    # distance criterion: a query whose nearest candidate is farther than
+    # max_dist (or that found none) gets the exact answer; the rest keep theirs
+    plain = model.match(_dev(q, cuda_device), _dev(r, cuda_device), n_probes=4)["nn_dist"].cpu().numpy()
+    out2 = model.match(_dev(q, cuda_device), _dev(r, cuda_device), n_probes=4, max_dist=40000.0)
+    far = ~(plain[:, 0].astype(np.float64) <= 40000.0)
+    assert out2["fallback"] == far.sum() and 0 < far.sum() < 900
+    idx2 = out2["nn_idx"].cpu().numpy().astype(np.int64)
+    np.testing.assert_array_equal(idx2[far], i[far])
+    np.testing.assert_array_equal(out2["nn_dist"].cpu().numpy()[far].astype(np.int64), d[far])
 
 
 def test_training_is_deterministic_and_learns(cuda_device):
