@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 #include <vector>
@@ -65,6 +66,9 @@ int ensure_ready(DeviceCtx*& out, int& dev) {
             if (cudaMalloc(&c.d_status, 4 * sizeof(int)) != cudaSuccess) return SIFT_ERR_ALLOC;
             if (cudaMemset(c.d_status, 0, 4 * sizeof(int)) != cudaSuccess) return SIFT_ERR_CUDA;
             if (cudaMallocHost(&c.h_status, 4 * sizeof(int)) != cudaSuccess) return SIFT_ERR_ALLOC;
+            if (cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking) != cudaSuccess) return SIFT_ERR_CUDA;
+            for (auto& e : c.chunk_ev)
+                if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return SIFT_ERR_CUDA;
             if (cudaDeviceSynchronize() != cudaSuccess) return SIFT_ERR_CUDA;
             c.ready = true;
         }
@@ -290,6 +294,115 @@ int stage_inputs(DeviceCtx& c, char* A, const InputPlan& ip, int type, const voi
     return SIFT_OK;
 }
 
+// Host u8 inputs (U8_HOST) with a large base: the base is copied to the
+// device in kChunks chunks on the copy stream while the search kernel runs
+// on the chunks that have landed (records, then one persistent pair-kernel
+// launch per chunk); the per-query pruning bounds carry over from chunk to
+// chunk and one merge combines every chunk's partial lists. Same results as
+// the single-launch path. Caller holds c.mu.
+constexpr int kChunkMinRows = 1 << 16;
+constexpr int kChunks = 8;
+
+int exact_match_chunked(const MatchArgs& a, DeviceCtx& c, cudaStream_t st) {
+    const int q_n = static_cast<int>(a.q_n), r_n = static_cast<int>(a.r_n);
+    const int workers = c.num_sms / 2;
+    const ExactPlan whole = make_exact_plan(q_n, r_n, workers, 2);
+    const int chunk_rows = ((r_n + kChunks - 1) / kChunks + kBN - 1) / kBN * kBN;
+    const int n_chunks = (r_n + chunk_rows - 1) / chunk_rows;
+    if (n_chunks > kMaxChunks) return SIFT_ERR_INVALID_ARG;
+    ChunkSet cs{};
+    cs.n = n_chunks;
+    cs.r_n = r_n;
+    cs.parts = 2;
+    cs.q_pad = whole.q_pad;
+    ExactPlan plans[kMaxChunks];
+    long long slots = 1;
+    for (int ch = 0; ch < n_chunks; ++ch) {
+        const int rows = std::min(chunk_rows, r_n - ch * chunk_rows);
+        plans[ch] = make_exact_plan(q_n, rows, workers, 2);
+        cs.W[ch] = plans[ch].units;
+        cs.G[ch] = plans[ch].grid;
+        cs.tiles[ch] = plans[ch].base_tiles;
+        slots = std::max<long long>(slots, static_cast<long long>(plans[ch].max_splits) * plans[ch].parts);
+    }
+    cs.slot_stride = slots * whole.q_pad;
+
+    const bool m_dev = !a.matches || is_device_accessible(a.matches);
+    const bool s_dev = !a.sorted || is_device_accessible(a.sorted);
+    const bool i_dev = !a.nn_idx || is_device_accessible(a.nn_idx);
+    const bool d_dev = !a.nn_dist || is_device_accessible(a.nn_dist);
+    Layout L;
+    const size_t o_q = L.take(static_cast<size_t>(q_n) * kDim);
+    const size_t o_r = L.take(static_cast<size_t>(r_n) * kDim + 16);
+    const size_t o_brec = L.take(static_cast<size_t>(whole.base_tiles) * kRecInts * 4 + 16);
+    const size_t o_qnorm = L.take(static_cast<size_t>(whole.q_pad) * 4);
+    const size_t o_thr = L.take(static_cast<size_t>(whole.q_pad) * 4);
+    const size_t o_part = L.take(static_cast<size_t>(n_chunks) * cs.slot_stride * sizeof(int4));
+    const size_t o_m = (a.matches && !m_dev) ? L.take(static_cast<size_t>(q_n) * 4) : 0;
+    const size_t o_s = (a.sorted && !s_dev) ? L.take(static_cast<size_t>(q_n) * 16) : 0;
+    const size_t o_i = (a.nn_idx && !i_dev) ? L.take(static_cast<size_t>(q_n) * 8) : 0;
+    const size_t o_d = (a.nn_dist && !d_dev) ? L.take(static_cast<size_t>(q_n) * 8) : 0;
+    SIFT_TRY(ensure_arena(c, L.off));
+    char* A = c.arena;
+    uint8_t* qd = reinterpret_cast<uint8_t*>(A + o_q);
+    uint8_t* rd = reinterpret_cast<uint8_t*>(A + o_r);
+    int32_t* brec = reinterpret_cast<int32_t*>(A + o_brec);
+    int32_t* qnorm = reinterpret_cast<int32_t*>(A + o_qnorm);
+    int32_t* thresh = reinterpret_cast<int32_t*>(A + o_thr);
+    int4* partial = reinterpret_cast<int4*>(A + o_part);
+    const uint8_t* rh = static_cast<const uint8_t*>(a.r);
+
+    // Queries first, on the search stream; the base chunks on the copy stream
+    // once every earlier use of the arena on the search stream is done.
+    SIFT_CUDA(cudaMemcpyAsync(qd, a.q, static_cast<size_t>(q_n) * kDim, cudaMemcpyHostToDevice, st));
+    SIFT_CUDA(launch_row_norms_u8(qd, q_n, whole.q_pad, kMetricL2, qnorm, nullptr, thresh, st));
+    SIFT_CUDA(cudaEventRecord(c.chunk_ev[kMaxChunks], st));
+    SIFT_CUDA(cudaStreamWaitEvent(c.copy_stream, c.chunk_ev[kMaxChunks], 0));
+    for (int ch = 0; ch < n_chunks; ++ch) {
+        const size_t off = static_cast<size_t>(ch) * chunk_rows;
+        SIFT_CUDA(cudaMemcpyAsync(rd + off * kDim, rh + off * kDim, static_cast<size_t>(plans[ch].r_n) * kDim,
+                                  cudaMemcpyHostToDevice, c.copy_stream));
+        SIFT_CUDA(cudaEventRecord(c.chunk_ev[ch], c.copy_stream));
+    }
+    CUtensorMap qmap, bmap;
+    SIFT_TRY(encode_u8_rows(&qmap, qd, q_n, kBM));
+    SIFT_TRY(encode_u8_rows(&bmap, rd, r_n, kBN / 2));
+    for (int ch = 0; ch < n_chunks; ++ch) {
+        const int off = ch * chunk_rows;
+        SIFT_CUDA(cudaStreamWaitEvent(st, c.chunk_ev[ch], 0));
+        SIFT_CUDA(launch_row_norms_u8(rd + static_cast<size_t>(off) * kDim, plans[ch].r_n, plans[ch].r_pad, a.metric,
+                                      nullptr, brec + static_cast<size_t>(off / kBN) * kRecInts, nullptr, st));
+        WorkItem it{};
+        it.n_a = q_n;
+        it.b_off = off;
+        it.n_b = plans[ch].r_n;
+        it.groups = plans[ch].q_groups;
+        it.tiles = plans[ch].base_tiles;
+        it.rec_off = off / kBN;
+        it.idx_base = off;
+        SIFT_CUDA(launch_exact2nn_u8_pair_item(qmap, bmap, brec, plans[ch], it, partial + ch * cs.slot_stride, thresh,
+                                               c.d_status, st));
+    }
+    g_launches += 1 + 2 * n_chunks + 1;
+
+    uint32_t* m_out = (a.matches && !m_dev) ? reinterpret_cast<uint32_t*>(A + o_m) : a.matches;
+    float4* s_out = (a.sorted && !s_dev) ? reinterpret_cast<float4*>(A + o_s) : reinterpret_cast<float4*>(a.sorted);
+    int32_t* i_out = (a.nn_idx && !i_dev) ? reinterpret_cast<int32_t*>(A + o_i) : a.nn_idx;
+    float* d_out = (a.nn_dist && !d_dev) ? reinterpret_cast<float*>(A + o_d) : a.nn_dist;
+    SIFT_CUDA(launch_merge2nn_chunks(partial, cs, q_n, qnorm, a.metric, a.threshold, 1.0f, m_out, s_out, i_out, d_out,
+                                     st));
+    if (a.matches && !m_dev)
+        SIFT_CUDA(cudaMemcpyAsync(a.matches, m_out, static_cast<size_t>(q_n) * 4, cudaMemcpyDeviceToHost, st));
+    if (a.sorted && !s_dev)
+        SIFT_CUDA(cudaMemcpyAsync(a.sorted, s_out, static_cast<size_t>(q_n) * 16, cudaMemcpyDeviceToHost, st));
+    if (a.nn_idx && !i_dev)
+        SIFT_CUDA(cudaMemcpyAsync(a.nn_idx, i_out, static_cast<size_t>(q_n) * 8, cudaMemcpyDeviceToHost, st));
+    if (a.nn_dist && !d_dev)
+        SIFT_CUDA(cudaMemcpyAsync(a.nn_dist, d_out, static_cast<size_t>(q_n) * 8, cudaMemcpyDeviceToHost, st));
+    SIFT_CUDA(cudaStreamSynchronize(st));
+    return collect_device_status(c, st);
+}
+
 // Core of every exact entry point.
 int exact_match(const MatchArgs& a) {
     if (a.q_n > 0 && !a.q) return SIFT_ERR_INVALID_ARG;
@@ -310,6 +423,7 @@ int exact_match(const MatchArgs& a) {
     const bool use_pair = variant != 1;
     // Half inputs are searched as FP16 by the FP16 tensor-core kernel in place.
     const bool use_f16 = variant == 0 && a.type == SIFT_HALF_DEVICE;
+    if (use_pair && a.type == SIFT_U8_HOST && r_n >= kChunkMinRows) return exact_match_chunked(a, c, st);
     const ExactPlan plan = use_pair ? make_exact_plan(q_n, r_n, c.num_sms / 2, 2) : make_exact_plan(q_n, r_n, c.num_sms, 1);
 
     // Output placement: direct when the device can write the pointer, else staged.

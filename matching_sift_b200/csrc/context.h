@@ -25,6 +25,8 @@ struct DeviceCtx {
     size_t arena_bytes = 0;
     int* d_status = nullptr;  // [0] device error code, [1] pack flag / value stats [1..3]
     int* h_status = nullptr;  // pinned mirror of d_status
+    cudaStream_t copy_stream = nullptr;  // host->device chunk copies that overlap the search
+    cudaEvent_t chunk_ev[17] = {};       // per-chunk "landed" events + one "arena free" event
 };
 
 // 256-byte aligned bump layout over the arena.

@@ -490,7 +490,74 @@ __global__ void __launch_bounds__(256) merge2nn_kernel(const int4* __restrict__ 
     }
 }
 
+// Merge of a search split over base chunks (indices already global).
+__global__ void __launch_bounds__(256) merge2nn_chunks_kernel(const int4* __restrict__ partial, const ChunkSet cs,
+                                                              int q_n, const int32_t* __restrict__ qnorm, int metric,
+                                                              float thr, float dscale, uint32_t* __restrict__ matches,
+                                                              float4* __restrict__ sorted,
+                                                              int32_t* __restrict__ nn_idx,
+                                                              float* __restrict__ nn_dist) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= q_n) return;
+    int a1 = INT_MAX, j1 = -1, a2 = INT_MAX, j2 = -1;
+    auto push = [&](int k, int i) {
+        if (i < 0) return;
+        if (lex_less(k, i, a1, j1) || j1 < 0) {
+            a2 = a1; j2 = j1;
+            a1 = k; j1 = i;
+        } else if (lex_less(k, i, a2, j2) || j2 < 0) {
+            a2 = k; j2 = i;
+        }
+    };
+    const int g = q / (kQT * kBM);
+    for (int c = 0; c < cs.n; ++c) {
+        if (cs.W[c] <= 0 || cs.tiles[c] <= 0) continue;
+        const long long first = static_cast<long long>(g) * cs.tiles[c];
+        const int c0 = plan_cta_of(first, cs.W[c], cs.G[c]);
+        const int c1 = plan_cta_of(first + cs.tiles[c] - 1, cs.W[c], cs.G[c]);
+        const int4* pc = partial + c * cs.slot_stride;
+        for (int s = 0; s < (c1 - c0 + 1) * cs.parts; ++s) {
+            const int4 p = pc[static_cast<size_t>(s) * cs.q_pad + q];
+            push(p.x, p.y);
+            push(p.z, p.w);
+        }
+    }
+    const bool v1 = j1 >= 0 && j1 < cs.r_n && a1 < kKeyPad;
+    const bool v2 = j2 >= 0 && j2 < cs.r_n && a2 < kKeyPad;
+    const int qn = metric == kMetricL2 ? qnorm[q] : 0;
+    const float d1 = v1 ? static_cast<float>(a1 + qn) * dscale : FLT_MAX;
+    const float d2 = v2 ? static_cast<float>(a2 + qn) * dscale : FLT_MAX;
+    if (matches) {
+        bool pass = false;
+        if (v1) {
+            const float f1 = metric == kMetricL2 ? sqrtf(d1) : sqrtf(d1 + 2.0f);
+            const float f2 = v2 ? (metric == kMetricL2 ? sqrtf(d2) : sqrtf(d2 + 2.0f)) : INFINITY;
+            pass = (f1 / f2) < thr;
+        }
+        matches[q] = pass ? static_cast<uint32_t>(j1) : UINT32_MAX;
+    }
+    if (sorted)
+        sorted[q] = make_float4(d1, d2, v1 ? static_cast<float>(j1) : FLT_MAX, v2 ? static_cast<float>(j2) : FLT_MAX);
+    if (nn_idx) {
+        nn_idx[2 * q] = v1 ? j1 : -1;
+        nn_idx[2 * q + 1] = v2 ? j2 : -1;
+    }
+    if (nn_dist) {
+        nn_dist[2 * q] = d1;
+        nn_dist[2 * q + 1] = d2;
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_merge2nn_chunks(const int4* partial, const ChunkSet& cs, int q_n, const int32_t* qnorm, int metric,
+                                   float threshold, float dist_scale, uint32_t* matches, float4* sorted,
+                                   int32_t* nn_idx, float* nn_dist, cudaStream_t stream) {
+    if (q_n <= 0) return cudaSuccess;
+    merge2nn_chunks_kernel<<<(q_n + 255) / 256, 256, 0, stream>>>(partial, cs, q_n, qnorm, metric, threshold,
+                                                                  dist_scale, matches, sorted, nn_idx, nn_dist);
+    return cudaGetLastError();
+}
 
 ExactPlan make_exact_plan(int q_n, int r_n, int num_sms, int parts) {
     ExactPlan p{};

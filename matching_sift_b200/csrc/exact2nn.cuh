@@ -59,14 +59,17 @@ __host__ __device__ inline int plan_cta_of(long long w, long long W, long long G
 // (a_off = rows of the problems before it); base sets are any row ranges of
 // one base tensor. Units of problem p: groups x tiles, numbered from u_begin;
 // its base-tile records start at rec_off. A single search is the batch of one
-// problem {0, q_n, 0, r_n, 0, q_groups, base_tiles, 0}.
+// problem {0, q_n, 0, r_n, 0, q_groups, base_tiles, 0, 0}. idx_base is added
+// to every base index the kernel reports (0 for batches, whose indices are
+// local to the problem; the first row of a chunk when one base is searched
+// chunk by chunk).
 struct WorkItem {
     int a_off, n_a;
     int b_off, n_b;
     long long u_begin;
     int groups, tiles;
     int rec_off;
-    int pad_;
+    int idx_base;
 };
 static_assert(sizeof(WorkItem) == 40, "WorkItem layout");
 
@@ -129,6 +132,29 @@ cudaError_t launch_exact2nn_u8_pair(const CUtensorMap& qmap, const CUtensorMap& 
 cudaError_t launch_exact2nn_u8_pair_batch(const CUtensorMap& qmap, const CUtensorMap& bmap_half, const int32_t* brec,
                                           const BatchPlan& bp, int4* partial, int32_t* thresh, int* err, int qpt,
                                           int qbuf, cudaStream_t stream);
+// One search split over base chunks (launched chunk by chunk while later
+// chunks are still being copied in): chunk c's partial lists start at
+// partial + c * slot_stride, laid out by its own plan (W, G, tiles); indices
+// in them are global base rows.
+constexpr int kMaxChunks = 16;
+struct ChunkSet {
+    int n;
+    int r_n;
+    int parts;
+    int q_pad;
+    long long slot_stride;
+    long long W[kMaxChunks];
+    int G[kMaxChunks];
+    int tiles[kMaxChunks];
+};
+// The pair kernel over one explicit work item (a chunk of the base).
+cudaError_t launch_exact2nn_u8_pair_item(const CUtensorMap& qmap, const CUtensorMap& bmap_half, const int32_t* brec,
+                                         const ExactPlan& plan, const WorkItem& item, int4* partial, int32_t* thresh,
+                                         int* err, cudaStream_t stream);
+cudaError_t launch_merge2nn_chunks(const int4* partial, const ChunkSet& cs, int q_n, const int32_t* qnorm, int metric,
+                                   float threshold, float dist_scale, uint32_t* matches, float4* sorted,
+                                   int32_t* nn_idx, float* nn_dist, cudaStream_t stream);
+
 // Base-tile records of every problem of a batch (rows of base set p past
 // n_b[p] are padding), total_tiles records.
 cudaError_t launch_batch_records(const uint8_t* base, int base_rows, const BatchPlan& bp, int metric, int32_t* rec,

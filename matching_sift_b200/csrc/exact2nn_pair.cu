@@ -405,7 +405,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                     st.thr = min(st.thr, shared_thr);
                     const int32_t* rec = r_smem + s * kRecInts;
                     const int4 gm = *reinterpret_cast<const int4*>(rec + 144);
-                    const int row0 = j * kBN;
+                    const int row0 = cur.it.idx_base + j * kBN;
                     uint32_t va[32];
                     ptx::tmem_ld32(taddr, va);
                     ptx::tmem_ld_wait(va);
@@ -534,6 +534,18 @@ cudaError_t launch_exact2nn_u8_pair(const CUtensorMap& qmap, const CUtensorMap& 
     if (plan.grid <= 0) return cudaSuccess;
     exact2nn_u8_pair_kernel<<<2 * plan.grid, CfgU8::kThreads, CfgU8::kSmemBytes, stream>>>(
         qmap, bmap_half, brec, plan, single_item(plan), partial, thresh, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_exact2nn_u8_pair_item(const CUtensorMap& qmap, const CUtensorMap& bmap_half, const int32_t* brec,
+                                         const ExactPlan& plan, const WorkItem& item, int4* partial, int32_t* thresh,
+                                         int* err, cudaStream_t stream) {
+    static bool attr_set[64] = {};
+    cudaError_t e = set_smem_once(exact2nn_u8_pair_kernel, CfgU8::kSmemBytes, attr_set);
+    if (e != cudaSuccess) return e;
+    if (plan.grid <= 0) return cudaSuccess;
+    exact2nn_u8_pair_kernel<<<2 * plan.grid, CfgU8::kThreads, CfgU8::kSmemBytes, stream>>>(
+        qmap, bmap_half, brec, plan, item, partial, thresh, err);
     return cudaGetLastError();
 }
 
