@@ -47,6 +47,9 @@ __device__ __forceinline__ void top2_update(Top2& s, int key, int idx) {
 // group bound gmin32 - 2 max(v) first, then per 8-row subgroup
 // gmin8 - 2 max(v[8k..8k+8)). Both bound every key of their rows from below,
 // so a (sub)group whose bound exceeds the thread's threshold holds no candidate.
+// A passing subgroup forms its 8 exact keys and updates the top-2 only when
+// their minimum is within the threshold (a key above it cannot reach the
+// final top-2: the threshold never exceeds the final second-best key).
 __device__ __forceinline__ void scan_group(const uint32_t (&v)[32], int row0, int gmin32, const int32_t* nrm,
                                            const int32_t* gm8, Top2& s) {
     int mx[4];
@@ -64,15 +67,20 @@ __device__ __forceinline__ void scan_group(const uint32_t (&v)[32], int row0, in
                 if (ps) {
                     const int4 na = *reinterpret_cast<const int4*>(nrm + 8 * k);
                     const int4 nb = *reinterpret_cast<const int4*>(nrm + 8 * k + 4);
-                    const int base = row0 + 8 * k;
-                    top2_update(s, na.x - 2 * static_cast<int>(v[8 * k + 0]), base + 0);
-                    top2_update(s, na.y - 2 * static_cast<int>(v[8 * k + 1]), base + 1);
-                    top2_update(s, na.z - 2 * static_cast<int>(v[8 * k + 2]), base + 2);
-                    top2_update(s, na.w - 2 * static_cast<int>(v[8 * k + 3]), base + 3);
-                    top2_update(s, nb.x - 2 * static_cast<int>(v[8 * k + 4]), base + 4);
-                    top2_update(s, nb.y - 2 * static_cast<int>(v[8 * k + 5]), base + 5);
-                    top2_update(s, nb.z - 2 * static_cast<int>(v[8 * k + 6]), base + 6);
-                    top2_update(s, nb.w - 2 * static_cast<int>(v[8 * k + 7]), base + 7);
+                    const int nr[8] = {na.x, na.y, na.z, na.w, nb.x, nb.y, nb.z, nb.w};
+                    int key[8];
+                    #pragma unroll
+                    for (int e = 0; e < 8; ++e) key[e] = nr[e] - 2 * static_cast<int>(v[8 * k + e]);
+                    // Exact keys first; the (rare) updates only when one can enter.
+                    int mk = __vimin3_s32(key[0], key[1], key[2]);
+                    mk = __vimin3_s32(mk, key[3], key[4]);
+                    mk = __vimin3_s32(mk, key[5], key[6]);
+                    mk = min(mk, key[7]);
+                    if (mk <= s.thr) {
+                        const int base = row0 + 8 * k;
+                        #pragma unroll
+                        for (int e = 0; e < 8; ++e) top2_update(s, key[e], base + e);
+                    }
                 }
             }
         }

@@ -22,20 +22,24 @@
 // numbered problem by problem and every CTA pair owns a contiguous range; all
 // roles walk the same range with a Cursor.
 //
-// Warp roles (64 + 32 * 8 * QPT threads per CTA):
+// Warp roles (96 + 32 * 8 * QPT threads per CTA):
 //   warp 0       TMA producer (both CTAs): its own query rows, its half of
 //                each base tile (completion counted on the leader's barrier)
 //                and the full norms record of the tile (local barrier)
-//   warp 1       TMEM allocator (both CTAs); MMA issuer (leader CTA only)
+//   warp 1       TMEM allocator (both CTAs); MMA issuer of the even units
+//                (leader CTA only)
 //   warps 2..    epilogue (both CTAs): warp w owns query tile (w - 2) / 8,
 //                buffer ((w - 2) / 4) % 2 (so it scans every other unit, all
 //                128 columns) and TMEM lane quarter w % 4
+//   last warp    MMA issuer of the odd units (leader CTA only)
 //
-// The MMA issuer is the critical path: on sm_100a every mbarrier test and
-// every tcgen05.commit costs the issuing thread on the order of a hundred
-// cycles, against 64 cycles per 256 x 128 x 32 MMA. So per unit (8 MMAs) it
-// waits on one stage barrier and one accumulator barrier, both tested one unit
-// ahead so the test latency overlaps MMA issue, and commits once.
+// MMA issue: on sm_100a every mbarrier test and every tcgen05.commit costs
+// the issuing thread on the order of a hundred cycles, against 64 cycles per
+// 256 x 128 x 32 MMA, and one thread issuing every unit (8 MMAs, two barrier
+// tests, a commit) left the tensor pipe idle half of the time. Two issuer
+// threads, each owning one accumulator buffer (unit parity), share the work;
+// each tests its next unit's barriers behind its queued MMAs and commits once
+// per unit.
 //
 // Barriers and who signals them (L = only the leader's copy is used):
 //   full[s]    (L) both CTAs' base halves of stage s landed        TMA tx
@@ -44,7 +48,7 @@
 //              done: its MMAs completed (they waited on tfull) and its
 //              record is no longer read (per CTA)                  arrive
 //   qfull[b]   (L) query tiles of both CTAs landed in buffer b      TMA tx
-//   qempty[b]  MMAs of the group in query buffer b done (both CTAs) commit, multicast
+//   qempty[b]  MMAs of the group in query buffer b done (both CTAs) commit x 2 (one per issuer), multicast
 //   tfull[b]   both query tiles' accumulators of buffer b done      commit, multicast
 //   tempty[b]  (L) the 8 warps of buffer b in each CTA read it      remote arrive
 // Every wait is bounded (2 s); an expired wait raises the CTA's abort flag
@@ -96,11 +100,14 @@ struct PairCfg {
     static constexpr int kBHalfBytes = kKBlocks * kBKBlock;  // 8 / 16 KB
     static constexpr int kSlots = 2 * QPT;                   // (query tile, buffer)
     static constexpr int kEpiWarps = 4 * kSlots;             // one per (slot, lane quarter)
-    static constexpr int kThreads = 64 + 32 * kEpiWarps;
+    static constexpr int kMma2Warp = 2 + kEpiWarps;          // second MMA issuer (odd units)
+    static constexpr int kThreads = 64 + 32 * kEpiWarps + 32;
     static constexpr int kTmemCols = kSlots * kBN;
     static constexpr int kStagesFit =
         static_cast<int>((kPSmemBudget - 1024 - 512 - QB * kQBufBytes) / (kBHalfBytes + kPRecBytes));
-    static constexpr int kStages = kStagesFit < 12 ? kStagesFit : 12;
+    // 16 stages when they fit (a power of two keeps the ring index cheap in
+    // the issue loop), else as many as fit.
+    static constexpr int kStages = kStagesFit >= 16 ? 16 : kStagesFit;
     struct __align__(8) Ctl {
         uint64_t full[kStages];
         uint64_t rfull[kStages];
@@ -219,13 +226,13 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
         }
         for (int b = 0; b < QB; ++b) {
             ptx::mbar_init(bar_qfull + 8 * b, 1);
-            ptx::mbar_init(bar_qempty + 8 * b, 1);
+            ptx::mbar_init(bar_qempty + 8 * b, 2);  // one commit per MMA issuer
         }
         for (int b = 0; b < 2; ++b) {
             ptx::mbar_init(bar_tfull + 8 * b, 1);
             ptx::mbar_init(bar_tempty + 8 * b, 2 * kPEpiWarps / 2);  // the warps of buffer b in each CTA
         }
-        ptx::mbar_init(bar_drain, 1);
+        ptx::mbar_init(bar_drain, 2);
         ctl->abort_flag = 0;
         ctl->no_abort = 0;
         ptx::fence_mbar_init();
@@ -297,18 +304,20 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                 ptx::mbar_wait_cluster(bar_qempty + 8 * (k % QB), (k / QB) & 1, never, err, kErrWaitDrain);
         }
         __syncwarp();
-    } else if (warp == 1) {
+    } else if (warp == 1 || warp == Cfg::kMma2Warp) {
         if (lane == 0 && leader) {
-            // -------------------------------------------------- MMA issuer
+            // ------------------------------------------------- MMA issuers
+            // Thread mt issues the units n with n % 2 == mt (accumulator
+            // buffer mt); both walk every unit to follow the query groups.
+            const int mt = warp == 1 ? 0 : 1;
             constexpr uint32_t idesc = Cfg::kIdesc;
             const uint64_t b_desc0 = ptx::sdesc_sw128(b_s);
             int ngroups = 0;
             bool new_group = true;
             uint64_t a_desc0 = ptx::sdesc_sw128(q_s);
             int qb = 0;
-            // Barrier tests of unit n issued while unit n - 1's MMAs are issued.
-            bool pre_full = ptx::mbar_try_wait(bar_full, 0);
-            bool pre_tempty = ptx::mbar_try_wait(bar_tempty, 1);
+            bool pre_full = ptx::mbar_test_wait(bar_full + 8 * (mt % kPStages), 0);
+            bool pre_tempty = ptx::mbar_test_wait(bar_tempty + 8 * mt, 1);
             for (int n = 0; n < n_units; ++n) {
                 if (new_group) {
                     qb = ngroups % QB;
@@ -317,41 +326,44 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                     a_desc0 = ptx::sdesc_sw128(q_s + qb * Cfg::kQBufBytes);
                     ++ngroups;
                 }
-                const int s = n % kPStages;
-                const int buf = n & 1;
-                if (!pre_full &&
-                    !ptx::mbar_wait_cluster(bar_full + 8 * s, (n / kPStages) & 1, abort_flag, err, kErrWaitMmaFull))
-                    break;
-                if (!pre_tempty && !ptx::mbar_wait_cluster(bar_tempty + 8 * buf, ((n >> 1) & 1) ^ 1, abort_flag, err,
-                                                           kErrWaitMmaTmem))
-                    break;
-                ptx::tc_fence_after();
-                const uint64_t b_desc = b_desc0 + static_cast<uint64_t>((s * kPBHalfBytes) >> 4);
-                #pragma unroll
-                for (int t = 0; t < QPT; ++t) {
-                    const uint32_t d = tmem + (t * 2 + buf) * kBN;
+                if ((n & 1) == mt) {
+                    const int s = n % kPStages;
+                    if (!pre_full &&
+                        !ptx::mbar_wait_cluster(bar_full + 8 * s, (n / kPStages) & 1, abort_flag, err, kErrWaitMmaFull))
+                        break;
+                    if (!pre_tempty && !ptx::mbar_wait_cluster(bar_tempty + 8 * mt, ((n >> 1) & 1) ^ 1, abort_flag,
+                                                               err, kErrWaitMmaTmem))
+                        break;
+                    ptx::tc_fence_after();
+                    const uint64_t b_desc = b_desc0 + static_cast<uint64_t>((s * kPBHalfBytes) >> 4);
                     #pragma unroll
-                    for (int kb = 0; kb < Cfg::kKBlocks; ++kb) {
-                        const uint64_t a_desc =
-                            a_desc0 + static_cast<uint64_t>((t * kPQTileBytes + kb * Cfg::kQKBlock) >> 4);
-                        const uint64_t b_kb = b_desc + static_cast<uint64_t>((kb * Cfg::kBKBlock) >> 4);
+                    for (int t = 0; t < QPT; ++t) {
+                        const uint32_t d = tmem + (t * 2 + mt) * kBN;
                         #pragma unroll
-                        for (int kk = 0; kk < 4; ++kk) {
-                            const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
-                            if constexpr (F16)
-                                ptx::mma_f16_pair(d, a_desc + 2 * kk, b_kb + 2 * kk, idesc, acc);
-                            else
-                                ptx::mma_i8_pair(d, a_desc + 2 * kk, b_kb + 2 * kk, idesc, acc);
+                        for (int kb = 0; kb < Cfg::kKBlocks; ++kb) {
+                            const uint64_t a_desc =
+                                a_desc0 + static_cast<uint64_t>((t * kPQTileBytes + kb * Cfg::kQKBlock) >> 4);
+                            const uint64_t b_kb = b_desc + static_cast<uint64_t>((kb * Cfg::kBKBlock) >> 4);
+                            #pragma unroll
+                            for (int kk = 0; kk < 4; ++kk) {
+                                const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
+                                if constexpr (F16)
+                                    ptx::mma_f16_pair(d, a_desc + 2 * kk, b_kb + 2 * kk, idesc, acc);
+                                else
+                                    ptx::mma_i8_pair(d, a_desc + 2 * kk, b_kb + 2 * kk, idesc, acc);
+                            }
                         }
                     }
+                    ptx::tc_commit_pair_mc(bar_tfull + 8 * mt, kPairMask);
+                    // Test the barriers of this issuer's next unit (n + 2) behind its queued MMAs.
+                    if (n + 2 < n_units) {
+                        pre_full = ptx::mbar_test_wait(bar_full + 8 * ((n + 2) % kPStages), ((n + 2) / kPStages) & 1);
+                        pre_tempty = ptx::mbar_test_wait(bar_tempty + 8 * mt, (((n + 2) >> 1) & 1) ^ 1);
+                    }
                 }
-                ptx::tc_commit_pair_mc(bar_tfull + 8 * buf, kPairMask);
+                // Both issuers release the query buffer at the end of a group
+                // (each commit covers that issuer's own MMAs).
                 if (n + 1 == n_units || cur.last_of_group()) ptx::tc_commit_pair_mc(bar_qempty + 8 * qb, kPairMask);
-                // Test the barriers of unit n + 1 now, behind this unit's queued MMAs.
-                if (n + 1 < n_units) {
-                    pre_full = ptx::mbar_try_wait(bar_full + 8 * ((n + 1) % kPStages), ((n + 1) / kPStages) & 1);
-                    pre_tempty = ptx::mbar_try_wait(bar_tempty + 8 * (buf ^ 1), (((n + 1) >> 1) & 1) ^ 1);
-                }
                 new_group = cur.next();
             }
             // Drain: all issued MMAs complete before TMEM is released.
