@@ -9,7 +9,9 @@
 // 128-byte swizzle (the layout TMA writes for the weights; the epilogue warps
 // write the activations in the same layout themselves).
 //
-// Warps: 0 = weight TMA, TMEM allocation, MMA issue (one thread);
+// Warps: 0 = weight and input-tile TMA, TMEM allocation, MMA issue (one
+//            thread); the u8 input tiles stream through a 2-stage ring,
+//            loaded two tiles ahead;
 //        1..4 = conversion and epilogue, thread = tile row (TMEM lane).
 // Per tile i (epilogue threads):
 //   convert x(i) -> x_s      [x_ready]     MMA1: TMEM[0,256) = x W1^T
@@ -33,16 +35,20 @@ constexpr int kW2Bytes = kMlpOutRows * kMlpHidden * 2;  // 16 KB
 constexpr int kXBytes = 128 * kMlpIn * 2;               // 32 KB
 constexpr int kHBytes = 128 * kMlpHidden * 2;           // 64 KB
 constexpr uint32_t kLTmemCols = 512;
+constexpr int kXStages = 2;                             // u8 input tile ring
+constexpr int kXTileBytes = 128 * kMlpIn;               // 16 KB
 
 struct __align__(8) MlpCtl {
     uint64_t w_full, x_ready, h_ready, m1, m2, drain;
+    uint64_t xfull[kXStages];
     uint32_t tmem_base;
     int abort_flag, no_abort;
     float b1[kMlpHidden];
     float b2[kMlpOutRows];
 };
 
-constexpr size_t kLSmemBytes = 1024 + kW1Bytes + kW2Bytes + kXBytes + kHBytes + sizeof(MlpCtl);
+constexpr size_t kLSmemBytes = 1024 + kW1Bytes + kW2Bytes + kXBytes + kHBytes + kXStages * kXTileBytes + sizeof(MlpCtl);
+static_assert(kLSmemBytes <= 227 * 1024, "MLP hash shared memory");
 
 // Byte offset of the 16-byte chunk `ch` (0..7) of row r in a K block of a
 // SW128 K-major tile (rows of 128 bytes, 8-row atoms).
@@ -55,13 +61,12 @@ __device__ __forceinline__ uint32_t bf16x2(float a, float b) {
     return *reinterpret_cast<const uint32_t*>(&h);
 }
 
-// Row r of the tile starting at global row g0 -> BF16 K blocks of x_s.
-__device__ __forceinline__ void convert_row(const uint8_t* __restrict__ x, int n, int g0, int r, uint8_t* x_s) {
-    const int g = g0 + r;
-    const uint4* src = reinterpret_cast<const uint4*>(x + static_cast<size_t>(g) * kMlpIn);
+// Row r of a u8 tile in shared memory (TMA, 128-byte swizzle; rows past the
+// end of the input are zeros) -> BF16 K blocks of x_s.
+__device__ __forceinline__ void convert_row(const uint8_t* u8_tile, int r, uint8_t* x_s) {
     #pragma unroll
     for (int c = 0; c < 8; ++c) {
-        const uint4 v = g < n ? __ldg(src + c) : make_uint4(0, 0, 0, 0);
+        const uint4 v = *reinterpret_cast<const uint4*>(u8_tile + sw128_off(r, c));
         const uint32_t w[4] = {v.x, v.y, v.z, v.w};
         uint32_t o[8];
         #pragma unroll
@@ -78,7 +83,7 @@ __device__ __forceinline__ void convert_row(const uint8_t* __restrict__ x, int n
 }
 
 __global__ void __launch_bounds__(kLThreads, 1)
-    mlp_hash_kernel(const uint8_t* __restrict__ x, int n, const __grid_constant__ CUtensorMap w1map,
+    mlp_hash_kernel(const __grid_constant__ CUtensorMap xmap, int n, const __grid_constant__ CUtensorMap w1map,
                     const __grid_constant__ CUtensorMap w2map, const float* __restrict__ b1,
                     const float* __restrict__ b2, int k, uint32_t* __restrict__ codes, float* __restrict__ zout,
                     int* __restrict__ err) {
@@ -89,7 +94,8 @@ __global__ void __launch_bounds__(kLThreads, 1)
     uint8_t* w2_s = w1_s + kW1Bytes;
     uint8_t* x_s = w2_s + kW2Bytes;
     uint8_t* h_s = x_s + kXBytes;
-    MlpCtl* ctl = reinterpret_cast<MlpCtl*>(h_s + kHBytes);
+    uint8_t* xr_s = h_s + kHBytes;  // u8 tile ring
+    MlpCtl* ctl = reinterpret_cast<MlpCtl*>(xr_s + kXStages * kXTileBytes);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tiles = (n + 127) / 128;
     const int bx = static_cast<int>(blockIdx.x), gx = static_cast<int>(gridDim.x);
@@ -105,6 +111,7 @@ __global__ void __launch_bounds__(kLThreads, 1)
         ptx::mbar_init(bar_m1, 1);
         ptx::mbar_init(bar_m2, 1);
         ptx::mbar_init(bar_drain, 1);
+        for (int s = 0; s < kXStages; ++s) ptx::mbar_init(ptx::smem_u32(&ctl->xfull[s]), 1);
         ctl->abort_flag = 0;
         ctl->no_abort = 0;
         ptx::fence_mbar_init();
@@ -123,11 +130,18 @@ __global__ void __launch_bounds__(kLThreads, 1)
     volatile int* never = &ctl->no_abort;
     const uint32_t w1_a = ptx::smem_u32(w1_s), w2_a = ptx::smem_u32(w2_s);
     const uint32_t x_a = ptx::smem_u32(x_s), h_a = ptx::smem_u32(h_s);
+    const uint32_t xr_a = ptx::smem_u32(xr_s), bar_xf = ptx::smem_u32(&ctl->xfull[0]);
 
     if (warp == 0) {
         if (lane == 0 && my_tiles > 0) {
             ptx::tma_prefetch_desc(&w1map);
             ptx::tma_prefetch_desc(&w2map);
+            ptx::tma_prefetch_desc(&xmap);
+            int issued = 0;  // input tiles whose TMA load has been issued
+            for (; issued < kXStages && issued < my_tiles; ++issued) {
+                ptx::mbar_arrive_expect_tx(bar_xf + 8 * issued, kXTileBytes);
+                ptx::tma_load_2d(xr_a + issued * kXTileBytes, &xmap, 0, (bx + issued * gx) * 128, bar_xf + 8 * issued);
+            }
             ptx::mbar_arrive_expect_tx(bar_w, kW1Bytes + kW2Bytes);
             for (int kb = 0; kb < 2; ++kb) ptx::tma_load_2d(w1_a + kb * (kMlpHidden * 128), &w1map, kb * 64, 0, bar_w);
             for (int kb = 0; kb < 4; ++kb) ptx::tma_load_2d(w2_a + kb * (kMlpOutRows * 128), &w2map, kb * 64, 0, bar_w);
@@ -147,6 +161,13 @@ __global__ void __launch_bounds__(kLThreads, 1)
                                      (kb | kk) ? 1u : 0u);
                 }
                 ptx::tc_commit(bar_m1);
+                // Tile i's u8 stage was converted (x_ready): reuse it for tile i + 2.
+                if (issued < my_tiles) {
+                    const int st = issued % kXStages;
+                    ptx::mbar_arrive_expect_tx(bar_xf + 8 * st, kXTileBytes);
+                    ptx::tma_load_2d(xr_a + st * kXTileBytes, &xmap, 0, (bx + issued * gx) * 128, bar_xf + 8 * st);
+                    ++issued;
+                }
                 if (!ptx::mbar_wait(bar_h, i & 1, abort_flag, err, kErrWaitMmaTmem)) break;
                 ptx::tc_fence_after();
                 #pragma unroll
@@ -160,6 +181,9 @@ __global__ void __launch_bounds__(kLThreads, 1)
                 ptx::tc_commit(bar_m2);
             }
             if (!ok) ptx::mbar_wait(bar_w, 0, never, err, kErrWaitDrain);  // weights landed before exit
+            // Input tiles in flight land before exit (the last kXStages issued).
+            for (int t = (issued > kXStages ? issued - kXStages : 0); t < issued; ++t)
+                ptx::mbar_wait(bar_xf + 8 * (t % kXStages), (t / kXStages) & 1, never, err, kErrWaitDrain);
             ptx::tc_commit(bar_drain);
             ptx::mbar_wait(bar_drain, 0, never, err, kErrWaitDrain);
         }
@@ -168,12 +192,14 @@ __global__ void __launch_bounds__(kLThreads, 1)
         const int quarter = warp & 3;
         const int r = quarter * 32 + lane;  // tile row = TMEM lane
         const uint32_t lane_base = static_cast<uint32_t>(quarter * 32) << 16;
+        bool conv_ok = true;
         if (my_tiles > 0) {
-            convert_row(x, n, bx * 128, r, x_s);
+            conv_ok = ptx::mbar_wait(bar_xf, 0, abort_flag, err, kErrWaitEpilogue);
+            if (conv_ok) convert_row(xr_s, r, x_s);
             ptx::fence_proxy_async();
             ptx::mbar_arrive(bar_x);
         }
-        for (int i = 0; i < my_tiles; ++i) {
+        for (int i = 0; i < my_tiles && __all_sync(0xffffffffu, conv_ok); ++i) {
             const int g0 = (bx + i * gx) * 128;
             bool waited = ptx::mbar_wait(bar_m1, i & 1, abort_flag, err, kErrWaitEpilogue);
             if (!__all_sync(0xffffffffu, waited)) break;
@@ -202,7 +228,9 @@ __global__ void __launch_bounds__(kLThreads, 1)
             ptx::fence_proxy_async();
             ptx::mbar_arrive(bar_h);
             if (i + 1 < my_tiles) {
-                convert_row(x, n, (bx + (i + 1) * gx) * 128, r, x_s);
+                const int st = (i + 1) % kXStages;
+                conv_ok = ptx::mbar_wait(bar_xf + 8 * st, ((i + 1) / kXStages) & 1, abort_flag, err, kErrWaitEpilogue);
+                if (conv_ok) convert_row(xr_s + st * kXTileBytes, r, x_s);
                 ptx::fence_proxy_async();
                 ptx::mbar_arrive(bar_x);
             }
@@ -287,7 +315,7 @@ __global__ void probe_codes_kernel(const uint32_t* __restrict__ codes, const flo
 
 size_t mlp_hash_smem_bytes() { return kLSmemBytes; }
 
-cudaError_t launch_mlp_hash(const uint8_t* x, int n, const CUtensorMap& w1map, const CUtensorMap& w2map,
+cudaError_t launch_mlp_hash(const CUtensorMap& xmap, int n, const CUtensorMap& w1map, const CUtensorMap& w2map,
                             const float* b1, const float* b2, int k, uint32_t* codes, float* z, int* err,
                             int num_sms, cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
@@ -296,7 +324,7 @@ cudaError_t launch_mlp_hash(const uint8_t* x, int n, const CUtensorMap& w1map, c
     if (e != cudaSuccess) return e;
     const int tiles = (n + 127) / 128;
     const int grid = tiles < num_sms ? tiles : num_sms;
-    mlp_hash_kernel<<<grid, kLThreads, kLSmemBytes, stream>>>(x, n, w1map, w2map, b1, b2, k, codes, z, err);
+    mlp_hash_kernel<<<grid, kLThreads, kLSmemBytes, stream>>>(xmap, n, w1map, w2map, b1, b2, k, codes, z, err);
     return cudaGetLastError();
 }
 

@@ -29,9 +29,10 @@ struct MlpModel {
     int k;
 };
 
-// Codes (and optionally z, [n][k] floats) of n u8 rows. w1map: the W1 tensor
-// map (dims {128, 256}, box {64, 256}); w2map: W2 (dims {256, k}, box {64, 32}).
-cudaError_t launch_mlp_hash(const uint8_t* x, int n, const CUtensorMap& w1map, const CUtensorMap& w2map,
+// Codes (and optionally z, [n][k] floats) of n u8 rows. xmap: the rows (u8,
+// box 128 x 128, 128-byte swizzle); w1map: the W1 tensor map (dims {128, 256},
+// box {64, 256}); w2map: W2 (dims {256, k}, box {64, 32}).
+cudaError_t launch_mlp_hash(const CUtensorMap& xmap, int n, const CUtensorMap& w1map, const CUtensorMap& w2map,
                             const float* b1, const float* b2, int k, uint32_t* codes, float* z, int* err,
                             int num_sms, cudaStream_t stream);
 size_t mlp_hash_smem_bytes();

@@ -95,7 +95,9 @@ int mlp_hash(const uint8_t* x, uint32_t n, const sift_mlp* model, uint32_t* code
     const MlpModel m = to_model(model);
     CUtensorMap w1map, w2map;
     SIFT_TRY(encode_model(m, &w1map, &w2map));
-    SIFT_CUDA(launch_mlp_hash(x, static_cast<int>(n), w1map, w2map, m.b1, m.b2, m.k, codes, z, cp->d_status,
+    CUtensorMap xmap;
+    SIFT_TRY(detail::encode_u8_rows(&xmap, x, n, 128));
+    SIFT_CUDA(launch_mlp_hash(xmap, static_cast<int>(n), w1map, w2map, m.b1, m.b2, m.k, codes, z, cp->d_status,
                               cp->num_sms, static_cast<cudaStream_t>(stream)));
     ++detail::g_launches;
     return SIFT_OK;
@@ -165,7 +167,10 @@ int mlp_match(const uint8_t* q, const uint8_t* r, uint32_t q_n_, uint32_t r_n_, 
     SIFT_TRY(encode_model(m, &w1map, &w2map));
     int launches = 0;
     if (r_n > 0) {
-        SIFT_CUDA(launch_mlp_hash(r, r_n, w1map, w2map, m.b1, m.b2, k, U32(o_cr), nullptr, c.d_status, c.num_sms, st));
+        CUtensorMap rmap;
+        SIFT_TRY(detail::encode_u8_rows(&rmap, r, r_n, 128));
+        SIFT_CUDA(launch_mlp_hash(rmap, r_n, w1map, w2map, m.b1, m.b2, k, U32(o_cr), nullptr, c.d_status, c.num_sms,
+                                  st));
         SIFT_CUDA(launch_lsh_buckets(U32(o_cr), r_n, 1, shift, nbins, I32(o_hist), I32(o_start), I32(o_order),
                                      U32(o_ocode), c.num_sms, st));
         SIFT_CUDA(launch_row_norms_u8(r, r_n, r_pad, kMetricL2, I32(o_rn), nullptr, nullptr, st));
@@ -174,7 +179,9 @@ int mlp_match(const uint8_t* q, const uint8_t* r, uint32_t q_n_, uint32_t r_n_, 
         SIFT_CUDA(cudaMemsetAsync(I32(o_start), 0, static_cast<size_t>(nbins + 1) * 4, st));
     }
     SIFT_CUDA(launch_row_norms_u8(q, q_n, q_pad, kMetricL2, I32(o_qn), nullptr, nullptr, st));
-    SIFT_CUDA(launch_mlp_hash(q, q_n, w1map, w2map, m.b1, m.b2, k, U32(o_cq), reinterpret_cast<float*>(A + o_z),
+    CUtensorMap qmap_h;
+    SIFT_TRY(detail::encode_u8_rows(&qmap_h, q, q_n, 128));
+    SIFT_CUDA(launch_mlp_hash(qmap_h, q_n, w1map, w2map, m.b1, m.b2, k, U32(o_cq), reinterpret_cast<float*>(A + o_z),
                               c.d_status, c.num_sms, st));
     SIFT_CUDA(launch_probe_codes(U32(o_cq), reinterpret_cast<float*>(A + o_z), q_n, k, flip, n_probes, U32(o_pc), st));
     SIFT_CUDA(launch_lsh_scan(q, r, q_n, r_n, 1, n_probes, shift, nbins, U32(o_pc), I32(o_start), I32(o_order),

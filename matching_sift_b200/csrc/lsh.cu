@@ -176,8 +176,15 @@ __global__ void __launch_bounds__(kHThreads, 1)
                 for (int t = 0; t < L; ++t) {
                     const int bit0 = t * k;
                     const int w = bit0 >> 5, sh = bit0 & 31;
-                    uint64_t pair = static_cast<uint64_t>(mask[w]);
-                    if (w + 1 < 8) pair |= static_cast<uint64_t>(mask[w + 1]) << 32;
+                    // mask[w], mask[w + 1] by selects (register-resident, no indexed access)
+                    uint32_t lo = mask[0], hi = mask[1];
+                    #pragma unroll
+                    for (int u = 1; u < 8; ++u) {
+                        lo = w == u ? mask[u] : lo;
+                        hi = w + 1 == u ? mask[u] : hi;
+                    }
+                    if (w + 1 >= 8) hi = 0;
+                    const uint64_t pair = static_cast<uint64_t>(lo) | (static_cast<uint64_t>(hi) << 32);
                     const uint32_t code = static_cast<uint32_t>(pair >> sh) & (k == 32 ? 0xffffffffu : ((1u << k) - 1));
                     codes[static_cast<size_t>(t) * n + point] = code;
                 }
