@@ -59,54 +59,98 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed
+    region: NVML polled every 5 ms from a thread (read-only queries), else
+    nvidia-smi every 200 ms. The timed regions last tens of milliseconds, so
+    the 200 ms tool alone sees one sample at most."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, period_s: float = 0.005):
         self.gpu = gpu_index
-        self.rows = []
+        self.period = period_s
+        self.rows = []  # (sm_mhz, max_mhz, set of reason names)
         self.proc = None
         self._t = None
+        self._stop = threading.Event()
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            u = str(torch.cuda.get_device_properties(self.gpu).uuid)
+            return pynvml.nvmlDeviceGetHandleByUUID(u if u.startswith("GPU-") else "GPU-" + u)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+
+    def _poll_nvml(self, nv, h):
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        while not self._stop.is_set():
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((sm, mx, {n for n, b in bits.items() if r & b}))
+            except Exception:
+                pass
+            self._stop.wait(self.period)
 
     def __enter__(self):
+        try:
+            import pynvml
+            h = self._nvml_handle()
+            self._t = threading.Thread(target=self._poll_nvml, args=(pynvml, h), daemon=True)
+            self._t.start()
+            self.source = "nvml"
+            return self
+        except Exception:
+            self._t = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t = threading.Thread(target=self._read_smi, daemon=True)
             self._t.start()
+            self.source = "nvidia-smi"
         except OSError:
             self.proc = None
         return self
 
-    def _read(self):
+    def _read_smi(self):
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                self.rows.append(parts)
+            if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                mx = float(parts[2]) if parts[2].replace(".", "").isdigit() else float("nan")
+                self.rows.append((float(parts[1]), mx,
+                                  {self.NAMES[k] for k in range(4) if parts[5 + k].lower() == "active"}))
 
     def __exit__(self, *exc):
+        self._stop.set()
         if self.proc is not None:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-            if self._t is not None:
-                self._t.join(timeout=2)
+        if self._t is not None:
+            self._t.join(timeout=2)
 
     def summary(self):
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[5 + k].lower() == "active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+        sm = [r[0] for r in self.rows]
+        mx = [r[1] for r in self.rows if r[1] == r[1]]
+        reasons = sorted(set().union(*(r[2] for r in self.rows)))
+        return {"sm_mhz": float(np.median(sm)), "sm_min_mhz": min(sm), "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows), "source": self.source}
 
 
 def _profile_value(name, key):

@@ -42,27 +42,26 @@ __device__ __forceinline__ void top2_update(Top2& s, int key, int idx) {
 }
 
 // One group of 32 consecutive base rows [row0, row0 + 32) for this thread's
-// query row; v[c] = q.b(row0 + c); rec points at the group's 32 norms in the
-// shared-memory record, gm8 at its four 8-row minima. Two-level pruning: the
-// group bound gmin32 - 2 max(v) first, then per 8-row subgroup
-// gmin8 - 2 max(v[8k..8k+8)). Both bound every key of their rows from below,
-// so a (sub)group whose bound exceeds the thread's threshold holds no candidate.
-// A passing subgroup forms its 8 exact keys and updates the top-2 only when
-// their minimum is within the threshold (a key above it cannot reach the
-// final top-2: the threshold never exceeds the final second-best key).
-__device__ __forceinline__ void scan_group(const uint32_t (&v)[32], int row0, int gmin32, const int32_t* nrm,
-                                           const int32_t* gm8, Top2& s) {
+// query row; v[c] = q.b(row0 + c); nrm points at the group's 32 norms in the
+// shared-memory record, gm8 at its four 8-row minima. Each 8-row subgroup is
+// bounded from below by gm8[k] - 2 max(v[8k..8k+8)) (no key of its rows is
+// smaller), so a subgroup whose bound exceeds the thread's threshold holds no
+// candidate; the four bounds are tested with one vote. A passing subgroup
+// forms its 8 exact keys and updates the top-2 only when their minimum is
+// within the threshold (a key above it cannot reach the final top-2: the
+// threshold never exceeds the final second-best key).
+__device__ __forceinline__ void scan_group(const uint32_t (&v)[32], int row0, const int32_t* nrm, const int32_t* gm8,
+                                           Top2& s) {
     int mx[4];
     #pragma unroll
     for (int k = 0; k < 4; ++k) mx[k] = max8(v + 8 * k);
-    const int m = max(__vimax3_s32(mx[0], mx[1], mx[2]), mx[3]);
-    const bool pass = (gmin32 - 2 * m) <= s.thr;
-    if (__any_sync(0xffffffffu, pass)) {
-        const int4 g8 = *reinterpret_cast<const int4*>(gm8);
-        const int gs[4] = {g8.x, g8.y, g8.z, g8.w};
+    const int4 g8 = *reinterpret_cast<const int4*>(gm8);
+    const int bnd[4] = {g8.x - 2 * mx[0], g8.y - 2 * mx[1], g8.z - 2 * mx[2], g8.w - 2 * mx[3]};
+    const int bmin = min(__vimin3_s32(bnd[0], bnd[1], bnd[2]), bnd[3]);
+    if (__any_sync(0xffffffffu, bmin <= s.thr)) {
         #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            const bool ps = pass && (gs[k] - 2 * mx[k]) <= s.thr;
+            const bool ps = bnd[k] <= s.thr;
             if (__any_sync(0xffffffffu, ps)) {
                 if (ps) {
                     const int4 na = *reinterpret_cast<const int4*>(nrm + 8 * k);

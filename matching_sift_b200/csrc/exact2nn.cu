@@ -29,14 +29,14 @@
 //   warps 2..17  epilogue: warp w owns query tile (w - 2) / 4 and TMEM lane
 //                quarter w % 4, i.e. 32 query rows, one thread per row
 //
-// Epilogue pruning. Per group of 32 base rows a thread takes the largest dot
-// product m of its query row; with n_min the smallest norm of the group
-// (precomputed), n_min - 2 m is a lower bound of every key in the group. If it
-// exceeds the thread's threshold the group is skipped (~0.7 instruction per
-// element); otherwise the same test runs per 8-row subgroup and only passing
-// subgroups form exact keys. The threshold is the thread's own second-best key
-// and an upper bound of the final second-best key that the CTAs splitting the
-// same query group share through global memory (atomicMin).
+// Epilogue pruning. Per 8-row subgroup of base rows a thread takes the largest
+// dot product m of its query row; with n_min the smallest norm of the subgroup
+// (precomputed), n_min - 2 m is a lower bound of every key in it. A group of
+// 32 rows (four subgroups, one vote) whose four bounds all exceed the thread's
+// threshold is skipped (~0.8 instruction per element); otherwise only the
+// passing subgroups form exact keys. The threshold is the thread's own
+// second-best key and an upper bound of the final second-best key that the
+// CTAs splitting the same query group share through global memory (atomicMin).
 #include <cfloat>
 #include <climits>
 #include <algorithm>
@@ -112,8 +112,7 @@ __global__ void __launch_bounds__(256) row_norms_kernel(const T* __restrict__ x,
     s += __shfl_xor_sync(0xffffffffu, s, 4);
     const int32_t v = row < n ? (metric == kMetricL2 ? static_cast<int32_t>(s) : 0) : kKeyPad;
     __shared__ int32_t nrm[32];
-    // Record of base tile (row / kBN): [0, 128) norms, [128, 144) 8-row minima,
-    // [144, 148) 32-row minima.
+    // Record of base tile (row / kBN): [0, 128) norms, [128, 144) 8-row minima.
     int32_t* r = rec ? rec + static_cast<size_t>(blockIdx.x / 4) * kRecInts : nullptr;
     const int part = blockIdx.x & 3;  // which 32-row quarter of the tile
     if (sub == 0) {
@@ -128,12 +127,6 @@ __global__ void __launch_bounds__(256) row_norms_kernel(const T* __restrict__ x,
         #pragma unroll
         for (int i = 1; i < 8; ++i) m = min(m, nrm[8 * threadIdx.x + i]);
         r[128 + part * 4 + threadIdx.x] = m;
-    }
-    if (threadIdx.x == 32 && r) {
-        int m = nrm[0];
-        #pragma unroll
-        for (int i = 1; i < 32; ++i) m = min(m, nrm[i]);
-        r[144 + part] = m;
     }
 }
 
@@ -185,12 +178,6 @@ __global__ void __launch_bounds__(256) batch_records_kernel(const uint8_t* __res
         #pragma unroll
         for (int i = 1; i < 8; ++i) m = min(m, nrm[8 * threadIdx.x + i]);
         r[128 + part * 4 + threadIdx.x] = m;
-    }
-    if (threadIdx.x == 32) {
-        int m = nrm[0];
-        #pragma unroll
-        for (int i = 1; i < 32; ++i) m = min(m, nrm[i]);
-        r[144 + part] = m;
     }
 }
 
@@ -380,24 +367,23 @@ __global__ void __launch_bounds__(kThreads, 1)
                 ptx::tc_fence_after();
                 st.thr = min(st.thr, shared_thr);
                 const int32_t* rec = r_smem + s * kRecInts;
-                const int4 gm = *reinterpret_cast<const int4*>(rec + 144);
                 const int row0 = j * kBN;
                 uint32_t va[32];
                 ptx::tmem_ld32(taddr0, va);
                 ptx::tmem_ld_wait(va);
-                scan_group(va, row0, gm.x, rec, rec + 128, st);
+                scan_group(va, row0, rec, rec + 128, st);
                 ptx::tmem_ld32(taddr0 + 32, va);
                 ptx::tmem_ld_wait(va);
-                scan_group(va, row0 + 32, gm.y, rec + 32, rec + 132, st);
+                scan_group(va, row0 + 32, rec + 32, rec + 132, st);
                 ptx::tmem_ld32(taddr0 + 64, va);
                 ptx::tmem_ld_wait(va);
-                scan_group(va, row0 + 64, gm.z, rec + 64, rec + 136, st);
+                scan_group(va, row0 + 64, rec + 64, rec + 136, st);
                 ptx::tmem_ld32(taddr0 + 96, va);
                 ptx::tmem_ld_wait(va);
                 ptx::tc_fence_before();
                 __syncwarp();
                 if (lane == 0) ptx::mbar_arrive(bar_tempty + 8 * t);
-                scan_group(va, row0 + 96, gm.w, rec + 96, rec + 140, st);
+                scan_group(va, row0 + 96, rec + 96, rec + 140, st);
                 if (st.k2 < published) {
                     atomicMin(thresh + q, st.k2);
                     published = st.k2;

@@ -16,7 +16,7 @@ constexpr int kEpiWarps = 4 * kQT;   // one epilogue warp per (query tile, TMEM 
 constexpr int kThreads = 64 + 32 * kEpiWarps;
 constexpr int kTmemCols = kQT * kBN; // one accumulator slot of kBN columns per query tile
 constexpr int32_t kKeyPad = 1 << 30; // ranking key of padding rows (never a real key)
-constexpr int kRecInts = 160;        // per-base-tile record: 128 norms, 16 8-row minima, 4 32-row minima, pad
+constexpr int kRecInts = 160;        // per-base-tile record: 128 norms, 16 8-row minima, pad
 
 // Distance definitions of the exact path.
 enum Metric : int {
@@ -101,9 +101,8 @@ ExactPlan make_exact_plan(int q_n, int r_n, int num_workers, int parts);
 // Per-row squared norms of u8 descriptors (or zeros for kMetricDot), padded
 // to n_pad rows (a multiple of kBN) with kKeyPad. Outputs (each optional):
 //   norm[n_pad]                       plain per-row norms
-//   rec[n_pad / kBN][kRecInts]        per base tile of kBN rows: the 128 norms,
-//                                     the 16 minima over 8-row groups and the
-//                                     4 minima over 32-row groups
+//   rec[n_pad / kBN][kRecInts]        per base tile of kBN rows: the 128 norms
+//                                     and the 16 minima over 8-row groups
 //   thresh[n_pad]                     set to INT_MAX (the per-query shared
 //                                     pruning bound of the search kernel)
 cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* norm, int32_t* rec,

@@ -416,28 +416,27 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                 if (active) {
                     st.thr = min(st.thr, shared_thr);
                     const int32_t* rec = r_smem + s * kRecInts;
-                    const int4 gm = *reinterpret_cast<const int4*>(rec + 144);
                     const int row0 = cur.it.idx_base + j * kBN;
                     uint32_t va[32];
                     ptx::tmem_ld32(taddr, va);
                     ptx::tmem_ld_wait(va);
                     if constexpr (F16) f32_to_dot(va, dscale);
-                    scan_group(va, row0, gm.x, rec, rec + 128, st);
+                    scan_group(va, row0, rec, rec + 128, st);
                     ptx::tmem_ld32(taddr + 32, va);
                     ptx::tmem_ld_wait(va);
                     if constexpr (F16) f32_to_dot(va, dscale);
-                    scan_group(va, row0 + 32, gm.y, rec + 32, rec + 132, st);
+                    scan_group(va, row0 + 32, rec + 32, rec + 132, st);
                     ptx::tmem_ld32(taddr + 64, va);
                     ptx::tmem_ld_wait(va);
                     if constexpr (F16) f32_to_dot(va, dscale);
-                    scan_group(va, row0 + 64, gm.z, rec + 64, rec + 136, st);
+                    scan_group(va, row0 + 64, rec + 64, rec + 136, st);
                     ptx::tmem_ld32(taddr + 96, va);
                     ptx::tmem_ld_wait(va);
                     if constexpr (F16) f32_to_dot(va, dscale);
                     ptx::tc_fence_before();
                     __syncwarp();
                     if (lane == 0) ptx::mbar_arrive_cluster_relaxed(lead_tempty);
-                    scan_group(va, row0 + 96, gm.w, rec + 96, rec + 140, st);
+                    scan_group(va, row0 + 96, rec + 96, rec + 140, st);
                     if (valid && st.k2 < published) {
                         atomicMin(thresh + q, st.k2);
                         published = st.k2;
