@@ -214,7 +214,13 @@ def main():
     ap.add_argument("--queries", type=int, default=Q_N, help="queries per GPU (profiling of smaller cases)")
     ap.add_argument("--no-variants", action="store_true",
                     help="skip the FP16, batched-pairs, learned-hash and LSH legs")
+    ap.add_argument("--base-file", help="base descriptors (.fvecs/.bvecs, e.g. ANN_SIFT1M sift_base.fvecs; "
+                                        "the first 1,000,000 rows) instead of the seeded generator")
+    ap.add_argument("--query-file", help="query descriptors (.fvecs/.bvecs; the first --queries rows)")
+    ap.add_argument("--truth-file", help="ground truth (.ivecs) for recall of the exact matches")
     args = ap.parse_args()
+    if bool(args.base_file) != bool(args.query_file):
+        ap.error("--base-file and --query-file go together")
     args.warmup = max(args.warmup, 3)
 
     world = _env_int("WORLD_SIZE", 1)
@@ -237,8 +243,17 @@ def main():
     from matching_sift_b200 import datagen
 
     q_n = args.queries
-    base = datagen.make_base(R_N, seed=0)
-    queries = datagen.make_queries(q_n, base, seed=rank)
+    if args.base_file:
+        from matching_sift_b200 import vecs
+
+        base = vecs.to_u8(vecs.read_vecs(args.base_file, count=R_N, dim=DIM))
+        queries = vecs.to_u8(vecs.read_vecs(args.query_file, count=q_n, dim=DIM))
+        data_note = (f"descriptor files {os.path.basename(args.base_file)} (first {R_N:,} rows) and "
+                     f"{os.path.basename(args.query_file)} (first {q_n:,} rows; the same queries on every rank)")
+    else:
+        base = datagen.make_base(R_N, seed=0)
+        queries = datagen.make_queries(q_n, base, seed=rank)
+        data_note = "synthetic (seeded generator standing in for ANN_SIFT1M; base seed 0, queries seed = rank)"
     lib = ms.lib()
 
     qd = torch.from_numpy(queries).to(dev)
@@ -357,7 +372,7 @@ def main():
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "u8",
-            "data": "synthetic (seeded generator standing in for ANN_SIFT1M; base seed 0, queries seed = rank)",
+            "data": data_note,
             "config": {"workload": WORKLOAD if q_n == Q_N else WORKLOAD.replace("10,000", f"{q_n:,}"),
                        "queries_per_gpu": q_n, "base_rows": R_N, "dim": DIM,
                        "ratio": THRESHOLD, "l2_between_steps": "flushed (256 MiB write outside the timed events)",
@@ -375,6 +390,14 @@ def main():
                          "frac_of_2x_bf16_" + peak_src: round(achieved / bf16x2, 4)},
             "clocks": clocks.summary(),
         }
+        if args.truth_file:
+            from matching_sift_b200 import vecs
+
+            truth = vecs.read_ivecs(args.truth_file, count=q_n)
+            line["recall_vs_truth"] = {
+                "nn1_recall@1": round(vecs.recall_at(nn_idx[:, 0].cpu().numpy(), truth, 1), 6),
+                "ratio_test_match_misses": vecs.recall_misses(matches.cpu().numpy().view(np.uint32), truth),
+                "file": os.path.basename(args.truth_file)}
         if "pairs" in variants:
             v = variants["pairs"]
             pk_ms = v["step_ms"] / v["steps"]
