@@ -161,6 +161,19 @@ SIFT_API int sift_lsh_match(const void* q, const void* r, int type, uint32_t q_n
                             int L, int k, float threshold, uint32_t* matches, int32_t* nn_idx, float* nn_dist,
                             void* stream);
 
+/* sift_lsh_match with query-directed multi-probe (the reference declares but
+   never implements neighbouring-bucket search, include/lsh_h.h:71 /
+   src/lsh_h.cu:393-407): per table the query also searches the buckets of
+   its code with subsets of its min(6, k) lowest-margin bits flipped (margin =
+   |q . plane|), the `probes` lightest subsets by summed margin, probe 0 the
+   code itself; 1 <= probes <= 2^min(6, k). candidates (optional device
+   [q_n]) receives the number of base rows compared per query (duplicates
+   across tables counted once per table). */
+SIFT_API int sift_lsh_match_probes(const void* q, const void* r, int type, uint32_t q_n, uint32_t r_n,
+                                   const int8_t* planes, int L, int k, int probes, float threshold,
+                                   uint32_t* matches, int32_t* nn_idx, float* nn_dist, uint32_t* candidates,
+                                   void* stream);
+
 /* Exact 2-NN that allocates no memory at all (no counterpart in the
    reference). For callers that cannot allocate device memory at call time:
    code whose device memory is owned by a custom allocator or pool, real-time
@@ -199,6 +212,32 @@ typedef struct sift_pair {
 SIFT_API int sift2nn_match_batch(const uint8_t* q, const uint8_t* r, uint32_t r_rows, const sift_pair* pairs,
                                  int n_pairs, float threshold, uint32_t* matches, int32_t* nn_idx, float* nn_dist,
                                  void* stream);
+
+/* Mutual nearest neighbours (cross-check) of the problems of a batch, e.g.
+   the two keypoint sets of each image pair: a holds every problem's first set
+   (consecutive, in problem order; `pairs` as in sift2nn_match_batch with
+   n_q = rows of the set in a), b the second sets at r_off. Both directions
+   run through the batched exact search; matches[row] (required) = j, local to
+   the problem's set in b, when j is the nearest row of b for that row of a,
+   that row is the nearest row of a for row j of b, and -- when threshold > 0
+   -- the forward ratio test passes; else UINT32_MAX. nn_idx / nn_dist
+   (optional) receive the forward 2-NN as in sift2nn_match_batch. Sets of b
+   that are not stored consecutively in problem order are gathered first.
+   No counterpart in the reference (which matches one direction per call). */
+SIFT_API int sift2nn_match_mutual_batch(const uint8_t* a, const uint8_t* b, uint32_t b_rows, const sift_pair* pairs,
+                                        int n_pairs, float threshold, uint32_t* matches, int32_t* nn_idx,
+                                        float* nn_dist, void* stream);
+
+/* Merge of 2-NN results searched over `parts` disjoint base shards (e.g. one
+   per rank of a base-sharded search, after an all-gather): nn_dist_parts /
+   nn_idx_parts are [parts][q_n][2] device arrays as sift2nn_match writes them
+   (indices local to the shard, -1 / FLT_MAX absent), offsets[parts] (host)
+   the first base row of each shard. Writes the lexicographic (distance,
+   global index) top-2 of every query and the ratio test at `threshold`, the
+   same result as one search over the whole base. parts <= 64. */
+SIFT_API int sift_merge_top2(const float* nn_dist_parts, const int32_t* nn_idx_parts, const int32_t* offsets,
+                             int parts, uint32_t q_n, float threshold, uint32_t* matches, int32_t* nn_idx,
+                             float* nn_dist, void* stream);
 
 /* A batch bound to fixed buffers, replayed as one CUDA graph: create times
    the kernel shapes on this batch when flags has SIFT_BATCH_TUNE (the choice

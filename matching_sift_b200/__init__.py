@@ -21,7 +21,8 @@ from ._native import (SIFT_BATCH_SHAPE, SIFT_BATCH_TUNE, SIFT_MLP_PARAMS, sift_m
 
 __all__ = [
     "cublas_2nn_sift", "cublas_2nn_f", "device_brute", "host_brute", "lsh_gpu", "match", "lsh_match", "lsh_hash",
-    "stream_status", "version", "match_batch", "BatchPlan", "batch_describe", "MlpHash", "mlp_loss_grad",
+    "stream_status", "version", "match_batch", "match_mutual", "match_mutual_batch", "BatchPlan", "batch_describe",
+    "MlpHash", "mlp_loss_grad",
     "SiftError", "FLOAT_HOST", "FLOAT_DEVICE", "HALF_DEVICE", "U8_DEVICE", "U8_HOST", "METRIC_L2", "METRIC_DOT",
 ]
 
@@ -91,7 +92,8 @@ def match(q, r, threshold: float = 0.8, metric: int = METRIC_L2, stream=None, ou
     FP16 kernel in place; float32 rows are packed to u8 first. Float values
     must be integers in [0, 255] times one common power of two.
     Returns a dict with the requested outputs as CUDA tensors: ``matches``
-    (int64 view of uint32; UINT32_MAX where the ratio test fails), ``nn_idx``
+    (uint32 -- an int32 tensor viewed as uint32 where torch has that dtype;
+    UINT32_MAX where the ratio test fails), ``nn_idx``
     [n, 2] int32 (-1 absent), ``nn_dist`` [n, 2] float32, ``sorted`` [n, 4].
     Asynchronous on ``stream`` (a torch.cuda.Stream or None for the current one)
     for uint8 inputs; float inputs synchronise once to validate the values.
@@ -141,11 +143,15 @@ def lsh_hash(x, planes, stream=None):
     return codes
 
 
-def lsh_match(q, r, planes, threshold: float = 0.0, stream=None):
+def lsh_match(q, r, planes, threshold: float = 0.0, stream=None, probes: int = 1, candidates: bool = False):
     """LSH 2-NN of uint8 CUDA tensors with int8 hyperplanes planes [L, k, 128].
 
     Returns {"matches", "nn_idx", "nn_dist"} like match(); only base rows
-    sharing a code with the query in some table are candidates.
+    sharing a code with the query in some table are candidates. probes > 1
+    also searches, per table, the buckets of the query's code with its
+    lowest-margin bits flipped (query-directed multi-probe, up to
+    2^min(6, k) codes); candidates=True adds "candidates", the base rows
+    compared per query.
     """
     import torch
 
@@ -155,10 +161,13 @@ def lsh_match(q, r, planes, threshold: float = 0.0, stream=None):
     out = {"matches": torch.empty(n, dtype=torch.int32, device=q.device),
            "nn_idx": torch.empty((n, 2), dtype=torch.int32, device=q.device),
            "nn_dist": torch.empty((n, 2), dtype=torch.float32, device=q.device)}
+    if candidates:
+        out["candidates"] = torch.empty(n, dtype=torch.int32, device=q.device)
     s = stream if stream is not None else torch.cuda.current_stream(q.device)
-    check(lib().sift_lsh_match(q.data_ptr(), r.data_ptr(), U8_DEVICE, n, r.shape[0], planes.data_ptr(), L, k,
-                               threshold, out["matches"].data_ptr(), out["nn_idx"].data_ptr(),
-                               out["nn_dist"].data_ptr(), s.cuda_stream), "sift_lsh_match")
+    check(lib().sift_lsh_match_probes(q.data_ptr(), r.data_ptr(), U8_DEVICE, n, r.shape[0], planes.data_ptr(), L, k,
+                                      probes, threshold, out["matches"].data_ptr(), out["nn_idx"].data_ptr(),
+                                      out["nn_dist"].data_ptr(), _ptr(out.get("candidates")), s.cuda_stream),
+          "sift_lsh_match_probes")
     return out
 
 
@@ -200,6 +209,38 @@ def match_batch(q, r, pairs, threshold: float = 0.8, stream=None):
                                     _ptr(out["matches"]), _ptr(out["nn_idx"]), _ptr(out["nn_dist"]), s.cuda_stream),
           "sift2nn_match_batch")
     return out
+
+
+def match_mutual_batch(a, b, pairs, threshold: float = 0.8, stream=None):
+    """Mutual nearest neighbours of the two sets of many problems (image
+    pairs) in two batched searches and one cross-check.
+
+    a: uint8 CUDA tensor, every problem's first set concatenated in order;
+    b: uint8 CUDA tensor holding the second sets; pairs: rows {n_a, n_b,
+    b_off}. Returns {"matches", "nn_idx", "nn_dist"} per row of a: matches[i]
+    = j (local to the problem's set in b) for mutual nearest neighbours that
+    pass the forward ratio test when threshold > 0, else 0xFFFFFFFF; nn_idx and
+    nn_dist are the forward 2-NN.
+    """
+    import torch
+
+    pa = _pairs_array(pairs)
+    total = int(pa[:, 0].sum()) if len(pa) else 0
+    if a.shape[0] != total:
+        raise ValueError(f"a has {a.shape[0]} rows, the pairs {total}")
+    out = _batch_outputs(total, a.device)
+    s = stream if stream is not None else torch.cuda.current_stream(a.device)
+    check(lib().sift2nn_match_mutual_batch(_ptr(a), _ptr(b), b.shape[0], pa.ctypes.data, len(pa), threshold,
+                                           _ptr(out["matches"]), _ptr(out["nn_idx"]), _ptr(out["nn_dist"]),
+                                           s.cuda_stream),
+          "sift2nn_match_mutual_batch")
+    return out
+
+
+def match_mutual(a, b, threshold: float = 0.8, stream=None):
+    """Mutual nearest neighbours of one pair of descriptor sets (uint8 CUDA
+    tensors [n, 128]); see match_mutual_batch."""
+    return match_mutual_batch(a, b, [[a.shape[0], b.shape[0], 0]], threshold, stream)
 
 
 class BatchPlan:

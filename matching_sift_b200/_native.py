@@ -43,12 +43,19 @@ _PROTOS = {
     "lsh_gpu": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, _vp, ctypes.c_float, _vp,
                                ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "sift_lsh_hash": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "sift_lsh_match_probes": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, _vp,
+                                             ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, _vp, _vp, _vp,
+                                             _vp, _vp]),
     "sift_lsh_match": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, _vp, ctypes.c_int,
                                       ctypes.c_int, ctypes.c_float, _vp, _vp, _vp, _vp]),
     "sift2nn_match_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, _vp, _vp,
                                              _vp, _vp]),
     "sift2nn_match_batch": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_int, ctypes.c_float, _vp, _vp,
                                            _vp, _vp]),
+    "sift_merge_top2": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_float, _vp, _vp, _vp,
+                                       _vp]),
+    "sift2nn_match_mutual_batch": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_int, ctypes.c_float, _vp,
+                                                  _vp, _vp, _vp]),
     "sift_batch_plan_create": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_int, ctypes.c_float, _vp, _vp,
                                               _vp, ctypes.c_int, ctypes.POINTER(_vp)]),
     "sift_batch_plan_run": (ctypes.c_int, [_vp, _vp]),

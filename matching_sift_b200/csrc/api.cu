@@ -18,6 +18,7 @@
 #include "exact2nn.cuh"
 #include "pack.cuh"
 #include "lsh.cuh"
+#include "learned.cuh"
 #include <cstdlib>
 
 namespace sift {
@@ -540,6 +541,11 @@ int encode_i8_rows(CUtensorMap* m, const void* base, uint64_t rows, uint32_t box
 int lsh_match(const LshArgs& a) {
     if (a.L < 1 || a.k < 1 || a.k > 32 || a.L * a.k > kLshMaxPlanes || !a.planes) return SIFT_ERR_INVALID_ARG;
     if (a.q_n > 0x7fffffffu / 32 || a.r_n > 0x7fffffffu / 32) return SIFT_ERR_INVALID_ARG;
+    // Multi-probe flips subsets of the min(6, k) lowest-margin bits: at most 2^flip distinct codes.
+    const int flip = a.k < 6 ? a.k : 6;
+    if (a.probes < 1 || a.probes > (1 << flip)) return SIFT_ERR_INVALID_ARG;
+    if (a.candidates && !is_device_accessible(a.candidates)) return SIFT_ERR_INVALID_ARG;
+    if (static_cast<long long>(a.q_n) * a.L * (a.k + a.probes) > 0x7fffffffLL) return SIFT_ERR_INVALID_ARG;
     DeviceCtx* cp = nullptr;
     int dev = 0;
     SIFT_TRY(ensure_ready(cp, dev));
@@ -565,6 +571,9 @@ int lsh_match(const LshArgs& a) {
     const size_t o_pl = planes_dev ? 0 : L.take(static_cast<size_t>(L_) * k * kDim);
     const size_t o_cr = L.take(static_cast<size_t>(L_) * r_n * 4 + 16);
     const size_t o_cq = L.take(static_cast<size_t>(L_) * q_n * 4);
+    const bool multi = a.probes > 1;
+    const size_t o_z = multi ? L.take(static_cast<size_t>(L_) * q_n * k * 4) : 0;
+    const size_t o_pc = multi ? L.take(static_cast<size_t>(L_) * a.probes * q_n * 4) : 0;
     const size_t o_hist = L.take(static_cast<size_t>(L_) * nbins * 4);
     const size_t o_start = L.take(static_cast<size_t>(L_) * (nbins + 1) * 4);
     const size_t o_order = L.take(static_cast<size_t>(L_) * r_n * 4 + 16);
@@ -603,17 +612,29 @@ int lsh_match(const LshArgs& a) {
     SIFT_TRY(encode_u8_rows(&qmap, qd, q_n, 128));
     if (r_n > 0) {
         SIFT_TRY(encode_u8_rows(&rmap, rd, r_n, 128));
-        SIFT_CUDA(launch_lsh_hash(rmap, pmap, r_n, P, L_, k, codes_r, c.d_status, c.num_sms, st));
+        SIFT_CUDA(launch_lsh_hash(rmap, pmap, r_n, P, L_, k, codes_r, nullptr, c.d_status, c.num_sms, st));
         ++g_launches;
     }
-    SIFT_CUDA(launch_lsh_hash(qmap, pmap, q_n, P, L_, k, codes_q, c.d_status, c.num_sms, st));
+    float* zq = multi ? reinterpret_cast<float*>(A + o_z) : nullptr;
+    SIFT_CUDA(launch_lsh_hash(qmap, pmap, q_n, P, L_, k, codes_q, zq, c.d_status, c.num_sms, st));
+    const uint32_t* probe_codes = codes_q;
+    if (multi) {
+        // Per table: the query's code with the lightest subsets of its
+        // lowest-margin bits flipped, [t][probe][query] as the scan reads them.
+        uint32_t* pc = reinterpret_cast<uint32_t*>(A + o_pc);
+        for (int t = 0; t < L_; ++t)
+            SIFT_CUDA(launch_probe_codes(codes_q + static_cast<size_t>(t) * q_n, zq + static_cast<size_t>(t) * q_n * k,
+                                         q_n, k, flip, a.probes, pc + static_cast<size_t>(t) * a.probes * q_n, st));
+        g_launches += L_;
+        probe_codes = pc;
+    }
     SIFT_CUDA(launch_lsh_buckets(codes_r, r_n, L_, shift, nbins, hist, start, order, ocode, c.num_sms, st));
     uint32_t* m_out = (a.matches && !m_dev) ? reinterpret_cast<uint32_t*>(A + o_m) : a.matches;
     int32_t* i_out = (a.nn_idx && !i_dev) ? reinterpret_cast<int32_t*>(A + o_i) : a.nn_idx;
     float* d_out = (a.nn_dist && !d_dev) ? reinterpret_cast<float*>(A + o_d) : a.nn_dist;
-    SIFT_CUDA(launch_lsh_scan(qd, rd, q_n, r_n, L_, 1, shift, nbins, codes_q, start, order, ocode, qnorm, rnorm,
-                              a.threshold, a.ratio ? 1 : 0, ldexpf(1.0f, -2 * vshift), m_out, nullptr, i_out, d_out,
-                              st));
+    SIFT_CUDA(launch_lsh_scan(qd, rd, q_n, r_n, L_, a.probes, shift, nbins, probe_codes, start, order, ocode, qnorm,
+                              rnorm, a.threshold, a.ratio ? 1 : 0, ldexpf(1.0f, -2 * vshift), m_out, a.candidates,
+                              i_out, d_out, st));
     g_launches += 1 + (r_n > 0 ? 3 : 0) + 1;
     if (a.matches && !m_dev)
         SIFT_CUDA(cudaMemcpyAsync(a.matches, m_out, static_cast<size_t>(q_n) * 4, cudaMemcpyDeviceToHost, st));
@@ -644,7 +665,7 @@ int lsh_hash(const uint8_t* x, uint32_t n, const int8_t* planes, int L_, int k, 
     CUtensorMap pmap, xmap;
     SIFT_TRY(encode_i8_rows(&pmap, planes, static_cast<uint64_t>(L_) * k, static_cast<uint32_t>(P)));
     SIFT_TRY(encode_u8_rows(&xmap, x, n, 128));
-    SIFT_CUDA(launch_lsh_hash(xmap, pmap, static_cast<int>(n), P, L_, k, codes, cp->d_status, cp->num_sms,
+    SIFT_CUDA(launch_lsh_hash(xmap, pmap, static_cast<int>(n), P, L_, k, codes, nullptr, cp->d_status, cp->num_sms,
                               static_cast<cudaStream_t>(stream)));
     ++g_launches;
     return SIFT_OK;
@@ -775,6 +796,17 @@ int sift_stream_status(void* stream) { return sift::stream_status(stream); }
 
 int sift_lsh_hash(const uint8_t* x, uint32_t n, const int8_t* planes, int L, int k, uint32_t* codes, void* stream) {
     return sift::lsh_hash(x, n, planes, L, k, codes, stream);
+}
+
+int sift_lsh_match_probes(const void* q, const void* r, int type, uint32_t q_n, uint32_t r_n, const int8_t* planes,
+                          int L, int k, int probes, float threshold, uint32_t* matches, int32_t* nn_idx,
+                          float* nn_dist, uint32_t* candidates, void* stream) {
+    sift::LshArgs a{};
+    a.q = q; a.r = r; a.type = type; a.q_n = q_n; a.r_n = r_n; a.planes = planes; a.L = L; a.k = k;
+    a.probes = probes; a.candidates = candidates;
+    a.threshold = threshold; a.ratio = threshold > 0.0f; a.matches = matches; a.nn_idx = nn_idx; a.nn_dist = nn_dist;
+    a.stream = stream; a.sync = false;
+    return sift::lsh_match(a);
 }
 
 int sift_lsh_match(const void* q, const void* r, int type, uint32_t q_n, uint32_t r_n, const int8_t* planes, int L,

@@ -31,6 +31,8 @@ struct LshArgs {
     int L = 1, k = 16;
     float threshold = 0.8f;
     bool ratio = false;  // apply the ratio test to `matches`
+    int probes = 1;      // buckets searched per table (query-directed multi-probe when > 1)
+    uint32_t* candidates = nullptr;  // optional device [q_n]: base rows compared per query
     uint32_t* matches = nullptr;
     int32_t* nn_idx = nullptr;
     float* nn_dist = nullptr;

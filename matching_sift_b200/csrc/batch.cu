@@ -189,6 +189,132 @@ int match_batch(const uint8_t* q, const uint8_t* r, uint32_t r_rows, const sift_
     return enqueue(c, q, r, r_rows, b, m, kShapes[shape], threshold, matches, nn_idx, nn_dist, st);
 }
 
+// Largest p with off[p] <= i over a non-decreasing off[0..n) (empty
+// problems share the offset of the next one, so p is the problem owning row i).
+__device__ __forceinline__ int owner_of(const int* __restrict__ off, int n, int i) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Rows of every problem's base set, in problem order, as one query array of
+// the reverse search: row k of the output is row k - b_row[p] of set p.
+__global__ void gather_sets_kernel(const uint8_t* __restrict__ b, const int* __restrict__ b_row,
+                                   const int* __restrict__ r_off, int n_pairs, int total, uint8_t* __restrict__ out) {
+    const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int k = static_cast<int>(t >> 3), part = static_cast<int>(t & 7);
+    if (k >= total) return;
+    const int p = owner_of(b_row, n_pairs, k);
+    const size_t src = static_cast<size_t>(r_off[p]) + (k - b_row[p]);
+    reinterpret_cast<uint4*>(out + static_cast<size_t>(k) * kDim)[part] =
+        reinterpret_cast<const uint4*>(b + src * kDim)[part];
+}
+
+// Mutual check: row i of a (problem p, local row li = i - a_off[p]) keeps its
+// nearest base row j (local to set p) when the reverse search of row j of set
+// p found li as its nearest row, and (ratio) the forward ratio test passed.
+__global__ void cross_check_kernel(const int32_t* __restrict__ nn_fwd, const uint32_t* __restrict__ m_fwd,
+                                   const int32_t* __restrict__ nn_rev, const int* __restrict__ a_off,
+                                   const int* __restrict__ b_row, int n_pairs, int total_a, int ratio,
+                                   uint32_t* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total_a) return;
+    const int p = owner_of(a_off, n_pairs, i);
+    const int j = nn_fwd[2 * static_cast<size_t>(i)];
+    uint32_t res = 0xffffffffu;
+    if (j >= 0 && (!ratio || m_fwd[i] != 0xffffffffu) &&
+        nn_rev[2 * (static_cast<size_t>(b_row[p]) + j)] == i - a_off[p])
+        res = static_cast<uint32_t>(j);
+    out[i] = res;
+}
+
+int match_mutual_batch(const uint8_t* a, const uint8_t* b, uint32_t b_rows, const sift_pair* pairs, int n_pairs,
+                       float threshold, uint32_t* matches, int32_t* nn_idx, float* nn_dist, void* stream) {
+    DeviceCtx* cp = nullptr;
+    int dev = 0;
+    SIFT_TRY(detail::ensure_ready(cp, dev));
+    DeviceCtx& c = *cp;
+    if (!matches || n_pairs < 0 || (n_pairs > 0 && !pairs)) return SIFT_ERR_INVALID_ARG;
+    // Reverse problems: set p of b searched against rows of problem p of a.
+    std::vector<sift_pair> rev(n_pairs);
+    std::vector<int> a_off(n_pairs + 1), b_row(n_pairs), r_off(n_pairs);
+    long long arow = 0, brow = 0;
+    bool contiguous = true;
+    for (int p = 0; p < n_pairs; ++p) {
+        if (brow > 0x7fffffffLL - 1024 || arow > 0x7fffffffLL - 1024) return SIFT_ERR_INVALID_ARG;
+        rev[p] = sift_pair{pairs[p].n_r, pairs[p].n_q, static_cast<uint32_t>(arow)};
+        a_off[p] = static_cast<int>(arow);
+        b_row[p] = static_cast<int>(brow);
+        r_off[p] = static_cast<int>(pairs[p].r_off);
+        if (pairs[p].r_off != brow) contiguous = false;
+        arow += pairs[p].n_q;
+        brow += pairs[p].n_r;
+    }
+    if (brow > 0x7fffffffLL - 1024 || arow > 0x7fffffffLL - 1024) return SIFT_ERR_INVALID_ARG;
+    a_off[n_pairs] = static_cast<int>(arow);
+    const int workers = c.num_sms / 2;
+    Built probe_f, bf, probe_r, br;
+    SIFT_TRY(build(pairs, n_pairs, b_rows, 2, workers, probe_f));
+    const int shape_f = cached_shape(probe_f);
+    SIFT_TRY(build(pairs, n_pairs, b_rows, kShapes[shape_f].qpt, workers, bf));
+    SIFT_TRY(build(rev.data(), n_pairs, static_cast<uint32_t>(arow), 2, workers, probe_r));
+    const int shape_r = cached_shape(probe_r);
+    SIFT_TRY(build(rev.data(), n_pairs, static_cast<uint32_t>(arow), kShapes[shape_r].qpt, workers, br));
+    SIFT_TRY(check_io(a, b, b_rows, bf.total_q, matches, nn_idx, nn_dist));
+    if (bf.total_q == 0) return SIFT_OK;
+    const int total_a = bf.total_q, total_b = static_cast<int>(brow);
+
+    std::lock_guard<std::mutex> lk(c.mu);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const BatchLayout lf = layout_for(&bf, 1), lr = layout_for(&br, 1);
+    detail::Layout L;
+    const size_t o_f = L.take(lf.bytes), o_r = L.take(lr.bytes);
+    const size_t o_nnf = L.take(static_cast<size_t>(total_a) * 8);
+    const size_t o_mf = L.take(static_cast<size_t>(total_a) * 4);
+    const size_t o_nnr = L.take(static_cast<size_t>(total_b) * 8 + 16);
+    const size_t o_rows = L.take(contiguous ? 0 : static_cast<size_t>(total_b) * kDim + 16);
+    const size_t o_off = L.take(sizeof(int) * (3 * static_cast<size_t>(n_pairs) + 1));
+    SIFT_TRY(detail::ensure_arena(c, L.off));
+    char* A = c.arena;
+    const Buffers mf = buffers_at(A + o_f, lf), mr = buffers_at(A + o_r, lr);
+    int32_t* nn_f = nn_idx ? nn_idx : reinterpret_cast<int32_t*>(A + o_nnf);
+    uint32_t* m_f = reinterpret_cast<uint32_t*>(A + o_mf);
+    int32_t* nn_r = reinterpret_cast<int32_t*>(A + o_nnr);
+    int* d_aoff = reinterpret_cast<int*>(A + o_off);
+    int* d_brow = d_aoff + n_pairs + 1;
+    int* d_roff = d_brow + n_pairs;
+    std::vector<int> offs(a_off);
+    offs.insert(offs.end(), b_row.begin(), b_row.end());
+    offs.insert(offs.end(), r_off.begin(), r_off.end());
+    SIFT_CUDA(cudaMemcpyAsync(d_aoff, offs.data(), sizeof(int) * offs.size(), cudaMemcpyHostToDevice, st));
+    if (!bf.items.empty())
+        SIFT_CUDA(cudaMemcpyAsync(mf.items, bf.items.data(), sizeof(WorkItem) * bf.items.size(),
+                                  cudaMemcpyHostToDevice, st));
+    if (!br.items.empty())
+        SIFT_CUDA(cudaMemcpyAsync(mr.items, br.items.data(), sizeof(WorkItem) * br.items.size(),
+                                  cudaMemcpyHostToDevice, st));
+    const uint8_t* qrev = b;
+    if (!contiguous && total_b > 0) {
+        uint8_t* rows = reinterpret_cast<uint8_t*>(A + o_rows);
+        gather_sets_kernel<<<static_cast<unsigned>((static_cast<long long>(total_b) * 8 + 255) / 256), 256, 0, st>>>(
+            b, d_brow, d_roff, n_pairs, total_b, rows);
+        SIFT_CUDA(cudaGetLastError());
+        ++detail::g_launches;
+        qrev = rows;
+    }
+    SIFT_TRY(enqueue(c, a, b, b_rows, bf, mf, kShapes[shape_f], threshold, m_f, nn_f, nn_dist, st));
+    SIFT_TRY(enqueue(c, qrev, a, static_cast<uint32_t>(total_a), br, mr, kShapes[shape_r], 0.0f, nullptr, nn_r,
+                     nullptr, st));
+    cross_check_kernel<<<(total_a + 255) / 256, 256, 0, st>>>(nn_f, m_f, nn_r, d_aoff, d_brow, n_pairs, total_a,
+                                                               threshold > 0.0f ? 1 : 0, matches);
+    SIFT_CUDA(cudaGetLastError());
+    ++detail::g_launches;
+    return SIFT_OK;
+}
+
 int batch_plan_create(const uint8_t* q, const uint8_t* r, uint32_t r_rows, const sift_pair* pairs, int n_pairs,
                       float threshold, uint32_t* matches, int32_t* nn_idx, float* nn_dist, int flags,
                       sift_batch_plan** out) {
@@ -339,6 +465,12 @@ int batch_describe(const sift_pair* pairs, int n_pairs, uint32_t r_rows, int qpt
 }  // namespace sift
 
 extern "C" {
+
+int sift2nn_match_mutual_batch(const uint8_t* a, const uint8_t* b, uint32_t b_rows, const sift_pair* pairs,
+                               int n_pairs, float threshold, uint32_t* matches, int32_t* nn_idx, float* nn_dist,
+                               void* stream) {
+    return sift::match_mutual_batch(a, b, b_rows, pairs, n_pairs, threshold, matches, nn_idx, nn_dist, stream);
+}
 
 int sift2nn_match_batch(const uint8_t* q, const uint8_t* r, uint32_t r_rows, const sift_pair* pairs, int n_pairs,
                         float threshold, uint32_t* matches, int32_t* nn_idx, float* nn_dist, void* stream) {

@@ -57,7 +57,8 @@ __host__ __device__ constexpr size_t hash_smem_bytes(int P) {
 // two accumulator buffers of P columns (rounded up to a power of two >= 32).
 __global__ void __launch_bounds__(kHThreads, 1)
     lsh_hash_kernel(const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap pmap, int n, int P,
-                    int L, int k, uint32_t tmem_cols, uint32_t* __restrict__ codes, int* __restrict__ err) {
+                    int L, int k, uint32_t tmem_cols, uint32_t* __restrict__ codes, float* __restrict__ z,
+                    int* __restrict__ err) {
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = ptx::smem_u32(smem_raw);
     uint8_t* smem = smem_raw + ((1024u - (raw & 1023u)) & 1023u);
@@ -155,6 +156,7 @@ __global__ void __launch_bounds__(kHThreads, 1)
             if (!__all_sync(0xffffffffu, waited)) break;
             ptx::tc_fence_after();
             const uint32_t taddr = tmem + (static_cast<uint32_t>(quarter * 32) << 16) + b * (tmem_cols / 2);
+            const int point = (blockIdx.x + i * gridDim.x) * 128 + quarter * 32 + lane;
             uint32_t mask[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             #pragma unroll
             for (int w = 0; w < 8; ++w) {
@@ -166,12 +168,21 @@ __global__ void __launch_bounds__(kHThreads, 1)
                     #pragma unroll
                     for (int c = 0; c < 32; ++c) m |= (v[c] >> 31) << c;
                     mask[w] = m;
+                    if (z && point < n) {
+                        // Dot products of the point with each hyperplane (multi-probe margins).
+                        #pragma unroll
+                        for (int c = 0; c < 32; ++c) {
+                            const int col = w * 32 + c;
+                            if (col < L * k)
+                                z[(static_cast<size_t>(col / k) * n + point) * k + col % k] =
+                                    static_cast<float>(static_cast<int>(v[c]));
+                        }
+                    }
                 }
             }
             ptx::tc_fence_before();
             __syncwarp();
             if (lane == 0) ptx::mbar_arrive(bar_tempty + 8 * b);
-            const int point = (blockIdx.x + i * gridDim.x) * 128 + quarter * 32 + lane;
             if (point < n) {
                 for (int t = 0; t < L; ++t) {
                     const int bit0 = t * k;
@@ -373,7 +384,7 @@ int lsh_planes_padded(int L, int k) { return ((L * k + 31) / 32) * 32; }
 size_t lsh_hash_smem(int P) { return hash_smem_bytes(P); }
 
 cudaError_t launch_lsh_hash(const CUtensorMap& xmap, const CUtensorMap& pmap, int n, int P, int L, int k,
-                            uint32_t* codes, int* err, int num_sms, cudaStream_t stream) {
+                            uint32_t* codes, float* z, int* err, int num_sms, cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
     const size_t smem = hash_smem_bytes(P);
     cudaError_t e = cudaFuncSetAttribute(lsh_hash_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -383,7 +394,7 @@ cudaError_t launch_lsh_hash(const CUtensorMap& xmap, const CUtensorMap& pmap, in
     while (cols < static_cast<uint32_t>(2 * P)) cols <<= 1;
     const int tiles = (n + 127) / 128;
     const int grid = tiles < num_sms ? tiles : num_sms;
-    lsh_hash_kernel<<<grid, kHThreads, smem, stream>>>(xmap, pmap, n, P, L, k, cols, codes, err);
+    lsh_hash_kernel<<<grid, kHThreads, smem, stream>>>(xmap, pmap, n, P, L, k, cols, codes, z, err);
     return cudaGetLastError();
 }
 

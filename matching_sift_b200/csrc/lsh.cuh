@@ -17,8 +17,10 @@ size_t lsh_hash_smem(int P);
 
 // codes[t][i] (t < L, i < n): bit j set when x_i . planes[t * k + j] < 0.
 // xmap: u8 rows [n][128], box 128 rows; pmap: s8 rows [L * k][128], box P rows.
+// z (optional): the dot products themselves, z[t][i][j] as floats (exact), the
+// margins that multi-probe ranks bits by.
 cudaError_t launch_lsh_hash(const CUtensorMap& xmap, const CUtensorMap& pmap, int n, int P, int L, int k,
-                            uint32_t* codes, int* err, int num_sms, cudaStream_t stream);
+                            uint32_t* codes, float* z, int* err, int num_sms, cudaStream_t stream);
 
 // Groups the n base points of every table by the top code bits
 // (bin = code >> shift, nbins = 2^(k - shift)): start[t][0..nbins] offsets,

@@ -147,6 +147,27 @@ def ratio_match(dist: np.ndarray, idx: np.ndarray, threshold: float) -> np.ndarr
     return out
 
 
+def mutual_match(a: np.ndarray, b: np.ndarray, threshold: float) -> np.ndarray:
+    """Mutual nearest neighbours of two descriptor sets (cross-check; no
+    counterpart in the reference, composed from brute_2nn_u8 in both
+    directions): out[i] = j when j is the nearest row of b for row i of a,
+    row i is the nearest row of a for row j of b and, when threshold > 0, the
+    ratio test of row i passes; else UINT32_MAX."""
+    d, i = brute_2nn_u8(a, b)
+    out = np.full(a.shape[0], 0xFFFFFFFF, np.uint32)
+    if a.shape[0] == 0 or b.shape[0] == 0:
+        return out
+    _, ir = brute_2nn_u8(b, a)
+    j = i[:, 0]
+    ok = j >= 0
+    if threshold > 0:
+        ok &= ratio_match(d, i, threshold) != 0xFFFFFFFF
+    back = np.where(ok, ir[np.where(ok, j, 0), 0], -1)
+    keep = ok & (back == np.arange(a.shape[0]))
+    out[keep] = j[keep].astype(np.uint32)
+    return out
+
+
 # ------------------------------------------------------------------- LSH ---
 
 def lsh_codes(x: np.ndarray, planes: np.ndarray):

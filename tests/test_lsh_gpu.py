@@ -117,3 +117,71 @@ def test_lsh_recall_against_exact(cuda_device):
     lsh = ms.lsh_match(qt, rt, torch.from_numpy(_planes(8, 12)).to(cuda_device))["nn_idx"].cpu().numpy()[:, 0]
     recall = (lsh == exact).mean()
     assert recall > 0.5, recall
+
+
+def _probe_codes(codes, dots, k, probes):
+    """Query-directed probes of one table: the min(6, k) lowest-margin bits
+    (|q . plane|, ties by bit index), their subsets by summed margin (ties by
+    subset id), the first `probes` applied to the code."""
+    flip = min(6, k)
+    out = np.empty((probes, len(codes)), np.uint32)
+    for i in range(len(codes)):
+        mag = np.abs(dots[i, :k])
+        kept = sorted(range(k), key=lambda j: (mag[j], j))[:flip]
+        subsets = sorted(range(1 << flip), key=lambda s: (sum(mag[kept[b]] for b in range(flip) if s >> b & 1), s))
+        for p in range(probes):
+            c = int(codes[i])
+            for b in range(flip):
+                if subsets[p] >> b & 1:
+                    c ^= 1 << kept[b]
+            out[p, i] = c
+    return out
+
+
+@pytest.mark.parametrize("L,k,probes", [(2, 16, 1), (2, 16, 4), (1, 12, 16), (3, 10, 8)])
+def test_multiprobe_vs_oracle(cuda_device, L, k, probes):
+    import torch
+
+    q, r = datagen.make_workload(1200, 30000, seed=probes + k)
+    planes = _planes(L, k, seed=L + probes)
+    out = ms.lsh_match(torch.from_numpy(q).to(cuda_device), torch.from_numpy(r).to(cuda_device),
+                       torch.from_numpy(planes).to(cuda_device), threshold=0.8, probes=probes, candidates=True)
+    assert ms.stream_status() == ms.SIFT_OK
+    qcodes, rcodes, cand = [], [], np.zeros(q.shape[0], np.int64)
+    for t in range(L):
+        qc, qdots = oracle.lsh_codes(q, planes[t].astype(np.float32))
+        rc, _ = oracle.lsh_codes(r, planes[t].astype(np.float32))
+        pc = _probe_codes(qc, qdots, k, probes)
+        sizes = dict(zip(*np.unique(rc, return_counts=True)))
+        for i in range(q.shape[0]):
+            cand[i] += sum(int(sizes.get(c, 0)) for c in set(pc[:, i].tolist()))
+        qcodes.append(pc)
+        rcodes.extend([rc] * probes)
+    d, i = oracle.lsh_scan(q, r, np.concatenate(qcodes), np.stack(rcodes))
+    np.testing.assert_array_equal(out["nn_idx"].cpu().numpy().astype(np.int64), i)
+    present = i >= 0
+    np.testing.assert_array_equal(out["nn_dist"].cpu().numpy()[present].astype(np.int64), d[present])
+    want = oracle.ratio_match(np.where(present, d, np.iinfo(np.int64).max), i, 0.8)
+    np.testing.assert_array_equal(out["matches"].cpu().numpy().view(np.uint32), want)
+    np.testing.assert_array_equal(out["candidates"].cpu().numpy().astype(np.int64), cand)
+
+
+def test_more_probes_never_lose_the_nearest(cuda_device):
+    import torch
+
+    q, r = datagen.make_workload(2000, 100000, seed=3)
+    planes = torch.from_numpy(_planes(4, 16, seed=9)).to(cuda_device)
+    qd, rd = torch.from_numpy(q).to(cuda_device), torch.from_numpy(r).to(cuda_device)
+    exact = ms.match(qd, rd, outputs=("nn_idx",))["nn_idx"][:, 0].cpu().numpy()
+    prev_d, prev_hits = None, -1
+    for probes in (1, 2, 8, 32):
+        o = ms.lsh_match(qd, rd, planes, probes=probes, candidates=True)
+        d1 = o["nn_dist"][:, 0].cpu().numpy()
+        hits = int((o["nn_idx"][:, 0].cpu().numpy() == exact).sum())
+        if prev_d is not None:
+            assert (d1 <= prev_d).all()
+            assert hits >= prev_hits
+        prev_d, prev_hits = d1, hits
+    assert prev_hits > 0
+    with pytest.raises(ms.SiftError):
+        ms.lsh_match(qd, rd, planes, probes=65)

@@ -125,3 +125,17 @@ def test_lsh_scan_is_exact_on_candidates():
         assert i[k, 0] == cand[o[0]] and d[k, 0] == dd[o[0]]
         if cand.size > 1:
             assert i[k, 1] == cand[o[1]] and d[k, 1] == dd[o[1]]
+
+
+def test_mutual_oracle_small_example():
+    """Mutual nearest neighbours on hand-made sets: rows 0 and 1 of a pick
+    each other's partners in b; row 2 of a prefers b[0], which prefers a[0]."""
+    a = np.zeros((3, 128), np.uint8)
+    b = np.zeros((2, 128), np.uint8)
+    a[0, 0], a[1, 1], a[2, 0], a[2, 2] = 100, 100, 90, 30
+    b[0, 0], b[1, 1] = 101, 99
+    m = oracle.mutual_match(a, b, 0.0)
+    assert list(m) == [0, 1, 0xFFFFFFFF]
+    assert list(oracle.mutual_match(b, a, 0.0)) == [0, 1]
+    assert list(oracle.mutual_match(a[:0], b, 0.8)) == []
+    assert list(oracle.mutual_match(a, b[:0], 0.8)) == [0xFFFFFFFF] * 3
