@@ -574,19 +574,23 @@ def learned_leg(args, ms, torch, dev, stream, qd, rd, base, truth):
 
 
 def lsh_leg(args, ms, torch, dev, stream, qd, rd, truth):
-    """Random-hyperplane LSH (int8 N(0,1)*32 planes, seed 1) at two (k, L)
-    settings: recall@1 against the exact results and queries/s per call."""
+    """Random-hyperplane LSH (int8 N(0,1)*32 planes, seed 1) at several (k, L,
+    probes) settings: recall@1 against the exact results, queries/s per call
+    and mean candidates compared per query."""
     from matching_sift_b200 import datagen
 
     q_n = qd.shape[0]
     points = []
-    for k, L in ((16, 8), (8, 16)):
+    for k, L, probes in ((16, 8, 1), (16, 8, 8), (16, 8, 32), (8, 16, 1)):
         planes = torch.from_numpy(datagen.quantize_planes(datagen.make_hyperplanes(k, L, seed=1))).to(dev)
-        ms_call, out = _time_calls(torch, stream, lambda: ms.lsh_match(qd, rd, planes, stream=stream), 2)
+        ms_call, out = _time_calls(
+            torch, stream, lambda: ms.lsh_match(qd, rd, planes, stream=stream, probes=probes, candidates=True), 2)
         got = out["nn_idx"][:, 0].cpu().numpy()
-        points.append({"k": k, "L": L, "ms_per_call": round(ms_call, 3), "value": round(q_n / (ms_call * 1e-3), 1),
-                       "recall1": round(float((got == truth).mean()), 4)})
-    return {"unit": "queries/s", "call": "sift_lsh_match (hash base + buckets + scan per call)", "points": points}
+        points.append({"k": k, "L": L, "probes": probes, "ms_per_call": round(ms_call, 3),
+                       "value": round(q_n / (ms_call * 1e-3), 1), "recall1": round(float((got == truth).mean()), 4),
+                       "candidates_mean": round(float(out["candidates"].double().mean().item()), 1)})
+    return {"unit": "queries/s", "call": "sift_lsh_match_probes (hash base + buckets + probe codes + scan per call)",
+            "points": points}
 
 
 def reference_arm(args, world, rank):
