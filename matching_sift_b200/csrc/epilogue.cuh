@@ -15,11 +15,10 @@ __device__ __forceinline__ int max8(const uint32_t* v) {
     return max(m, static_cast<int>(v[7]));
 }
 
-// f32 accumulators holding integer multiples of 1/dscale (dscale a power of
-// two; exact, see the FP16 kernel) -> the integer dot products, in place.
-__device__ __forceinline__ void f32_to_dot(uint32_t (&v)[32], float dscale) {
-    #pragma unroll
-    for (int c = 0; c < 32; ++c) v[c] = static_cast<uint32_t>(__float2int_rn(__uint_as_float(v[c]) * dscale));
+// An f32 accumulator holding an integer multiple of 1/dscale (dscale a power
+// of two; exact, see the FP16 kernel) -> the integer dot product.
+__device__ __forceinline__ int f32_dot(uint32_t bits, float dscale) {
+    return __float2int_rn(__uint_as_float(bits) * dscale);
 }
 
 // Per-thread running top-2 of one query row over base rows visited in
@@ -42,7 +41,12 @@ __device__ __forceinline__ void top2_update(Top2& s, int key, int idx) {
 }
 
 // One group of 32 consecutive base rows [row0, row0 + 32) for this thread's
-// query row; v[c] = q.b(row0 + c); nrm points at the group's 32 norms in the
+// query row; v[c] = q.b(row0 + c) as s32, or (F32) as the f32 accumulator of
+// the FP16 kernel, q.b / dscale. Those are never negative (inputs are
+// integers in [0, 255] times 2^-s), so their bit patterns, compared as int32,
+// order like the values (-0.0 only below +0.0, and both convert to 0): the
+// max trees run on the raw bits, and only the four subgroup maxima and the
+// values of passing subgroups are converted. nrm points at the group's 32 norms in the
 // shared-memory record, gm8 at its four 8-row minima. Each 8-row subgroup is
 // bounded from below by gm8[k] - 2 max(v[8k..8k+8)) (no key of its rows is
 // smaller), so a subgroup whose bound exceeds the thread's threshold holds no
@@ -50,11 +54,15 @@ __device__ __forceinline__ void top2_update(Top2& s, int key, int idx) {
 // forms its 8 exact keys and updates the top-2 only when their minimum is
 // within the threshold (a key above it cannot reach the final top-2: the
 // threshold never exceeds the final second-best key).
+template <bool F32 = false>
 __device__ __forceinline__ void scan_group(const uint32_t (&v)[32], int row0, const int32_t* nrm, const int32_t* gm8,
-                                           Top2& s) {
+                                           Top2& s, float dscale = 1.0f) {
     int mx[4];
     #pragma unroll
-    for (int k = 0; k < 4; ++k) mx[k] = max8(v + 8 * k);
+    for (int k = 0; k < 4; ++k) {
+        mx[k] = max8(v + 8 * k);
+        if constexpr (F32) mx[k] = f32_dot(static_cast<uint32_t>(mx[k]), dscale);
+    }
     const int4 g8 = *reinterpret_cast<const int4*>(gm8);
     const int bnd[4] = {g8.x - 2 * mx[0], g8.y - 2 * mx[1], g8.z - 2 * mx[2], g8.w - 2 * mx[3]};
     const int bmin = min(__vimin3_s32(bnd[0], bnd[1], bnd[2]), bnd[3]);
@@ -69,7 +77,8 @@ __device__ __forceinline__ void scan_group(const uint32_t (&v)[32], int row0, co
                     const int nr[8] = {na.x, na.y, na.z, na.w, nb.x, nb.y, nb.z, nb.w};
                     int key[8];
                     #pragma unroll
-                    for (int e = 0; e < 8; ++e) key[e] = nr[e] - 2 * static_cast<int>(v[8 * k + e]);
+                    for (int e = 0; e < 8; ++e)
+                        key[e] = nr[e] - 2 * (F32 ? f32_dot(v[8 * k + e], dscale) : static_cast<int>(v[8 * k + e]));
                     // Exact keys first; the (rare) updates only when one can enter.
                     int mk = __vimin3_s32(key[0], key[1], key[2]);
                     mk = __vimin3_s32(mk, key[3], key[4]);

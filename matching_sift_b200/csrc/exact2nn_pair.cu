@@ -65,10 +65,12 @@
 //                             are integers times 2^-s (|integer| <= 255), so
 //                             every product and partial sum is an integer
 //                             multiple of 2^-2s below 2^24 * 2^-2s and the f32
-//                             accumulators are exact; the epilogue turns them
-//                             into the same integer dot products as the u8
-//                             kernel (times dscale = 2^2s, rounded) and the
-//                             rest is shared.
+//                             accumulators are exact. The epilogue prunes on
+//                             the raw f32 bits (non-negative values order like
+//                             int32) and converts to the u8 kernel's integer
+//                             dot products (times dscale = 2^2s, rounded) only
+//                             the subgroup maxima and the values of passing
+//                             subgroups; the rest is shared.
 //   exact2nn_u8_pair_batch_kernel<QPT, QB>  u8 batches with the shapes the
 //                             batch autotuner chooses from.
 #include <climits>
@@ -420,23 +422,19 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                     uint32_t va[32];
                     ptx::tmem_ld32(taddr, va);
                     ptx::tmem_ld_wait(va);
-                    if constexpr (F16) f32_to_dot(va, dscale);
-                    scan_group(va, row0, rec, rec + 128, st);
+                    scan_group<F16>(va, row0, rec, rec + 128, st, dscale);
                     ptx::tmem_ld32(taddr + 32, va);
                     ptx::tmem_ld_wait(va);
-                    if constexpr (F16) f32_to_dot(va, dscale);
-                    scan_group(va, row0 + 32, rec + 32, rec + 132, st);
+                    scan_group<F16>(va, row0 + 32, rec + 32, rec + 132, st, dscale);
                     ptx::tmem_ld32(taddr + 64, va);
                     ptx::tmem_ld_wait(va);
-                    if constexpr (F16) f32_to_dot(va, dscale);
-                    scan_group(va, row0 + 64, rec + 64, rec + 136, st);
+                    scan_group<F16>(va, row0 + 64, rec + 64, rec + 136, st, dscale);
                     ptx::tmem_ld32(taddr + 96, va);
                     ptx::tmem_ld_wait(va);
-                    if constexpr (F16) f32_to_dot(va, dscale);
                     ptx::tc_fence_before();
                     __syncwarp();
                     if (lane == 0) ptx::mbar_arrive_cluster_relaxed(lead_tempty);
-                    scan_group(va, row0 + 96, rec + 96, rec + 140, st);
+                    scan_group<F16>(va, row0 + 96, rec + 96, rec + 140, st, dscale);
                     if (valid && st.k2 < published) {
                         atomicMin(thresh + q, st.k2);
                         published = st.k2;
