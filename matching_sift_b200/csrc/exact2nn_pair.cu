@@ -49,8 +49,12 @@
 //              record is no longer read (per CTA)                  arrive
 //   qfull[b]   (L) query tiles of both CTAs landed in buffer b      TMA tx
 //   qempty[b]  MMAs of the group in query buffer b done (both CTAs) commit x 2 (one per issuer), multicast
-//   tfull[b]   both query tiles' accumulators of buffer b done      commit, multicast
-//   tempty[b]  (L) the 8 warps of buffer b in each CTA read it      remote arrive
+//   tfull[sl]  accumulators of TMEM slot sl = (query tile t, buffer b) done
+//              (one commit per tile, so a tile's epilogue starts
+//              before the next tile's MMAs finish)                commit, multicast
+//   tempty[sl] (L) the 4 warps of slot sl in each CTA read it: the
+//              issuer's next MMAs into that tile start without
+//              waiting for the other tile's epilogue              remote arrive
 // Every wait is bounded (2 s); an expired wait raises the CTA's abort flag
 // and records an error code, and every role still reaches the teardown.
 //
@@ -115,7 +119,7 @@ struct PairCfg {
         uint64_t rfull[kStages];
         uint64_t sfree[kStages];
         uint64_t qfull[QB], qempty[QB];
-        uint64_t tfull[2], tempty[2];
+        uint64_t tfull[2 * QPT], tempty[2 * QPT];  // per TMEM slot (tile t, buffer b) = 2 t + b
         uint64_t drain;
         uint32_t tmem_base;
         int abort_flag;
@@ -230,9 +234,9 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
             ptx::mbar_init(bar_qfull + 8 * b, 1);
             ptx::mbar_init(bar_qempty + 8 * b, 2);  // one commit per MMA issuer
         }
-        for (int b = 0; b < 2; ++b) {
-            ptx::mbar_init(bar_tfull + 8 * b, 1);
-            ptx::mbar_init(bar_tempty + 8 * b, 2 * kPEpiWarps / 2);  // the warps of buffer b in each CTA
+        for (int sl = 0; sl < 2 * QPT; ++sl) {
+            ptx::mbar_init(bar_tfull + 8 * sl, 1);
+            ptx::mbar_init(bar_tempty + 8 * sl, 2 * 4);  // the 4 warps of the slot in each CTA
         }
         ptx::mbar_init(bar_drain, 2);
         ctl->abort_flag = 0;
@@ -333,13 +337,20 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                     if (!pre_full &&
                         !ptx::mbar_wait_cluster(bar_full + 8 * s, (n / kPStages) & 1, abort_flag, err, kErrWaitMmaFull))
                         break;
-                    if (!pre_tempty && !ptx::mbar_wait_cluster(bar_tempty + 8 * mt, ((n >> 1) & 1) ^ 1, abort_flag,
-                                                               err, kErrWaitMmaTmem))
-                        break;
-                    ptx::tc_fence_after();
+                    const uint32_t tpar_free = ((n >> 1) & 1) ^ 1;
                     const uint64_t b_desc = b_desc0 + static_cast<uint64_t>((s * kPBHalfBytes) >> 4);
+                    bool ok = true;
                     #pragma unroll
                     for (int t = 0; t < QPT; ++t) {
+                        // Each tile's slot is handed back on its own: the tile's MMAs
+                        // start as soon as its epilogue warps release it.
+                        if (!(t == 0 && pre_tempty) &&
+                            !ptx::mbar_wait_cluster(bar_tempty + 8 * (t * 2 + mt), tpar_free, abort_flag, err,
+                                                    kErrWaitMmaTmem)) {
+                            ok = false;
+                            break;
+                        }
+                        ptx::tc_fence_after();
                         const uint32_t d = tmem + (t * 2 + mt) * kBN;
                         #pragma unroll
                         for (int kb = 0; kb < Cfg::kKBlocks; ++kb) {
@@ -355,12 +366,13 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                                     ptx::mma_i8_pair(d, a_desc + 2 * kk, b_kb + 2 * kk, idesc, acc);
                             }
                         }
+                        ptx::tc_commit_pair_mc(bar_tfull + 8 * (t * 2 + mt), kPairMask);
                     }
-                    ptx::tc_commit_pair_mc(bar_tfull + 8 * mt, kPairMask);
+                    if (!ok) break;
                     // Test the barriers of this issuer's next unit (n + 2) behind its queued MMAs.
                     if (n + 2 < n_units) {
                         pre_full = ptx::mbar_test_wait(bar_full + 8 * ((n + 2) % kPStages), ((n + 2) / kPStages) & 1);
-                        pre_tempty = ptx::mbar_test_wait(bar_tempty + 8 * mt, (((n + 2) >> 1) & 1) ^ 1);
+                        pre_tempty = ptx::mbar_test_wait(bar_tempty + 8 * mt, (((n + 2) >> 1) & 1) ^ 1);  // tile 0
                     }
                 }
                 // Both issuers release the query buffer at the end of a group
@@ -380,7 +392,8 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
         const int buf = (e >> 2) & 1;     // accumulator buffer = parity of the units this warp scans
         const int quarter = warp & 3;     // TMEM lane quarter this warp may access
         const uint32_t taddr = tmem + (static_cast<uint32_t>(quarter * 32) << 16) + (t * 2 + buf) * kBN;
-        const uint32_t lead_tempty = ptx::mapa(bar_tempty + 8 * buf, 0);
+        const int slot = t * 2 + buf;     // TMEM slot and its barriers
+        const uint32_t lead_tempty = ptx::mapa(bar_tempty + 8 * slot, 0);
         Top2 st{INT_MAX, -1, INT_MAX, -1, INT_MAX};
         int published = INT_MAX;
         int split = 0, q = 0;
@@ -408,11 +421,11 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                 const uint32_t rpar = (n / kPStages) & 1, tpar = (static_cast<uint32_t>(n) >> 1) & 1;
                 // Both tests are issued back to back so their latencies overlap.
                 const bool r_ok = ptx::mbar_try_wait(bar_rfull + 8 * s, rpar);
-                const bool t_ok = ptx::mbar_try_wait_cluster(bar_tfull + 8 * buf, tpar, 0u);
+                const bool t_ok = ptx::mbar_try_wait_cluster(bar_tfull + 8 * slot, tpar, 0u);
                 bool waited = true;
                 if (!r_ok) waited = ptx::mbar_wait(bar_rfull + 8 * s, rpar, abort_flag, err, kErrWaitEpilogue);
                 if (waited && !t_ok)
-                    waited = ptx::mbar_wait_cluster(bar_tfull + 8 * buf, tpar, abort_flag, err, kErrWaitEpilogue);
+                    waited = ptx::mbar_wait_cluster(bar_tfull + 8 * slot, tpar, abort_flag, err, kErrWaitEpilogue);
                 if (!__all_sync(0xffffffffu, waited)) break;
                 ptx::tc_fence_after();
                 if (active) {
