@@ -306,6 +306,7 @@ def main():
         if not torch.equal(variants["fp16"].pop("nn_idx"), nn_idx):
             raise RuntimeError("FP16 and u8 kernels disagree")
         variants["pairs"] = pairs_leg(args, ms, torch, dev, stream)
+        variants["mutual"] = mutual_leg(args, ms, torch, dev, stream)
         truth = nn_idx[:, 0].cpu().numpy()
         variants["learned"] = learned_leg(args, ms, torch, dev, stream, qd, rd, base, truth)
         variants["lsh"] = lsh_leg(args, ms, torch, dev, stream, qd, rd, truth)
@@ -415,6 +416,17 @@ def main():
                              "unit": "TFLOP/s", "frac": round(ach / peak_int8, 4), "ops_per_step": v["ops"],
                              "note": "whole graph time (4 launches), 2 ops per MAC"},
                 "gpu_launches": v["launches"]}
+        if "mutual" in variants:
+            v = variants["mutual"]
+            mu_ms = v["step_ms"] / v["steps"]
+            line.setdefault("variants", {})["mutual512"] = {
+                "value": round(world * v["rows"] / (mu_ms * 1e-3), 1), "unit": "queries/s",
+                "ms_per_step": round(mu_ms, 4), "steps": v["steps"], "dtype": "u8",
+                "workload": f"the {v['pairs']} image pairs of pairs512 matched both ways, {v['rows']:,} rows of the "
+                            "first sets",
+                "call": "sift2nn_match_mutual_batch + sift_compact_matches (two batched searches, cross-check, "
+                        "per-pair match lists), preallocated outputs",
+                "mutual_matches": v["mutual_matches"]}
         for key in ("learned", "lsh"):
             if key in variants:
                 v = dict(variants[key])
@@ -522,6 +534,50 @@ def pairs_leg(args, ms, torch, dev, stream):
             "tuned_ms": [round(x, 4) for x in info["tuned_ms"]],
             # graph replays are not counted by the library's launch counter; 4 kernels per replay
             "launches": int(ms.lib().sift_launch_count() - launches0) + 4 * steps}
+
+
+def mutual_leg(args, ms, torch, dev, stream):
+    """The 512 uneven image pairs matched both ways: sift2nn_match_mutual_batch
+    (forward search with the ratio test, reverse search, cross-check) and
+    sift_compact_matches (per-pair match lists for geometric verification),
+    preallocated outputs, no host synchronisation inside the timed calls."""
+    import ctypes
+
+    from matching_sift_b200 import datagen
+
+    data = datagen.make_pairs(512, seed=0)
+    a = np.concatenate([x for x, _ in data])
+    b = np.concatenate([y for _, y in data])
+    pairs, off = [], 0
+    for x, y in data:
+        pairs.append([x.shape[0], y.shape[0], off])
+        off += y.shape[0]
+    pa = np.ascontiguousarray(np.asarray(pairs, dtype=np.uint32))
+    ad, bd = torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)
+    rows = a.shape[0]
+    m = torch.empty(rows, dtype=torch.int32, device=dev)
+    nn_idx = torch.empty((rows, 2), dtype=torch.int32, device=dev)
+    nn_dist = torch.empty((rows, 2), dtype=torch.float32, device=dev)
+    recs = torch.empty((rows, 5), dtype=torch.int32, device=dev)
+    offs = torch.empty(len(pairs) + 1, dtype=torch.int32, device=dev)
+    lib = ms.lib()
+    pp = pa.ctypes.data_as(ctypes.c_void_p)
+
+    def step():
+        ms.check(lib.sift2nn_match_mutual_batch(ad.data_ptr(), bd.data_ptr(), b.shape[0], pp, len(pairs), THRESHOLD,
+                                                m.data_ptr(), nn_idx.data_ptr(), nn_dist.data_ptr(),
+                                                stream.cuda_stream), "sift2nn_match_mutual_batch")
+        ms.check(lib.sift_compact_matches(m.data_ptr(), nn_dist.data_ptr(), rows, pp, len(pairs), recs.data_ptr(),
+                                          rows, offs.data_ptr(), stream.cuda_stream), "sift_compact_matches")
+
+    for _ in range(args.warmup):
+        step()
+    steps = max(3, args.steps)
+    ms_call, _ = _time_calls(torch, stream, step, steps)
+    if ms.stream_status(stream.cuda_stream) != 0:
+        raise RuntimeError("device status after the mutual steps")
+    return {"step_ms": ms_call * steps, "steps": steps, "rows": rows, "pairs": len(pairs),
+            "mutual_matches": int(offs[-1].item())}
 
 
 def _time_calls(torch, stream, fn, steps):

@@ -228,6 +228,24 @@ SIFT_API int sift2nn_match_mutual_batch(const uint8_t* a, const uint8_t* b, uint
                                         int n_pairs, float threshold, uint32_t* matches, int32_t* nn_idx,
                                         float* nn_dist, void* stream);
 
+/* Match lists for geometric verification (e.g. RANSAC on each image pair):
+   the rows of a batch whose matches[row] is not UINT32_MAX (matches and
+   nn_dist as sift2nn_match_batch / sift2nn_match_mutual_batch write them,
+   device memory, `rows` = sum of pairs[].n_q) as records grouped by problem,
+   rows in order. pair_offsets (device, [n_pairs + 1]) receives the first
+   record of each problem and, last, the number of matches; records past
+   `capacity` are not written (compare the count with it). nn_dist may be
+   NULL (d1 = d2 = 0). Asynchronous on `stream`. */
+typedef struct sift_match {
+    uint32_t pair; /* problem */
+    uint32_t a;    /* row within the problem's first set */
+    uint32_t b;    /* matched row within its second set */
+    float d1, d2;  /* squared distances to the nearest and second nearest */
+} sift_match;
+SIFT_API int sift_compact_matches(const uint32_t* matches, const float* nn_dist, uint32_t rows, const sift_pair* pairs,
+                                  int n_pairs, sift_match* out, uint32_t capacity, uint32_t* pair_offsets,
+                                  void* stream);
+
 /* Merge of 2-NN results searched over `parts` disjoint base shards (e.g. one
    per rank of a base-sharded search, after an all-gather): nn_dist_parts /
    nn_idx_parts are [parts][q_n][2] device arrays as sift2nn_match writes them

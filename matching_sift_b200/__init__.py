@@ -21,7 +21,7 @@ from ._native import (SIFT_BATCH_SHAPE, SIFT_BATCH_TUNE, SIFT_MLP_PARAMS, sift_m
 
 __all__ = [
     "cublas_2nn_sift", "cublas_2nn_f", "device_brute", "host_brute", "lsh_gpu", "match", "lsh_match", "lsh_hash",
-    "stream_status", "version", "match_batch", "match_mutual", "match_mutual_batch", "BatchPlan", "batch_describe",
+    "stream_status", "version", "match_batch", "match_mutual", "match_mutual_batch", "compact_matches", "BatchPlan", "batch_describe",
     "MlpHash", "mlp_loss_grad",
     "SiftError", "FLOAT_HOST", "FLOAT_DEVICE", "HALF_DEVICE", "U8_DEVICE", "U8_HOST", "METRIC_L2", "METRIC_DOT",
 ]
@@ -235,6 +235,29 @@ def match_mutual_batch(a, b, pairs, threshold: float = 0.8, stream=None):
                                            s.cuda_stream),
           "sift2nn_match_mutual_batch")
     return out
+
+
+def compact_matches(out, pairs, capacity=None, stream=None):
+    """Per-problem match lists for geometric verification from the outputs
+    of match_batch / match_mutual_batch (dict with "matches" and optionally
+    "nn_dist"). Returns {"pair", "a", "b" (int64), "d1", "d2" (float32)} over
+    all matches, grouped by problem with rows in order, and "offsets"
+    ([n_pairs + 1], first match of each problem, then the count)."""
+    import torch
+
+    pa = _pairs_array(pairs)
+    m = out["matches"]
+    rows = m.shape[0]
+    cap = rows if capacity is None else int(capacity)
+    rec = torch.empty((max(cap, 1), 5), dtype=torch.int32, device=m.device)  # sift_match = 5 x 4 bytes
+    offs = torch.empty(len(pa) + 1, dtype=torch.int32, device=m.device)
+    s = stream if stream is not None else torch.cuda.current_stream(m.device)
+    check(lib().sift_compact_matches(_ptr(m), _ptr(out.get("nn_dist")), rows, pa.ctypes.data, len(pa), _ptr(rec), cap,
+                                     _ptr(offs), s.cuda_stream), "sift_compact_matches")
+    n = min(int(offs[-1].item()), cap)
+    r = rec[:n]
+    return {"pair": r[:, 0].long(), "a": r[:, 1].long(), "b": r[:, 2].long(),
+            "d1": r[:, 3].view(torch.float32), "d2": r[:, 4].view(torch.float32), "offsets": offs.long()}
 
 
 def match_mutual(a, b, threshold: float = 0.8, stream=None):

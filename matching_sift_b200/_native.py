@@ -54,6 +54,8 @@ _PROTOS = {
                                            _vp, _vp]),
     "sift_merge_top2": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_float, _vp, _vp, _vp,
                                        _vp]),
+    "sift_compact_matches": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_int, _vp, ctypes.c_uint32, _vp,
+                                            _vp]),
     "sift2nn_match_mutual_batch": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_int, ctypes.c_float, _vp,
                                                   _vp, _vp, _vp]),
     "sift_batch_plan_create": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_int, ctypes.c_float, _vp, _vp,

@@ -315,6 +315,163 @@ int match_mutual_batch(const uint8_t* a, const uint8_t* b, uint32_t b_rows, cons
     return SIFT_OK;
 }
 
+// ---- match lists for geometric verification ---------------------------
+// Deterministic stream compaction of the rows with a match, 1024 rows per
+// block: block counts, one scan of them, then each block's rows placed by
+// warp ballots. The lists come out grouped by problem, rows in order.
+constexpr int kCompactRows = 1024;
+
+__global__ void __launch_bounds__(kCompactRows) count_matches_kernel(const uint32_t* __restrict__ matches, int rows,
+                                                                       int* __restrict__ block_counts) {
+    const int i = blockIdx.x * kCompactRows + threadIdx.x;
+    const bool v = i < rows && matches[i] != 0xffffffffu;
+    const int c = __syncthreads_count(v);
+    if (threadIdx.x == 0) block_counts[blockIdx.x] = c;
+}
+
+// Exclusive prefix of the block counts (one block, chunks of 1024 with a
+// running carry); offsets[n_blocks] = total.
+__global__ void __launch_bounds__(1024) scan_counts_kernel(const int* __restrict__ counts, int n_blocks,
+                                                           int* __restrict__ offsets) {
+    __shared__ int warp_sum[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int base = 0; base < n_blocks; base += 1024) {
+        const int i = base + threadIdx.x;
+        const int c = i < n_blocks ? counts[i] : 0;
+        int x = c;  // inclusive warp scan
+        #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_sum[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            int w = warp_sum[lane];
+            #pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += y;
+            }
+            warp_sum[lane] = w;  // inclusive over warps
+        }
+        __syncthreads();
+        const int before = carry + (warp > 0 ? warp_sum[warp - 1] : 0) + x - c;
+        if (i < n_blocks) offsets[i] = before;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += warp_sum[31];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) offsets[n_blocks] = carry;
+}
+
+// Position of row i among the matched rows: its block's offset plus the
+// matched rows before it in the block (ballots).
+__global__ void __launch_bounds__(kCompactRows) scatter_matches_kernel(
+    const uint32_t* __restrict__ matches, const float* __restrict__ nn_dist, int rows, const int* __restrict__ offsets,
+    const int* __restrict__ a_off, int n_pairs, sift_match* __restrict__ out, uint32_t capacity) {
+    __shared__ int warp_count[32];
+    const int i = blockIdx.x * kCompactRows + threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool v = i < rows && matches[i] != 0xffffffffu;
+    const unsigned bal = __ballot_sync(0xffffffffu, v);
+    if (lane == 0) warp_count[warp] = __popc(bal);
+    __syncthreads();
+    if (!v) return;
+    int pos = offsets[blockIdx.x] + __popc(bal & ((1u << lane) - 1u));
+    for (int w = 0; w < warp; ++w) pos += warp_count[w];
+    if (static_cast<uint32_t>(pos) >= capacity) return;
+    const int p = owner_of(a_off, n_pairs, i);
+    sift_match m;
+    m.pair = static_cast<uint32_t>(p);
+    m.a = static_cast<uint32_t>(i - a_off[p]);
+    m.b = matches[i];
+    m.d1 = nn_dist ? nn_dist[2 * static_cast<size_t>(i)] : 0.0f;
+    m.d2 = nn_dist ? nn_dist[2 * static_cast<size_t>(i) + 1] : 0.0f;
+    out[pos] = m;
+}
+
+// pair_offsets[p] = matched rows before problem p's first row (one warp per
+// problem: the block offset plus ballots over the block's earlier rows).
+__global__ void pair_offsets_kernel(const uint32_t* __restrict__ matches, const int* __restrict__ offsets,
+                                    const int* __restrict__ a_off, int n_pairs, int n_blocks,
+                                    uint32_t* __restrict__ pair_offsets) {
+    const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (p > n_pairs) return;
+    if (p == n_pairs) {
+        if (lane == 0) pair_offsets[p] = static_cast<uint32_t>(offsets[n_blocks]);
+        return;
+    }
+    const int row = a_off[p];
+    const int blk = row / kCompactRows;
+    if (blk >= n_blocks) {  // no rows from here on
+        if (lane == 0) pair_offsets[p] = static_cast<uint32_t>(offsets[n_blocks]);
+        return;
+    }
+    int before = 0;
+    for (int r0 = blk * kCompactRows; r0 < row; r0 += 32) {
+        const int r = r0 + lane;
+        before += __popc(__ballot_sync(0xffffffffu, r < row && matches[r] != 0xffffffffu));
+    }
+    if (lane == 0) pair_offsets[p] = static_cast<uint32_t>(offsets[blk] + before);
+}
+
+int compact_matches(const uint32_t* matches, const float* nn_dist, uint32_t rows, const sift_pair* pairs, int n_pairs,
+                    sift_match* out, uint32_t capacity, uint32_t* pair_offsets, void* stream) {
+    DeviceCtx* cp = nullptr;
+    int dev = 0;
+    SIFT_TRY(detail::ensure_ready(cp, dev));
+    DeviceCtx& c = *cp;
+    if (n_pairs < 0 || (n_pairs > 0 && !pairs) || !pair_offsets || rows > 0x7fffffffu - kCompactRows)
+        return SIFT_ERR_INVALID_ARG;
+    std::vector<int> a_off(n_pairs + 1);
+    long long row = 0;
+    for (int p = 0; p < n_pairs; ++p) {
+        a_off[p] = static_cast<int>(row);
+        row += pairs[p].n_q;
+        if (row > static_cast<long long>(rows)) return SIFT_ERR_INVALID_ARG;
+    }
+    if (row != static_cast<long long>(rows)) return SIFT_ERR_INVALID_ARG;
+    a_off[n_pairs] = static_cast<int>(row);
+    if (!detail::is_device_accessible(pair_offsets) || (rows > 0 && (!matches || !detail::is_device_accessible(matches))) ||
+        (nn_dist && !detail::is_device_accessible(nn_dist)) ||
+        (capacity > 0 && (!out || !detail::is_device_accessible(out))))
+        return SIFT_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c.mu);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int n_blocks = static_cast<int>((rows + kCompactRows - 1) / kCompactRows);
+    detail::Layout L;
+    const size_t o_cnt = L.take(sizeof(int) * (static_cast<size_t>(n_blocks) + 1));
+    const size_t o_off = L.take(sizeof(int) * (static_cast<size_t>(n_blocks) + 1));
+    const size_t o_aoff = L.take(sizeof(int) * (static_cast<size_t>(n_pairs) + 1));
+    SIFT_TRY(detail::ensure_arena(c, L.off));
+    int* d_cnt = reinterpret_cast<int*>(c.arena + o_cnt);
+    int* d_off = reinterpret_cast<int*>(c.arena + o_off);
+    int* d_aoff = reinterpret_cast<int*>(c.arena + o_aoff);
+    SIFT_CUDA(cudaMemcpyAsync(d_aoff, a_off.data(), sizeof(int) * a_off.size(), cudaMemcpyHostToDevice, st));
+    if (n_blocks > 0) {
+        count_matches_kernel<<<n_blocks, kCompactRows, 0, st>>>(matches, static_cast<int>(rows), d_cnt);
+        SIFT_CUDA(cudaGetLastError());
+    }
+    scan_counts_kernel<<<1, 1024, 0, st>>>(d_cnt, n_blocks, d_off);
+    SIFT_CUDA(cudaGetLastError());
+    if (n_blocks > 0) {
+        scatter_matches_kernel<<<n_blocks, kCompactRows, 0, st>>>(matches, nn_dist, static_cast<int>(rows), d_off,
+                                                                  d_aoff, n_pairs, out, capacity);
+        SIFT_CUDA(cudaGetLastError());
+    }
+    const long long threads = 32LL * (n_pairs + 1);
+    pair_offsets_kernel<<<static_cast<unsigned>((threads + 255) / 256), 256, 0, st>>>(matches, d_off, d_aoff, n_pairs,
+                                                                                     n_blocks, pair_offsets);
+    SIFT_CUDA(cudaGetLastError());
+    detail::g_launches += 2 + (n_blocks > 0 ? 2 : 0);
+    return SIFT_OK;
+}
+
 int batch_plan_create(const uint8_t* q, const uint8_t* r, uint32_t r_rows, const sift_pair* pairs, int n_pairs,
                       float threshold, uint32_t* matches, int32_t* nn_idx, float* nn_dist, int flags,
                       sift_batch_plan** out) {
@@ -465,6 +622,11 @@ int batch_describe(const sift_pair* pairs, int n_pairs, uint32_t r_rows, int qpt
 }  // namespace sift
 
 extern "C" {
+
+int sift_compact_matches(const uint32_t* matches, const float* nn_dist, uint32_t rows, const sift_pair* pairs,
+                         int n_pairs, sift_match* out, uint32_t capacity, uint32_t* pair_offsets, void* stream) {
+    return sift::compact_matches(matches, nn_dist, rows, pairs, n_pairs, out, capacity, pair_offsets, stream);
+}
 
 int sift2nn_match_mutual_batch(const uint8_t* a, const uint8_t* b, uint32_t b_rows, const sift_pair* pairs,
                                int n_pairs, float threshold, uint32_t* matches, int32_t* nn_idx, float* nn_dist,

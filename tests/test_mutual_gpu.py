@@ -89,3 +89,50 @@ def test_mutual_single_pair_is_symmetric(cuda_device):
     pairs_ab = {(i, int(j)) for i, j in enumerate(ab) if j != 0xFFFFFFFF}
     pairs_ba = {(int(j), i) for i, j in enumerate(ba) if j != 0xFFFFFFFF}
     assert pairs_ab == pairs_ba and len(pairs_ab) > 300
+
+
+def _expected_lists(m, dist, pairs):
+    recs, offs, row = [], [], 0
+    for p, (na, nb, off) in enumerate(pairs):
+        offs.append(len(recs))
+        for a in range(int(na)):
+            j = m[row + a]
+            if j != 0xFFFFFFFF:
+                recs.append((p, a, int(j), dist[row + a, 0], dist[row + a, 1]))
+        row += int(na)
+    offs.append(len(recs))
+    return recs, offs
+
+
+@pytest.mark.parametrize("contiguous", [True, False])
+def test_match_lists_for_verification(cuda_device, contiguous):
+    """Compaction of mutual matches into per-pair lists equals a row-order
+    filter of the same outputs (grouped by pair, offsets, distances)."""
+    a, b, pairs, _ = _pairs(6 if contiguous else 7, 30, contiguous)
+    out = ms.match_mutual_batch(_dev(a, cuda_device), _dev(b, cuda_device), pairs, 0.8)
+    lists = ms.compact_matches(out, pairs)
+    assert ms.stream_status() == ms.SIFT_OK
+    m = out["matches"].cpu().numpy().view(np.uint32)
+    dist = out["nn_dist"].cpu().numpy()
+    recs, offs = _expected_lists(m, dist, pairs)
+    assert len(recs) > 100
+    np.testing.assert_array_equal(lists["offsets"].cpu().numpy(), offs)
+    got = np.stack([lists[k].cpu().numpy().astype(np.float64) for k in ("pair", "a", "b", "d1", "d2")], 1)
+    np.testing.assert_array_equal(got, np.array(recs, np.float64))
+    # a capacity below the count: the first `capacity` records, the full count in the offsets
+    cap = len(recs) // 3
+    part = ms.compact_matches(out, pairs, capacity=cap)
+    assert int(part["offsets"][-1]) == len(recs) and part["a"].shape[0] == cap
+    np.testing.assert_array_equal(part["b"].cpu().numpy(), got[:cap, 2])
+
+
+def test_match_lists_of_a_plain_batch(cuda_device):
+    """Lists from the one-shot batch (ratio-test matches) and without distances."""
+    a, b, pairs, _ = _pairs(8, 12, True)
+    out = ms.match_batch(_dev(a, cuda_device), _dev(b, cuda_device), pairs, 0.8)
+    m = out["matches"].cpu().numpy().view(np.uint32)
+    lists = ms.compact_matches({"matches": out["matches"]}, pairs)
+    recs, offs = _expected_lists(m, np.zeros((m.shape[0], 2), np.float32), pairs)
+    np.testing.assert_array_equal(lists["offsets"].cpu().numpy(), offs)
+    np.testing.assert_array_equal(lists["a"].cpu().numpy(), [r[1] for r in recs])
+    assert (lists["d1"].cpu().numpy() == 0).all()
