@@ -313,6 +313,7 @@ def main():
 
     # ---- end to end through the C ABI with host buffers
     e2e_ms = float("nan")
+    h2d_ms = float("nan")
     if not args.skip_e2e:
         qh = torch.from_numpy(queries).pin_memory()
         rh = torch.from_numpy(base).pin_memory()
@@ -337,6 +338,21 @@ def main():
             b.synchronize()
             e2e_ms += a.elapsed_time(b)
         np.testing.assert_array_equal(mh.numpy(), matches.cpu().numpy())
+        # The PCIe bound of this leg on this box: the same bytes copied from
+        # pinned host memory alone (one copy each of queries and base).
+        qd2, rd2 = torch.empty_like(qd), torch.empty_like(rd)
+        h2d = []
+        for _ in range(3):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record(legacy)
+            qd2.copy_(qh, non_blocking=True)
+            rd2.copy_(rh, non_blocking=True)
+            b.record(legacy)
+            b.synchronize()
+            h2d.append(a.elapsed_time(b))
+        h2d_ms = min(h2d)
+        del qd2, rd2
 
     # ---- max over ranks
     vkeys = sorted(variants)
@@ -380,7 +396,12 @@ def main():
                        "parallelism": f"query-sharded x{world}, base replicated"},
             "e2e": {"value": round(e2e_qps, 1) if e2e_qps else None, "unit": "queries/s",
                     "h2d_bytes_per_step": (q_n + R_N) * DIM, "d2h_bytes_per_step": q_n * 4,
-                    "call": "cublas_2nn_sift(type=SIFT_U8_HOST) with pinned host buffers"},
+                    "call": "cublas_2nn_sift(type=SIFT_U8_HOST) with pinned host buffers",
+                    "h2d_copy_ms": round(h2d_ms, 4) if h2d_ms == h2d_ms else None,
+                    "frac_of_h2d_copy": (round(h2d_ms / (e2e_ms / args.steps), 4)
+                                         if h2d_ms == h2d_ms and e2e_ms == e2e_ms else None),
+                    "h2d_note": "h2d_copy_ms: the step's input bytes copied alone from pinned memory on this box "
+                                "(the PCIe bound of the call); frac = that / the call's time"},
             "gpu_launches": int(launches),
             "roofline": {"bound": "tensor", "kernel": "exact2nn_u8_pair_kernel", "achieved": round(achieved, 1),
                          "peak": round(peak_int8, 1), "unit": "TFLOP/s", "frac": round(achieved / peak_int8, 4),
