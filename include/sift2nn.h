@@ -152,6 +152,18 @@ SIFT_API int sift2nn_match(const void* q, const void* r, int type, uint32_t q_n,
 SIFT_API int sift_lsh_hash(const uint8_t* x, uint32_t n, const int8_t* planes, int L, int k, uint32_t* codes,
                            void* stream);
 
+/* Bucket table of LSH codes (codes[t * n + i], t < L, as sift_lsh_hash writes
+   them; device memory): per table the n points grouped by the top
+   B = min(k, 16) code bits, the grouping the LSH search scans. Replaces the
+   reference's thrust sort by code + host run-length encoding
+   (lsh_thread_sort_reduce, src/lsh_h.cu:565-629). Outputs (device):
+   start[t * (2^B + 1) + b] .. start[t * (2^B + 1) + b + 1] are the positions
+   of group b, order[t * n + pos] the point id at a position and
+   ocode[t * n + pos] its code. Within a group, positions are in no fixed
+   order (the groups themselves are). Asynchronous on `stream`. */
+SIFT_API int sift_lsh_buckets(const uint32_t* codes, uint32_t n, int L, int k, int* start, int* order,
+                              uint32_t* ocode, void* stream);
+
 /* LSH 2-NN with caller-given int8 hyperplanes [L][k][128] (host or device
    memory): each query is compared exactly with the base rows that share its
    code in at least one table. Outputs as sift2nn_match (nn_dist = squared
@@ -188,9 +200,20 @@ SIFT_API int sift_lsh_match_probes(const void* q, const void* r, int type, uint3
    device share that array, so calls that overlap on the GPU race: serialise
    them. The first call on a device looks the array's address up with
    cudaGetSymbolAddress; make it before any stream capture. Asynchronous on
-   `stream` (NULL = legacy default stream). */
+   `stream` (NULL = legacy default stream). q, r and the outputs must be
+   device or managed memory (host pointers return SIFT_ERR_INVALID_ARG). If a
+   bounded wait inside the search expires (no correct run does this), every
+   output row of that call is written as "no result" (UINT32_MAX, -1,
+   FLT_MAX) and sift2nn_noalloc_status reports it. */
 SIFT_API int sift2nn_match_noalloc(const uint8_t* q, const uint8_t* r, uint32_t q_n, uint32_t r_n, float threshold,
                                    uint32_t* matches, int32_t* nn_idx, float* nn_dist, void* stream);
+
+/* Device status of sift2nn_match_noalloc (no counterpart in the reference):
+   synchronises `stream` and returns SIFT_ERR_DEVICE_TIMEOUT if a call on the
+   current device hit an expired bounded wait since the last check (then
+   clears the record), else SIFT_OK. Reads a word of the library's own array;
+   allocates nothing. */
+SIFT_API int sift2nn_noalloc_status(void* stream);
 
 /* Batched exact 2-NN of many independent (query set, base set) problems,
    e.g. the keypoint descriptors of many image pairs of uneven sizes, in one
@@ -344,6 +367,35 @@ SIFT_API int sift_mlp_match(const uint8_t* q, const uint8_t* r, uint32_t q_n, ui
                             int32_t* nn_idx, float* nn_dist, uint32_t* candidates, uint32_t* fallback_count,
                             void* stream);
 
+/* Persistent hash index of a base (no counterpart in the reference, whose
+   lsh_gpu hashes and sorts the base again on every call, src/lsh_h.cu:894-972):
+   the base is hashed and bucketed once at creation and searched any number
+   of times. The index keeps its own bucket table, base-tile records and a
+   copy of the hash (hyperplanes or model); it reads the base rows `r` (uint8
+   [r_n][128], 16-byte aligned device memory) by reference, so they must stay
+   valid and unchanged while the index lives. Creation synchronises.
+     sift_lsh_index_create: random-hyperplane hash with int8 planes
+       [L][k][128] (host or device memory), as sift_lsh_match.
+     sift_mlp_index_create: the learned hash `model` (L = 1 table).
+   sift_index_search: 2-NN of q_n uint8 device queries as sift_lsh_match
+   (probes: 1..2^min(6, k) buckets per table, query-directed multi-probe), with
+   the exact fallback of sift_mlp_match when min_candidates > 0 or
+   max_dist > 0 (then it synchronises once). Outputs as sift_mlp_match.
+   sift_index_buckets: copies the bucket table into caller device buffers
+   (start, order, ocode laid out as sift_lsh_buckets writes them; any may be
+   NULL) on `stream`, and returns its group bits B in top_bits. */
+typedef struct sift_code_index sift_code_index;
+SIFT_API int sift_lsh_index_create(const uint8_t* r, uint32_t r_n, const int8_t* planes, int L, int k,
+                                   sift_code_index** index);
+SIFT_API int sift_mlp_index_create(const uint8_t* r, uint32_t r_n, const sift_mlp* model, sift_code_index** index);
+SIFT_API int sift_index_search(const sift_code_index* index, const uint8_t* q, uint32_t q_n, int probes,
+                               int min_candidates, float max_dist, float threshold, uint32_t* matches,
+                               int32_t* nn_idx, float* nn_dist, uint32_t* candidates, uint32_t* fallback_count,
+                               void* stream);
+SIFT_API int sift_index_buckets(const sift_code_index* index, int* start, int* order, uint32_t* ocode, int* top_bits,
+                                void* stream);
+SIFT_API void sift_index_destroy(sift_code_index* index);
+
 /* Loss and gradients of one training step, for checking the training
    kernels: x = [3 * batch][128] uint8 device rows (queries, their
    neighbours, random rows), params / grads = SIFT_MLP_PARAMS device floats
@@ -376,6 +428,19 @@ SIFT_API int sift_profile_collect(double* total_ms, int* launches);
    the FP16 kernel), 1 the single-CTA u8 kernel, 2 the CTA-pair u8 kernel for
    every input type (half inputs packed to u8). All return identical results. */
 SIFT_API int sift_set_kernel_variant(int variant);
+
+/* Fault injection for failure-detection tests (no counterpart in the
+   reference, which checks no errors, src/knn_brute.cu:254-275). Neither hook
+   faults, traps or hangs the GPU.
+   sift_test_inject_wait_expiry(n): the next n exact searches first run a
+   one-thread probe whose bounded mbarrier wait (the wait every pipeline stage
+   of the search kernels uses) can never complete; it expires after 1 ms and
+   records the same device error an expired wait in a search records, so
+   sift_stream_status / sift2nn_noalloc_status report SIFT_ERR_DEVICE_TIMEOUT.
+   sift_test_fail_arena(n): the next n calls that request the scratch arena
+   fail with SIFT_ERR_ALLOC as if the allocation had failed. n = 0 disarms. */
+SIFT_API int sift_test_inject_wait_expiry(int calls);
+SIFT_API int sift_test_fail_arena(int calls);
 
 #ifdef __cplusplus
 }

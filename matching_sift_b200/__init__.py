@@ -20,9 +20,9 @@ from ._native import (SIFT_BATCH_SHAPE, SIFT_BATCH_TUNE, SIFT_MLP_PARAMS, sift_m
                       SiftError, check, lib, status_string)
 
 __all__ = [
-    "cublas_2nn_sift", "cublas_2nn_f", "device_brute", "host_brute", "lsh_gpu", "match", "lsh_match", "lsh_hash",
+    "cublas_2nn_sift", "cublas_2nn_f", "device_brute", "host_brute", "lsh_gpu", "match", "lsh_match", "lsh_hash", "lsh_buckets",
     "stream_status", "version", "match_batch", "match_mutual", "match_mutual_batch", "compact_matches", "BatchPlan", "batch_describe",
-    "MlpHash", "mlp_loss_grad",
+    "MlpHash", "mlp_loss_grad", "HashIndex",
     "SiftError", "FLOAT_HOST", "FLOAT_DEVICE", "HALF_DEVICE", "U8_DEVICE", "U8_HOST", "METRIC_L2", "METRIC_DOT",
 ]
 
@@ -141,6 +141,26 @@ def lsh_hash(x, planes, stream=None):
     check(lib().sift_lsh_hash(x.data_ptr(), x.shape[0], planes.data_ptr(), L, k, codes.data_ptr(), s.cuda_stream),
           "sift_lsh_hash")
     return codes
+
+
+def lsh_buckets(codes, k: int, stream=None):
+    """Bucket table of LSH codes [L, n] (CUDA int32 / uint32 view) with k bits
+    per table: (start [L, 2^B + 1], order [L, n], ocode [L, n]) as CUDA int32
+    tensors, B = min(k, 16) -- group b of table t holds the point ids
+    order[t, start[t, b]:start[t, b + 1]] (codes ocode[...]), the points whose
+    code's top B bits are b."""
+    import torch
+
+    codes = codes.contiguous()
+    L, n = codes.shape
+    top = min(k, 16)
+    start = torch.empty((L, (1 << top) + 1), dtype=torch.int32, device=codes.device)
+    order = torch.empty((L, n), dtype=torch.int32, device=codes.device)
+    ocode = torch.empty((L, n), dtype=torch.int32, device=codes.device)
+    s = stream if stream is not None else torch.cuda.current_stream(codes.device)
+    check(lib().sift_lsh_buckets(codes.data_ptr(), n, L, k, start.data_ptr(), order.data_ptr(), ocode.data_ptr(),
+                                 s.cuda_stream), "sift_lsh_buckets")
+    return start, order, ocode
 
 
 def lsh_match(q, r, planes, threshold: float = 0.0, stream=None, probes: int = 1, candidates: bool = False):
@@ -395,6 +415,84 @@ class MlpHash:
                                    _ptr(out["candidates"]), ctypes.byref(fb), s.cuda_stream), "sift_mlp_match")
         out["fallback"] = fb.value
         return out
+
+
+class HashIndex:
+    """A base hashed and bucketed once, searched many times (sift_index_*).
+
+    ``HashIndex.lsh(r, planes)`` uses int8 hyperplanes [L, k, 128];
+    ``HashIndex.mlp(r, model)`` a trained :class:`MlpHash`. The index reads
+    the base tensor ``r`` (uint8 [n, 128] on the GPU) by reference and keeps
+    it alive.
+    """
+
+    def __init__(self, handle, r, k: int, L: int, keep=None):
+        self._h = handle
+        self.r, self.k, self.L = r, k, L
+        self._keep = keep
+
+    @classmethod
+    def lsh(cls, r, planes):
+        r = r.contiguous()
+        planes = planes.contiguous()
+        h = ctypes.c_void_p()
+        check(lib().sift_lsh_index_create(_ptr(r), r.shape[0], _ptr(planes), planes.shape[0], planes.shape[1],
+                                          ctypes.byref(h)), "sift_lsh_index_create")
+        return cls(h, r, planes.shape[1], planes.shape[0])
+
+    @classmethod
+    def mlp(cls, r, model: "MlpHash"):
+        r = r.contiguous()
+        h = ctypes.c_void_p()
+        check(lib().sift_mlp_index_create(_ptr(r), r.shape[0], ctypes.byref(model._c), ctypes.byref(h)),
+              "sift_mlp_index_create")
+        return cls(h, r, model.k, 1)
+
+    def search(self, q, probes: int = 1, min_candidates: int = 0, max_dist: float = 0.0, threshold: float = 0.0,
+               stream=None):
+        """{"matches", "nn_idx", "nn_dist", "candidates", "fallback"} for uint8 CUDA queries q [n, 128]."""
+        import torch
+
+        q = q.contiguous()
+        n = q.shape[0]
+        out = {"matches": torch.empty(n, dtype=torch.int32, device=q.device),
+               "nn_idx": torch.empty((n, 2), dtype=torch.int32, device=q.device),
+               "nn_dist": torch.empty((n, 2), dtype=torch.float32, device=q.device),
+               "candidates": torch.empty(n, dtype=torch.int32, device=q.device)}
+        fb = ctypes.c_uint32(0)
+        s = stream if stream is not None else torch.cuda.current_stream(q.device)
+        check(lib().sift_index_search(self._h, _ptr(q), n, probes, min_candidates, max_dist, threshold,
+                                      _ptr(out["matches"]), _ptr(out["nn_idx"]), _ptr(out["nn_dist"]),
+                                      _ptr(out["candidates"]), ctypes.byref(fb), s.cuda_stream), "sift_index_search")
+        out["fallback"] = fb.value
+        return out
+
+    def buckets(self, stream=None):
+        """The bucket table as CUDA int32 tensors (start [L, 2^B + 1], order [L, n],
+        ocode [L, n]) and its group bits B, laid out as :func:`lsh_buckets`."""
+        import torch
+
+        top = ctypes.c_int(0)
+        check(lib().sift_index_buckets(self._h, None, None, None, ctypes.byref(top), None), "sift_index_buckets")
+        dev, n = self.r.device, self.r.shape[0]
+        start = torch.empty((self.L, (1 << top.value) + 1), dtype=torch.int32, device=dev)
+        order = torch.empty((self.L, n), dtype=torch.int32, device=dev)
+        ocode = torch.empty((self.L, n), dtype=torch.int32, device=dev)
+        s = stream if stream is not None else torch.cuda.current_stream(dev)
+        check(lib().sift_index_buckets(self._h, _ptr(start), _ptr(order), _ptr(ocode), ctypes.byref(top),
+                                       s.cuda_stream), "sift_index_buckets")
+        return start, order, ocode, top.value
+
+    def close(self):
+        if self._h is not None and self._h.value:
+            lib().sift_index_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def mlp_loss_grad(x, batch: int, k: int, params, neg_weight: float = 1.0, balance_weight: float = 1.0):

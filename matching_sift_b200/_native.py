@@ -43,6 +43,7 @@ _PROTOS = {
     "lsh_gpu": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, _vp, ctypes.c_float, _vp,
                                ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "sift_lsh_hash": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "sift_lsh_buckets": (ctypes.c_int, [_vp, ctypes.c_uint32, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]),
     "sift_lsh_match_probes": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, _vp,
                                              ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, _vp, _vp, _vp,
                                              _vp, _vp]),
@@ -50,6 +51,9 @@ _PROTOS = {
                                       ctypes.c_int, ctypes.c_float, _vp, _vp, _vp, _vp]),
     "sift2nn_match_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, _vp, _vp,
                                              _vp, _vp]),
+    "sift2nn_noalloc_status": (ctypes.c_int, [_vp]),
+    "sift_test_inject_wait_expiry": (ctypes.c_int, [ctypes.c_int]),
+    "sift_test_fail_arena": (ctypes.c_int, [ctypes.c_int]),
     "sift2nn_match_batch": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_int, ctypes.c_float, _vp, _vp,
                                            _vp, _vp]),
     "sift_merge_top2": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_float, _vp, _vp, _vp,
@@ -73,6 +77,13 @@ _PROTOS = {
     "sift_mlp_match": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, _vp, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_float, ctypes.c_float, _vp, _vp, _vp, _vp,
                                       ctypes.POINTER(ctypes.c_uint32), _vp]),
+    "sift_lsh_index_create": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, ctypes.c_int, ctypes.c_int,
+                                             ctypes.POINTER(_vp)]),
+    "sift_mlp_index_create": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, ctypes.POINTER(_vp)]),
+    "sift_index_search": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                         ctypes.c_float, _vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_uint32), _vp]),
+    "sift_index_buckets": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_int), _vp]),
+    "sift_index_destroy": (None, [_vp]),
     "sift_mlp_loss_grad": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.c_float, ctypes.c_float, _vp,
                                           ctypes.POINTER(ctypes.c_float)]),
 }

@@ -70,6 +70,7 @@ int ensure_ready(DeviceCtx*& out, int& dev) {
             if (cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking) != cudaSuccess) return SIFT_ERR_CUDA;
             for (auto& e : c.chunk_ev)
                 if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return SIFT_ERR_CUDA;
+            if (cudaEventCreateWithFlags(&c.arena_ev, cudaEventDisableTiming) != cudaSuccess) return SIFT_ERR_CUDA;
             if (cudaDeviceSynchronize() != cudaSuccess) return SIFT_ERR_CUDA;
             c.ready = true;
         }
@@ -79,6 +80,7 @@ int ensure_ready(DeviceCtx*& out, int& dev) {
 }
 
 int ensure_arena(DeviceCtx& c, size_t bytes) {
+    if (arena_fault()) return SIFT_ERR_ALLOC;
     if (bytes <= c.arena_bytes) return SIFT_OK;
     if (c.arena) {
         cudaDeviceSynchronize();
@@ -415,8 +417,8 @@ int exact_match(const MatchArgs& a) {
     int dev = 0;
     SIFT_TRY(ensure_ready(cp, dev));
     DeviceCtx& c = *cp;
-    std::lock_guard<std::mutex> lk(c.mu);
     cudaStream_t st = static_cast<cudaStream_t>(a.stream);
+    ArenaLock lk(c, st);
     const int q_n = static_cast<int>(a.q_n), r_n = static_cast<int>(a.r_n);
     if (q_n == 0) return SIFT_OK;
 
@@ -485,6 +487,7 @@ int exact_match(const MatchArgs& a) {
             SIFT_TRY(encode_u8_rows(&qmap, qd, q_n, kBM));
             SIFT_TRY(encode_u8_rows(&bmap, rd, r_n, use_pair ? kBN / 2 : kBN));
         }
+        SIFT_CUDA(maybe_inject_wait_expiry(c.d_status, st));
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         const bool prof = g_profile.load();
         if (prof) {
@@ -550,14 +553,13 @@ int lsh_match(const LshArgs& a) {
     int dev = 0;
     SIFT_TRY(ensure_ready(cp, dev));
     DeviceCtx& c = *cp;
-    std::lock_guard<std::mutex> lk(c.mu);
     cudaStream_t st = static_cast<cudaStream_t>(a.stream);
+    ArenaLock lk(c, st);
     const int q_n = static_cast<int>(a.q_n), r_n = static_cast<int>(a.r_n);
     if (q_n == 0) return SIFT_OK;
     const int L_ = a.L, k = a.k, P = lsh_planes_padded(L_, k);
     const int top = k < kLshMaxTopBits ? k : kLshMaxTopBits;
     const int shift = k - top, nbins = 1 << top;
-    const int r_pad = ((r_n + 127) / 128) * 128, q_pad = ((q_n + 127) / 128) * 128;
 
     const bool m_dev = !a.matches || is_device_accessible(a.matches);
     const bool i_dev = !a.nn_idx || is_device_accessible(a.nn_idx);
@@ -578,8 +580,6 @@ int lsh_match(const LshArgs& a) {
     const size_t o_start = L.take(static_cast<size_t>(L_) * (nbins + 1) * 4);
     const size_t o_order = L.take(static_cast<size_t>(L_) * r_n * 4 + 16);
     const size_t o_ocode = L.take(static_cast<size_t>(L_) * r_n * 4 + 16);
-    const size_t o_qn = L.take(static_cast<size_t>(q_pad) * 4);
-    const size_t o_rn = L.take(static_cast<size_t>(r_pad) * 4 + 16);
     const size_t o_m = (a.matches && !m_dev) ? L.take(static_cast<size_t>(q_n) * 4) : 0;
     const size_t o_i = (a.nn_idx && !i_dev) ? L.take(static_cast<size_t>(q_n) * 8) : 0;
     const size_t o_d = (a.nn_dist && !d_dev) ? L.take(static_cast<size_t>(q_n) * 8) : 0;
@@ -601,12 +601,7 @@ int lsh_match(const LshArgs& a) {
     int* start = reinterpret_cast<int*>(A + o_start);
     int* order = reinterpret_cast<int*>(A + o_order);
     uint32_t* ocode = reinterpret_cast<uint32_t*>(A + o_ocode);
-    int32_t* qnorm = reinterpret_cast<int32_t*>(A + o_qn);
-    int32_t* rnorm = reinterpret_cast<int32_t*>(A + o_rn);
 
-    SIFT_CUDA(launch_row_norms_u8(rd, r_n, r_pad, kMetricL2, rnorm, nullptr, nullptr, st));
-    SIFT_CUDA(launch_row_norms_u8(qd, q_n, q_pad, kMetricL2, qnorm, nullptr, nullptr, st));
-    g_launches += (r_pad > 0 ? 1 : 0) + 1;
     CUtensorMap pmap, qmap, rmap;
     SIFT_TRY(encode_i8_rows(&pmap, pl, static_cast<uint64_t>(L_) * k, static_cast<uint32_t>(P)));
     SIFT_TRY(encode_u8_rows(&qmap, qd, q_n, 128));
@@ -632,9 +627,9 @@ int lsh_match(const LshArgs& a) {
     uint32_t* m_out = (a.matches && !m_dev) ? reinterpret_cast<uint32_t*>(A + o_m) : a.matches;
     int32_t* i_out = (a.nn_idx && !i_dev) ? reinterpret_cast<int32_t*>(A + o_i) : a.nn_idx;
     float* d_out = (a.nn_dist && !d_dev) ? reinterpret_cast<float*>(A + o_d) : a.nn_dist;
-    SIFT_CUDA(launch_lsh_scan(qd, rd, q_n, r_n, L_, a.probes, shift, nbins, probe_codes, start, order, ocode, qnorm,
-                              rnorm, a.threshold, a.ratio ? 1 : 0, ldexpf(1.0f, -2 * vshift), m_out, a.candidates,
-                              i_out, d_out, st));
+    SIFT_CUDA(launch_lsh_scan(qd, rd, q_n, r_n, L_, a.probes, shift, nbins, probe_codes, start, order, ocode,
+                              a.threshold, a.ratio ? 1 : 0, ldexpf(1.0f, -2 * vshift), m_out, a.candidates, i_out,
+                              d_out, st));
     g_launches += 1 + (r_n > 0 ? 3 : 0) + 1;
     if (a.matches && !m_dev)
         SIFT_CUDA(cudaMemcpyAsync(a.matches, m_out, static_cast<size_t>(q_n) * 4, cudaMemcpyDeviceToHost, st));
@@ -668,6 +663,36 @@ int lsh_hash(const uint8_t* x, uint32_t n, const int8_t* planes, int L_, int k, 
     SIFT_CUDA(launch_lsh_hash(xmap, pmap, static_cast<int>(n), P, L_, k, codes, nullptr, cp->d_status, cp->num_sms,
                               static_cast<cudaStream_t>(stream)));
     ++g_launches;
+    return SIFT_OK;
+}
+
+// Bucket table of given codes (the counting sort lsh_match runs on the base):
+// per table, points grouped by the top min(k, 16) code bits. Replaces the
+// reference's thrust sort + host run-length loop (lsh_thread_sort_reduce,
+// src/lsh_h.cu:587-620) and exposes the grouping for inspection.
+int lsh_buckets(const uint32_t* codes, uint32_t n, int L_, int k, int* start, int* order, uint32_t* ocode,
+                void* stream) {
+    if (L_ < 1 || k < 1 || k > 32 || L_ * k > kLshMaxPlanes || !start) return SIFT_ERR_INVALID_ARG;
+    if (n > 0x7fffffffu / static_cast<uint32_t>(L_)) return SIFT_ERR_INVALID_ARG;
+    if (n && (!codes || !order || !ocode)) return SIFT_ERR_INVALID_ARG;
+    if (!is_device_accessible(start) || (n && (!is_device_accessible(codes) || !is_device_accessible(order) ||
+                                               !is_device_accessible(ocode))))
+        return SIFT_ERR_INVALID_ARG;
+    DeviceCtx* cp = nullptr;
+    int dev = 0;
+    SIFT_TRY(ensure_ready(cp, dev));
+    DeviceCtx& c = *cp;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    ArenaLock lk(c, st);
+    const int top = k < kLshMaxTopBits ? k : kLshMaxTopBits;
+    const int nbins = 1 << top;
+    Layout L;
+    const size_t o_hist = L.take(static_cast<size_t>(L_) * nbins * 4);
+    SIFT_TRY(ensure_arena(c, L.off));
+    int* hist = reinterpret_cast<int*>(c.arena + o_hist);
+    SIFT_CUDA(launch_lsh_buckets(codes, static_cast<int>(n), L_, k - top, nbins, hist, start, order, ocode, c.num_sms,
+                                 st));
+    g_launches += n > 0 ? 3 : 0;
     return SIFT_OK;
 }
 
@@ -796,6 +821,11 @@ int sift_stream_status(void* stream) { return sift::stream_status(stream); }
 
 int sift_lsh_hash(const uint8_t* x, uint32_t n, const int8_t* planes, int L, int k, uint32_t* codes, void* stream) {
     return sift::lsh_hash(x, n, planes, L, k, codes, stream);
+}
+
+int sift_lsh_buckets(const uint32_t* codes, uint32_t n, int L, int k, int* start, int* order, uint32_t* ocode,
+                     void* stream) {
+    return sift::lsh_buckets(codes, n, L, k, start, order, ocode, stream);
 }
 
 int sift_lsh_match_probes(const void* q, const void* r, int type, uint32_t q_n, uint32_t r_n, const int8_t* planes,

@@ -44,6 +44,8 @@ int mlp_train(const uint8_t* base, uint32_t r_n, const uint8_t* tq, uint32_t t_n
               float lr, float neg_w, float bal_w, unsigned long long seed, void* w1_out, float* b1_out, void* w2_out,
               float* b2_out, float* params_out, float* loss_curve);
 int lsh_hash(const uint8_t* x, uint32_t n, const int8_t* planes, int L, int k, uint32_t* codes, void* stream);
+int lsh_buckets(const uint32_t* codes, uint32_t n, int L, int k, int* start, int* order, uint32_t* ocode,
+                void* stream);
 void reference_planes(int L, int nbits, int8_t* out);
 int stream_status(void* stream);
 void set_last_status(int s);

@@ -178,8 +178,8 @@ int match_batch(const uint8_t* q, const uint8_t* r, uint32_t r_rows, const sift_
     SIFT_TRY(build(pairs, n_pairs, r_rows, kShapes[shape].qpt, c.num_sms / 2, b));
     SIFT_TRY(check_io(q, r, r_rows, b.total_q, matches, nn_idx, nn_dist));
     if (b.total_q == 0) return SIFT_OK;
-    std::lock_guard<std::mutex> lk(c.mu);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    detail::ArenaLock lk(c, st);
     const BatchLayout o = layout_for(&b, 1);
     SIFT_TRY(detail::ensure_arena(c, o.bytes));
     const Buffers m = buffers_at(c.arena, o);
@@ -267,8 +267,8 @@ int match_mutual_batch(const uint8_t* a, const uint8_t* b, uint32_t b_rows, cons
     if (bf.total_q == 0) return SIFT_OK;
     const int total_a = bf.total_q, total_b = static_cast<int>(brow);
 
-    std::lock_guard<std::mutex> lk(c.mu);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    detail::ArenaLock lk(c, st);
     const BatchLayout lf = layout_for(&bf, 1), lr = layout_for(&br, 1);
     detail::Layout L;
     const size_t o_f = L.take(lf.bytes), o_r = L.take(lr.bytes);
@@ -441,8 +441,8 @@ int compact_matches(const uint32_t* matches, const float* nn_dist, uint32_t rows
         (nn_dist && !detail::is_device_accessible(nn_dist)) ||
         (capacity > 0 && (!out || !detail::is_device_accessible(out))))
         return SIFT_ERR_INVALID_ARG;
-    std::lock_guard<std::mutex> lk(c.mu);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    detail::ArenaLock lk(c, st);
     const int n_blocks = static_cast<int>((rows + kCompactRows - 1) / kCompactRows);
     detail::Layout L;
     const size_t o_cnt = L.take(sizeof(int) * (static_cast<size_t>(n_blocks) + 1));

@@ -27,6 +27,43 @@ struct DeviceCtx {
     int* h_status = nullptr;  // pinned mirror of d_status
     cudaStream_t copy_stream = nullptr;  // host->device chunk copies that overlap the search
     cudaEvent_t chunk_ev[17] = {};       // per-chunk "landed" events + one "arena free" event
+    cudaEvent_t arena_ev = nullptr;      // recorded after the last call's arena work
+    bool arena_used = false;
+};
+
+// Holds the device's mutex for one call that uses the arena and orders the
+// call's GPU work after the previous call's: the mutex only orders when work
+// is enqueued, so two calls on different streams would otherwise run at the
+// same time on the GPU over the same scratch. The constructor makes `st` wait
+// for the event recorded by the previous call; the destructor records it on
+// `st` after this call's work. Streams being captured into a graph neither
+// wait nor record (a captured call is ordered by the graph's launch).
+class ArenaLock {
+public:
+    ArenaLock(DeviceCtx& c, cudaStream_t st) : c_(c), lk_(c.mu), st_(st) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
+            cudaGetLastError();
+            cs = cudaStreamCaptureStatusActive;
+        }
+        capturing_ = cs != cudaStreamCaptureStatusNone;
+        if (!capturing_ && c.arena_used && cudaStreamWaitEvent(st, c.arena_ev, 0) != cudaSuccess) cudaGetLastError();
+    }
+    ~ArenaLock() {
+        if (capturing_) return;
+        if (cudaEventRecord(c_.arena_ev, st_) == cudaSuccess)
+            c_.arena_used = true;
+        else
+            cudaGetLastError();
+    }
+    ArenaLock(const ArenaLock&) = delete;
+    ArenaLock& operator=(const ArenaLock&) = delete;
+
+private:
+    DeviceCtx& c_;
+    std::lock_guard<std::mutex> lk_;
+    cudaStream_t st_;
+    bool capturing_ = false;
 };
 
 // 256-byte aligned bump layout over the arena.
@@ -56,6 +93,11 @@ int encode_bf16_2d(CUtensorMap* m, const void* base, uint64_t inner, uint64_t ro
 int map_cuda(cudaError_t e);
 // Reads and clears the device status words. Caller has synchronised `st`.
 int collect_device_status(DeviceCtx& c, cudaStream_t st);
+// Fault injection for the failure-detection tests (faults.cu): launches the
+// wait-expiry probe on `st` when armed, recording into *err.
+cudaError_t maybe_inject_wait_expiry(int* err, cudaStream_t st);
+// True when the next arena request is armed to fail.
+bool arena_fault();
 
 }  // namespace detail
 }  // namespace sift

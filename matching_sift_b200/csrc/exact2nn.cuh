@@ -33,6 +33,7 @@ enum DeviceError : int {
     kErrWaitEpilogue = 4,
     kErrWaitQuery = 5,
     kErrWaitDrain = 6,
+    kErrWaitProbe = 7,  // the fault-injection probe (faults.cu) let its wait expire
 };
 
 // Work decomposition of one exact search. A "unit" is (query group g, base

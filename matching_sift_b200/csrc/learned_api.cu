@@ -9,6 +9,7 @@
 #include "api_internal.h"
 #include "context.h"
 #include "exact2nn.cuh"
+#include "index.cuh"
 #include "learned.cuh"
 #include "lsh.cuh"
 
@@ -16,43 +17,6 @@ namespace sift {
 namespace {
 
 using detail::DeviceCtx;
-
-// Queries whose probed buckets compared fewer than min_cand candidates, or
-// (max_dist > 0) whose nearest candidate lies farther than max_dist.
-__global__ void flag_kernel(const uint32_t* __restrict__ counts, const float* __restrict__ dist, int n,
-                            uint32_t min_cand, float max_dist, int* __restrict__ idx, int* __restrict__ n_out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const bool far = max_dist > 0.0f && !(dist[2 * i] <= max_dist);
-    if (counts[i] < min_cand || far) idx[atomicAdd(n_out, 1)] = i;
-}
-
-__global__ void gather_rows_kernel(const uint8_t* __restrict__ q, const int* __restrict__ idx, int n,
-                                   uint8_t* __restrict__ out) {
-    const long long e = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-    if (e >= static_cast<long long>(n) * 8) return;
-    const int f = static_cast<int>(e >> 3), c = static_cast<int>(e & 7);
-    reinterpret_cast<uint4*>(out + static_cast<size_t>(f) * kDim)[c] =
-        reinterpret_cast<const uint4*>(q + static_cast<size_t>(idx[f]) * kDim)[c];
-}
-
-__global__ void scatter_results_kernel(const int* __restrict__ idx, int n, const uint32_t* __restrict__ m_in,
-                                       const int32_t* __restrict__ i_in, const float* __restrict__ d_in,
-                                       uint32_t* __restrict__ matches, int32_t* __restrict__ nn_idx,
-                                       float* __restrict__ nn_dist) {
-    const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= n) return;
-    const int q = idx[f];
-    if (matches) matches[q] = m_in[f];
-    if (nn_idx) {
-        nn_idx[2 * q] = i_in[2 * f];
-        nn_idx[2 * q + 1] = i_in[2 * f + 1];
-    }
-    if (nn_dist) {
-        nn_dist[2 * q] = d_in[2 * f];
-        nn_dist[2 * q + 1] = d_in[2 * f + 1];
-    }
-}
 
 int encode_model(const MlpModel& m, CUtensorMap* w1map, CUtensorMap* w2map) {
     SIFT_TRY(detail::encode_bf16_2d(w1map, m.w1, kMlpIn, kMlpHidden, 64, kMlpHidden));
@@ -120,20 +84,14 @@ int mlp_match(const uint8_t* q, const uint8_t* r, uint32_t q_n_, uint32_t r_n_, 
     int dev = 0;
     SIFT_TRY(detail::ensure_ready(cp, dev));
     DeviceCtx& c = *cp;
-    std::lock_guard<std::mutex> lk(c.mu);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    detail::ArenaLock lk(c, st);
     const int q_n = static_cast<int>(q_n_), r_n = static_cast<int>(r_n_);
     const MlpModel m = to_model(model);
     const int k = m.k;
     const int top = k < kLshMaxTopBits ? k : kLshMaxTopBits;
     const int shift = k - top, nbins = 1 << top;
     const int flip = k < 6 ? k : 6;
-    const int q_pad = ((q_n + 127) / 128) * 128, r_pad = ((r_n + 127) / 128) * 128;
-    // Exact fallback over at most q_n gathered queries: scratch for the worst
-    // case (a group of 512 queries spans at most grid / groups + 2 workers).
-    const ExactPlan worst = make_exact_plan(q_n, r_n, c.num_sms / 2, 2);
-    const size_t fb_part = static_cast<size_t>(worst.grid + 2 * worst.q_groups + 2) * (kQT * kBM) * 2 * sizeof(int4);
-
     detail::Layout L;
     const size_t o_cr = L.take(static_cast<size_t>(r_n) * 4 + 16);
     const size_t o_cq = L.take(static_cast<size_t>(q_n) * 4);
@@ -143,19 +101,10 @@ int mlp_match(const uint8_t* q, const uint8_t* r, uint32_t q_n_, uint32_t r_n_, 
     const size_t o_start = L.take(static_cast<size_t>(nbins + 1) * 4);
     const size_t o_order = L.take(static_cast<size_t>(r_n) * 4 + 16);
     const size_t o_ocode = L.take(static_cast<size_t>(r_n) * 4 + 16);
-    const size_t o_qn = L.take(static_cast<size_t>(q_pad) * 4);
-    const size_t o_rn = L.take(static_cast<size_t>(r_pad) * 4 + 16);
     const size_t o_cnt = L.take(static_cast<size_t>(q_n) * 4);
-    const size_t o_fidx = L.take(static_cast<size_t>(q_n) * 4 + 16);
-    const size_t o_frows = L.take(static_cast<size_t>(q_n) * kDim + 16);
-    const size_t o_fm = L.take(static_cast<size_t>(q_n) * 4);
-    const size_t o_fi = L.take(static_cast<size_t>(q_n) * 8);
-    const size_t o_fd = L.take(static_cast<size_t>(q_n) * 8);
-    const size_t o_brec = L.take(static_cast<size_t>(worst.base_tiles) * kRecInts * 4 + 16);
-    const size_t o_fqn = L.take(static_cast<size_t>(q_pad) * 4);
-    const size_t o_fthr = L.take(static_cast<size_t>(q_pad) * 4);
-    const size_t o_fpart = L.take(fb_part);
     const size_t o_dist = L.take(static_cast<size_t>(q_n) * 8);  // distances when the caller takes none
+    FallbackScratch fs{};
+    fallback_layout(L, q_n, r_n, c.num_sms / 2, true, fs);
     SIFT_TRY(detail::ensure_arena(c, L.off));
     char* A = c.arena;
     auto U32 = [&](size_t o) { return reinterpret_cast<uint32_t*>(A + o); };
@@ -173,60 +122,25 @@ int mlp_match(const uint8_t* q, const uint8_t* r, uint32_t q_n_, uint32_t r_n_, 
                                   st));
         SIFT_CUDA(launch_lsh_buckets(U32(o_cr), r_n, 1, shift, nbins, I32(o_hist), I32(o_start), I32(o_order),
                                      U32(o_ocode), c.num_sms, st));
-        SIFT_CUDA(launch_row_norms_u8(r, r_n, r_pad, kMetricL2, I32(o_rn), nullptr, nullptr, st));
-        launches += 5;
+        launches += 4;
     } else {
         SIFT_CUDA(cudaMemsetAsync(I32(o_start), 0, static_cast<size_t>(nbins + 1) * 4, st));
     }
-    SIFT_CUDA(launch_row_norms_u8(q, q_n, q_pad, kMetricL2, I32(o_qn), nullptr, nullptr, st));
     CUtensorMap qmap_h;
     SIFT_TRY(detail::encode_u8_rows(&qmap_h, q, q_n, 128));
     SIFT_CUDA(launch_mlp_hash(qmap_h, q_n, w1map, w2map, m.b1, m.b2, k, U32(o_cq), reinterpret_cast<float*>(A + o_z),
                               c.d_status, c.num_sms, st));
     SIFT_CUDA(launch_probe_codes(U32(o_cq), reinterpret_cast<float*>(A + o_z), q_n, k, flip, n_probes, U32(o_pc), st));
     SIFT_CUDA(launch_lsh_scan(q, r, q_n, r_n, 1, n_probes, shift, nbins, U32(o_pc), I32(o_start), I32(o_order),
-                              U32(o_ocode), I32(o_qn), I32(o_rn), threshold, threshold > 0.f ? 1 : 0, 1.0f, matches,
-                              counts, nn_idx, dist, st));
-    launches += 4;
+                              U32(o_ocode), threshold, threshold > 0.f ? 1 : 0, 1.0f, matches, counts, nn_idx, dist,
+                              st));
+    launches += 3;
     detail::g_launches += launches;
     if ((min_candidates <= 0 && max_dist <= 0.0f) || r_n == 0) return SIFT_OK;
 
     // ---- exact fallback for queries with too few candidates
-    int* fidx = I32(o_fidx);
-    int* fcount = fidx + q_n;  // the 16 bytes past the index list
-    SIFT_CUDA(cudaMemsetAsync(fcount, 0, sizeof(int), st));
-    flag_kernel<<<(q_n + 255) / 256, 256, 0, st>>>(counts, dist, q_n, static_cast<uint32_t>(min_candidates), max_dist,
-                                                    fidx, fcount);
-    SIFT_CUDA(cudaGetLastError());
-    SIFT_CUDA(cudaMemcpyAsync(c.h_status + 1, fcount, sizeof(int), cudaMemcpyDeviceToHost, st));
-    SIFT_CUDA(cudaStreamSynchronize(st));
-    const int nf = c.h_status[1];
-    if (fallback_count) *fallback_count = static_cast<uint32_t>(nf);
-    ++detail::g_launches;
-    if (nf == 0) return SIFT_OK;
-    uint8_t* frows = reinterpret_cast<uint8_t*>(A + o_frows);
-    gather_rows_kernel<<<static_cast<unsigned>((static_cast<long long>(nf) * 8 + 255) / 256), 256, 0, st>>>(
-        q, fidx, nf, frows);
-    SIFT_CUDA(cudaGetLastError());
-    const ExactPlan plan = make_exact_plan(nf, r_n, c.num_sms / 2, 2);
-    if (static_cast<size_t>(plan.max_splits) * plan.parts * plan.q_pad * sizeof(int4) > fb_part)
-        return SIFT_ERR_INVALID_ARG;  // guard: fb_part bounds every plan of <= q_n queries
-    int32_t* brec = I32(o_brec);
-    SIFT_CUDA(launch_row_norms_u8(r, r_n, plan.r_pad, kMetricL2, nullptr, brec, nullptr, st));
-    SIFT_CUDA(launch_row_norms_u8(frows, nf, plan.q_pad, kMetricL2, I32(o_fqn), nullptr, I32(o_fthr), st));
-    CUtensorMap qmap, bmap;
-    SIFT_TRY(detail::encode_u8_rows(&qmap, frows, nf, kBM));
-    SIFT_TRY(detail::encode_u8_rows(&bmap, r, r_n, kBN / 2));
-    int4* part = reinterpret_cast<int4*>(A + o_fpart);
-    SIFT_CUDA(launch_exact2nn_u8_pair(qmap, bmap, brec, plan, part, I32(o_fthr), c.d_status, st));
-    uint32_t* fm = U32(o_fm);
-    int32_t* fi = I32(o_fi);
-    float* fd = reinterpret_cast<float*>(A + o_fd);
-    SIFT_CUDA(launch_merge2nn(part, plan, I32(o_fqn), kMetricL2, threshold, 1.0f, fm, nullptr, fi, fd, st));
-    scatter_results_kernel<<<(nf + 255) / 256, 256, 0, st>>>(fidx, nf, fm, fi, fd, matches, nn_idx, nn_dist);
-    SIFT_CUDA(cudaGetLastError());
-    detail::g_launches += 6;
-    return SIFT_OK;
+    return exact_fallback(c, A, fs, q, r, q_n, r_n, nullptr, counts, dist, min_candidates, max_dist, threshold,
+                          matches, nn_idx, nn_dist, fallback_count, st);
 }
 
 int mlp_loss_grad(const uint8_t* x, int B, int k, const float* params, float neg_w, float bal_w, float* grads,
@@ -238,7 +152,7 @@ int mlp_loss_grad(const uint8_t* x, int B, int k, const float* params, float neg
     int dev = 0;
     SIFT_TRY(detail::ensure_ready(cp, dev));
     DeviceCtx& c = *cp;
-    std::lock_guard<std::mutex> lk(c.mu);
+    detail::ArenaLock lk(c, nullptr);
     const int R = 3 * B;
     detail::Layout L;
     const size_t o_w1b = L.take(kMlpHidden * kMlpIn * 2);

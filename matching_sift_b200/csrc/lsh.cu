@@ -21,9 +21,11 @@
 // instead, src/lsh_h.cu:599,617 vs :469,482, which is not the bucket).
 //
 // Candidate scan. One warp per query over its L buckets (L x P with P probe
-// codes per table: multi-probe); each lane takes one candidate at a time and forms |q - b|^2 = |q|^2 + |b|^2 - 2 q.b with dp4a;
-// the per-query top-2 is lexicographic in (distance, index) and counts a base
-// point found in several tables once.
+// codes per table: multi-probe); candidate rows are fetched by groups of 8
+// lanes with coalesced 16-byte loads (4 rows per warp-wide load) and scored as
+// |q - b|^2 = |q|^2 + |b|^2 - 2 q.b with dp4a; the per-query top-2 is
+// lexicographic in (distance, index) and counts a base point found in several
+// tables once.
 #include <climits>
 #include <cfloat>
 #include <cstdint>
@@ -290,32 +292,34 @@ __device__ __forceinline__ void push_dedup(int d, int i, int& d1, int& i1, int& 
     }
 }
 
-// One warp per query. Each lane holds the query row (32 words) and scans one
-// candidate at a time; lanes' top-2 lists are merged at the end.
-__global__ void __launch_bounds__(256) lsh_scan_kernel(const uint8_t* __restrict__ q, const uint8_t* __restrict__ r,
-                                                       int q_n, int r_n, int L, int probes, int shift, int nbins,
-                                                       const uint32_t* __restrict__ qcodes,
-                                                       const int* __restrict__ start, const int* __restrict__ order,
-                                                       const uint32_t* __restrict__ ocode,
-                                                       const int32_t* __restrict__ qnorm,
-                                                       const int32_t* __restrict__ rnorm, float thr, int ratio,
-                                                       float dscale, uint32_t* __restrict__ matches,
-                                                       uint32_t* __restrict__ counts,
-                                                       int32_t* __restrict__ nn_idx,
-                                                       float* __restrict__ nn_dist) {
+// One warp per query, its buckets walked 32 positions at a time. The ids and
+// codes of a chunk are one coalesced 128-byte load each (the next chunk's are
+// fetched while the current chunk's rows load); members whose full code
+// matches are compacted through shared memory; then every 8 lanes fetch one
+// candidate row with coalesced 16-byte loads (4 rows per warp-wide load, up
+// to 8 loads = 32 rows in flight per lane before any arithmetic), each lane
+// forms the squared distance of its 16 bytes (byte-wise absolute difference,
+// then dp4a) and 3 shuffles sum them: exact integers, no norms needed. The
+// lane leading each group of 8 keeps a lexicographic (distance, index)
+// top-2; the four lists are merged at the end. A base row found in several
+// tables (or probes) is compared each time but enters a list once.
+constexpr int kScanThreads = 256;
+
+__global__ void __launch_bounds__(kScanThreads) lsh_scan_kernel(
+    const uint8_t* __restrict__ q, const uint8_t* __restrict__ r, int q_n, int r_n, int L, int probes, int shift,
+    int nbins, const uint32_t* __restrict__ qcodes, const int* __restrict__ start, const int* __restrict__ order,
+    const uint32_t* __restrict__ ocode, float thr, int ratio, float dscale, uint32_t* __restrict__ matches,
+    uint32_t* __restrict__ counts, int32_t* __restrict__ nn_idx, float* __restrict__ nn_dist) {
+    __shared__ int s_ids[kScanThreads / 32][32];
     const int wq = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
+    const int sub = lane >> 3, part = lane & 7;  // row slot of a 4-row load, 16-byte chunk of the row
     if (wq >= q_n) return;
-    uint32_t qw[32];
-    const uint4* qrow = reinterpret_cast<const uint4*>(q + static_cast<size_t>(wq) * 128);
-    #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-        const uint4 x = __ldg(qrow + c);
-        qw[4 * c] = x.x; qw[4 * c + 1] = x.y; qw[4 * c + 2] = x.z; qw[4 * c + 3] = x.w;
-    }
-    const int nq = qnorm[wq];
+    int* ids = s_ids[threadIdx.x >> 5];
+    const uint4 qv = __ldg(reinterpret_cast<const uint4*>(q + static_cast<size_t>(wq) * 128) + part);
+    const bool whole_bins = shift == 0;  // a group holds exactly one code
     int d1 = INT_MAX, i1 = -1, d2 = INT_MAX, i2 = -1;
-    uint32_t seen = 0;  // candidates this lane compared (bucket members)
+    uint32_t seen = 0;  // candidates compared (bucket members)
     for (int c = 0; c < L * probes; ++c) {
         const int t = c / probes;  // probe c of the query searches table t
         const uint32_t code = qcodes[static_cast<size_t>(c) * q_n + wq];
@@ -328,34 +332,69 @@ __global__ void __launch_bounds__(256) lsh_scan_kernel(const uint8_t* __restrict
         const int s = st[bin], e = st[bin + 1];
         const int* ord = order + static_cast<size_t>(t) * r_n;
         const uint32_t* oc = ocode + static_cast<size_t>(t) * r_n;
-        for (int p = s + lane; p < e; p += 32) {
-            if (oc[p] != code) continue;
-            ++seen;
-            const int id = ord[p];
-            const uint4* rrow = reinterpret_cast<const uint4*>(r + static_cast<size_t>(id) * 128);
-            uint32_t dot = 0;
-            #pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                const uint4 x = __ldg(rrow + c);
-                dot = __dp4a(qw[4 * c], x.x, dot);
-                dot = __dp4a(qw[4 * c + 1], x.y, dot);
-                dot = __dp4a(qw[4 * c + 2], x.z, dot);
-                dot = __dp4a(qw[4 * c + 3], x.w, dot);
+        int nid = -1;
+        uint32_t ncode = ~code;
+        if (s + lane < e) {
+            nid = ord[s + lane];
+            ncode = whole_bins ? code : oc[s + lane];
+        }
+        for (int p0 = s; p0 < e; p0 += 32) {
+            const int id = nid;
+            const bool hit = id >= 0 && ncode == code;
+            const int pn = p0 + 32 + lane;
+            nid = -1;
+            ncode = ~code;
+            if (pn < e) {
+                nid = ord[pn];
+                ncode = whole_bins ? code : oc[pn];
             }
-            const int dist = nq + rnorm[id] - 2 * static_cast<int>(dot);
-            push_dedup(dist, id, d1, i1, d2, i2);
+            const uint32_t mask = __ballot_sync(0xffffffffu, hit);
+            const int nm = __popc(mask);
+            if (nm == 0) continue;
+            seen += nm;
+            if (hit) ids[__popc(mask & ((1u << lane) - 1u))] = id;
+            __syncwarp();
+            uint4 rv[8];
+            int cid[8];
+            #pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int rank = 4 * j + sub;
+                cid[j] = rank < nm ? ids[rank] : -1;
+                if (cid[j] >= 0)
+                    rv[j] = __ldg(reinterpret_cast<const uint4*>(r + static_cast<size_t>(cid[j]) * 128) + part);
+            }
+            __syncwarp();
+            #pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (4 * j >= nm) break;
+                // |q - b|^2 of this lane's 16 bytes: byte-wise |q - b| (SIMD
+                // absolute difference), then the sum of their squares by dp4a.
+                uint32_t dist = 0;
+                if (cid[j] >= 0) {
+                    uint32_t a = __vabsdiffu4(qv.x, rv[j].x);
+                    dist = __dp4a(a, a, dist);
+                    a = __vabsdiffu4(qv.y, rv[j].y);
+                    dist = __dp4a(a, a, dist);
+                    a = __vabsdiffu4(qv.z, rv[j].z);
+                    dist = __dp4a(a, a, dist);
+                    a = __vabsdiffu4(qv.w, rv[j].w);
+                    dist = __dp4a(a, a, dist);
+                }
+                dist += __shfl_xor_sync(0xffffffffu, dist, 1);
+                dist += __shfl_xor_sync(0xffffffffu, dist, 2);
+                dist += __shfl_xor_sync(0xffffffffu, dist, 4);
+                if (part == 0 && cid[j] >= 0) push_dedup(static_cast<int>(dist), cid[j], d1, i1, d2, i2);
+            }
         }
     }
-    // Merge the 32 lane lists (lexicographic, duplicates counted once).
+    // Merge the four group lists (lexicographic, duplicates counted once).
     #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
+    for (int o = 8; o < 32; o <<= 1) {
         const int od1 = __shfl_xor_sync(0xffffffffu, d1, o), oi1 = __shfl_xor_sync(0xffffffffu, i1, o);
         const int od2 = __shfl_xor_sync(0xffffffffu, d2, o), oi2 = __shfl_xor_sync(0xffffffffu, i2, o);
         push_dedup(od1, oi1, d1, i1, d2, i2);
         push_dedup(od2, oi2, d1, i1, d2, i2);
     }
-    #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) seen += __shfl_xor_sync(0xffffffffu, seen, o);
     if (lane == 0) {
         if (counts) counts[wq] = seen;
         const bool v1 = i1 >= 0, v2 = i2 >= 0;
@@ -415,15 +454,13 @@ cudaError_t launch_lsh_buckets(const uint32_t* codes, int n, int L, int shift, i
 
 cudaError_t launch_lsh_scan(const uint8_t* q, const uint8_t* r, int q_n, int r_n, int L, int probes, int shift,
                             int nbins, const uint32_t* qcodes, const int* start, const int* order,
-                            const uint32_t* ocode, const int32_t* qnorm, const int32_t* rnorm, float thr, int ratio,
-                            float dist_scale, uint32_t* matches, uint32_t* counts, int32_t* nn_idx, float* nn_dist,
-                            cudaStream_t stream) {
+                            const uint32_t* ocode, float thr, int ratio, float dist_scale, uint32_t* matches,
+                            uint32_t* counts, int32_t* nn_idx, float* nn_dist, cudaStream_t stream) {
     if (q_n <= 0) return cudaSuccess;
-    const long long blocks = (static_cast<long long>(q_n) * 32 + 255) / 256;
-    lsh_scan_kernel<<<static_cast<unsigned>(blocks), 256, 0, stream>>>(q, r, q_n, r_n, L, probes, shift, nbins,
-                                                                      qcodes, start, order, ocode, qnorm, rnorm, thr,
-                                                                      ratio, dist_scale, matches, counts, nn_idx,
-                                                                      nn_dist);
+    const long long blocks = (static_cast<long long>(q_n) * 32 + kScanThreads - 1) / kScanThreads;
+    lsh_scan_kernel<<<static_cast<unsigned>(blocks), kScanThreads, 0, stream>>>(
+        q, r, q_n, r_n, L, probes, shift, nbins, qcodes, start, order, ocode, thr, ratio, dist_scale, matches, counts,
+        nn_idx, nn_dist);
     return cudaGetLastError();
 }
 

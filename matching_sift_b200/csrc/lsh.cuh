@@ -35,8 +35,7 @@ cudaError_t launch_lsh_buckets(const uint32_t* codes, int n, int L, int shift, i
 // inputs scaled by 2^-s). counts (optional): candidates compared per query.
 cudaError_t launch_lsh_scan(const uint8_t* q, const uint8_t* r, int q_n, int r_n, int L, int probes, int shift,
                             int nbins, const uint32_t* qcodes, const int* start, const int* order,
-                            const uint32_t* ocode, const int32_t* qnorm, const int32_t* rnorm, float thr, int ratio,
-                            float dist_scale, uint32_t* matches, uint32_t* counts, int32_t* nn_idx, float* nn_dist,
-                            cudaStream_t stream);
+                            const uint32_t* ocode, float thr, int ratio, float dist_scale, uint32_t* matches,
+                            uint32_t* counts, int32_t* nn_idx, float* nn_dist, cudaStream_t stream);
 
 }  // namespace sift

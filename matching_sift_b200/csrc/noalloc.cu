@@ -20,7 +20,13 @@
 //     serialise them (one stream, or events);
 //   * the first call on a device resolves the array's device address with
 //     cudaGetSymbolAddress (with that device current); make that first call
-//     before any stream capture.
+//     before any stream capture;
+//   * a bounded wait that expires inside a call's search kernel (an error no
+//     correct run produces) leaves that call's outputs marked "no result"
+//     (UINT32_MAX, -1, FLT_MAX) rather than half written, and is reported by
+//     sift2nn_noalloc_status, which reads a word in the same array (no
+//     allocation there either).
+#include <cfloat>
 #include <climits>
 #include <cstdint>
 #include <functional>
@@ -28,10 +34,40 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include "sift2nn.h"
+#include "context.h"
 #include "exact2nn.cuh"
 
 namespace sift {
 namespace {
+
+// Layout of the array: [0] this call's device error word (cleared by every
+// call), [1] the sticky status word (set by any call whose search reported an
+// error, cleared by sift2nn_noalloc_status), then 256-byte aligned regions.
+constexpr size_t kNoAllocErrOff = 0;
+constexpr size_t kNoAllocStickyOff = sizeof(int);
+constexpr size_t kNoAllocHeader = 256;
+
+// After the merge: if this call's search reported an error, its partial lists
+// may be stale, so every output row is overwritten with "no result" and the
+// error is recorded in the sticky word.
+__global__ void noalloc_invalidate_kernel(const int* __restrict__ err, int* __restrict__ sticky, int q_n,
+                                          uint32_t* __restrict__ matches, int32_t* __restrict__ nn_idx,
+                                          float* __restrict__ nn_dist) {
+    const int code = *err;
+    if (code == 0) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) atomicCAS(sticky, 0, code);
+    if (i >= q_n) return;
+    if (matches) matches[i] = UINT32_MAX;
+    if (nn_idx) {
+        nn_idx[2 * i] = -1;
+        nn_idx[2 * i + 1] = -1;
+    }
+    if (nn_dist) {
+        nn_dist[2 * i] = FLT_MAX;
+        nn_dist[2 * i + 1] = FLT_MAX;
+    }
+}
 
 constexpr uint32_t kNoAllocMaxQueries = 16384;
 constexpr uint32_t kNoAllocMaxBase = 1u << 20;
@@ -104,14 +140,21 @@ extern "C" SIFT_API int sift2nn_match_noalloc(const uint8_t* q, const uint8_t* r
         cudaGetLastError();
         return SIFT_ERR_NO_DEVICE;
     }
+    // Inputs and outputs must be memory the GPU reads and writes directly: a
+    // host pointer would reach the tensor map or the kernel stores.
+    // (cudaPointerGetAttributes allocates nothing.)
+    using detail::is_device_accessible;
+    if (!is_device_accessible(q) || (r_n && !is_device_accessible(r)) ||
+        (matches && !is_device_accessible(matches)) || (nn_idx && !is_device_accessible(nn_idx)) ||
+        (nn_dist && !is_device_accessible(nn_dist)))
+        return SIFT_ERR_INVALID_ARG;
     NoAllocDevice& d = g_noalloc[dev];
     std::call_once(d.once, noalloc_setup, std::ref(d), dev);
     if (d.status != SIFT_OK) return d.status;
 
     const ExactPlan plan = make_exact_plan(static_cast<int>(q_n), static_cast<int>(r_n), d.num_sms / 2, 2);
-    size_t off = 0;
-    const size_t o_err = off;
-    off = align256(off + sizeof(int));
+    const size_t o_err = kNoAllocErrOff;
+    size_t off = kNoAllocHeader;
     const size_t o_rec = off;
     off = align256(off + static_cast<size_t>(plan.base_tiles) * kRecInts * 4 + 16);
     const size_t o_qnorm = off;
@@ -132,6 +175,7 @@ extern "C" SIFT_API int sift2nn_match_noalloc(const uint8_t* q, const uint8_t* r
     // The status word is the only scratch that must start at zero; every other
     // region is fully written by the kernels before it is read.
     if (cudaMemsetAsync(err, 0, sizeof(int), st) != cudaSuccess) return SIFT_ERR_CUDA;
+    if (detail::maybe_inject_wait_expiry(err, st) != cudaSuccess) return SIFT_ERR_CUDA;
     if (launch_row_norms_u8(r, static_cast<int>(r_n), plan.r_pad, kMetricL2, nullptr, rec, nullptr, st) != cudaSuccess ||
         launch_row_norms_u8(q, static_cast<int>(q_n), plan.q_pad, kMetricL2, qnorm, nullptr, thresh, st) != cudaSuccess)
         return SIFT_ERR_CUDA;
@@ -145,5 +189,35 @@ extern "C" SIFT_API int sift2nn_match_noalloc(const uint8_t* q, const uint8_t* r
     if (launch_merge2nn(partial, plan, qnorm, kMetricL2, threshold, 1.0f, matches, nullptr, nn_idx, nn_dist, st) !=
         cudaSuccess)
         return SIFT_ERR_CUDA;
+    noalloc_invalidate_kernel<<<(q_n + 255) / 256, 256, 0, st>>>(err, reinterpret_cast<int*>(S + kNoAllocStickyOff),
+                                                                 static_cast<int>(q_n), matches, nn_idx, nn_dist);
+    if (cudaGetLastError() != cudaSuccess) return SIFT_ERR_CUDA;
     return SIFT_OK;
+}
+
+// Synchronises `stream` and reports whether a search of sift2nn_match_noalloc
+// on the current device hit an expired bounded wait since the last check
+// (SIFT_ERR_DEVICE_TIMEOUT; SIFT_OK otherwise), clearing the record. Reads the
+// word through the array's device address: no allocation.
+extern "C" SIFT_API int sift2nn_noalloc_status(void* stream) {
+    using namespace sift;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+        cudaGetLastError();
+        return SIFT_ERR_NO_DEVICE;
+    }
+    NoAllocDevice& d = g_noalloc[dev];
+    std::call_once(d.once, noalloc_setup, std::ref(d), dev);
+    if (d.status != SIFT_OK) return d.status;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int* sticky = reinterpret_cast<int*>(d.scratch + kNoAllocStickyOff);
+    int word = 0;
+    if (cudaStreamSynchronize(st) != cudaSuccess ||
+        cudaMemcpyAsync(&word, sticky, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return SIFT_ERR_CUDA;
+    if (word == 0) return SIFT_OK;
+    if (cudaMemsetAsync(sticky, 0, sizeof(int), st) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess)
+        return SIFT_ERR_CUDA;
+    return SIFT_ERR_DEVICE_TIMEOUT;
 }

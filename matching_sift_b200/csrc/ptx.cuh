@@ -74,21 +74,25 @@ __device__ __forceinline__ bool mbar_try_wait_sleep(uint32_t bar, uint32_t parit
 
 // Waits until the phase with the given parity has completed. Returns false
 // (after recording `code` in *err and raising the CTA abort flag) when the
-// wait exceeds kWaitTimeoutNs or another thread has already aborted.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* err,
-                                          int code) {
+// wait exceeds limit_ns or another thread has already aborted.
+__device__ __forceinline__ bool mbar_wait_limit(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* err,
+                                                int code, uint64_t limit_ns) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = globaltimer();
     #pragma unroll 1
     while (true) {
         if (mbar_try_wait_sleep(bar, parity, 20000u)) return true;
         if (*abort_flag) return false;
-        if (globaltimer() - t0 > kWaitTimeoutNs) {
+        if (globaltimer() - t0 > limit_ns) {
             *abort_flag = 1;
             atomicCAS(err, 0, code);
             return false;
         }
     }
+}
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* err,
+                                          int code) {
+    return mbar_wait_limit(bar, parity, abort_flag, err, code, kWaitTimeoutNs);
 }
 
 // ----------------------------------------------------------------- TMA ---

@@ -27,7 +27,23 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _ORACLE_SO = os.path.join(_HERE, "liboracle.so")
 _REF_SO = os.path.join(_HERE, "_ref", "libref.so")
-REF_SRC = os.environ.get("SIFT_REFERENCE_DIR", "/root/reference")
+_CALLER = os.path.join(_HERE, "_ref", "reference_caller")
+
+
+def _reference_dir() -> str:
+    """Where the reference checkout lives: $SIFT_REFERENCE_DIR, else the path in
+    oracle/reference_dir.txt (configuration of the build machine), else ''."""
+    env = os.environ.get("SIFT_REFERENCE_DIR")
+    if env:
+        return env
+    cfg = os.path.join(_HERE, "reference_dir.txt")
+    if os.path.exists(cfg):
+        with open(cfg) as f:
+            return f.read().strip()
+    return ""
+
+
+REF_SRC = _reference_dir()
 
 _lib = None
 _ref = None
@@ -40,8 +56,14 @@ def build(force: bool = False) -> None:
     """Compile liboracle.so (gcc) and, when the reference sources exist, _ref/libref.so (nvcc)."""
     if force or not os.path.exists(_ORACLE_SO):
         subprocess.run(["make", "-s", "-C", _HERE, "oracle"], check=True)
-    if os.path.isdir(os.path.join(REF_SRC, "src")) and (force or not os.path.exists(_REF_SO)):
+    if REF_SRC and os.path.isdir(os.path.join(REF_SRC, "src")) and (
+            force or not os.path.exists(_REF_SO) or not os.path.exists(_CALLER)):
         subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={REF_SRC}"], check=True)
+
+
+def reference_caller() -> str:
+    """Path of the C++ program that calls the library through the reference's own headers ('' if not built)."""
+    return _CALLER if os.path.exists(_CALLER) else ""
 
 
 def lib():
