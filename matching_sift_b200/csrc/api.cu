@@ -129,11 +129,12 @@ int encode_bf16_2d(CUtensorMap* m, const void* base, uint64_t inner, uint64_t ro
     return r == CUDA_SUCCESS ? SIFT_OK : SIFT_ERR_CUDA;
 }
 
-// FP16 rows of 128 halves (256 B): dims {128, rows}, box {64, box_rows} (one
-// 128-byte K block per load, the widest SWIZZLE_128B box).
-int encode_f16_rows(CUtensorMap* m, const void* base, uint64_t rows, uint32_t box_rows) {
-    cuuint64_t dims[2] = {static_cast<cuuint64_t>(kDim), static_cast<cuuint64_t>(rows)};
-    cuuint64_t strides[1] = {static_cast<cuuint64_t>(kDim) * 2};
+// FP16 rows of `width` halves (128, or 256 for split [hi | lo] rows): dims
+// {width, rows}, box {64, box_rows} (one 128-byte K block per load, the widest
+// SWIZZLE_128B box).
+int encode_f16_rows(CUtensorMap* m, const void* base, uint64_t rows, uint32_t box_rows, uint64_t width = kDim) {
+    cuuint64_t dims[2] = {static_cast<cuuint64_t>(width), static_cast<cuuint64_t>(rows)};
+    cuuint64_t strides[1] = {static_cast<cuuint64_t>(width) * 2};
     cuuint32_t box[2] = {static_cast<cuuint32_t>(kDim / 2), box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
@@ -406,6 +407,121 @@ int exact_match_chunked(const MatchArgs& a, DeviceCtx& c, cudaStream_t st) {
     return collect_device_status(c, st);
 }
 
+// General float / half descriptors (values that are not integers times one
+// power of two, e.g. the unit-normalised rand() vectors of the reference
+// benchmark, src/helper.cu:40-58): searched on the tensor cores with f32
+// accumulation and float keys. Half rows are read in place (exact products);
+// float rows are first split into FP16 hi + lo parts after scaling by a power
+// of two 2^e that puts the largest |value| in [2^14, 2^15), and the dot
+// product is hi.hi' + hi.lo' + lo.hi' (22 significant bits per value, the
+// f32 accumulation of the tensor cores). Norms are f32 sums of the scaled
+// values. Distances come back in the caller's units (x 2^-2e). Caller holds
+// the arena lock.
+int exact_match_float(const MatchArgs& a, DeviceCtx& c, cudaStream_t st) {
+    const int q_n = static_cast<int>(a.q_n), r_n = static_cast<int>(a.r_n);
+    const bool half = a.type == SIFT_HALF_DEVICE;
+    const bool host_in = a.type == SIFT_FLOAT_HOST;
+    const bool has_lo = !half;
+    constexpr int kGroupTiles = 2;  // query groups of 256 rows (one 128-row tile per CTA of a pair)
+    const ExactPlan plan = make_exact_plan(q_n, r_n, c.num_sms / 2, 2, kGroupTiles);
+    if (!host_in && ((reinterpret_cast<uintptr_t>(a.q) & 15) || (r_n && (reinterpret_cast<uintptr_t>(a.r) & 15))))
+        return SIFT_ERR_INVALID_ARG;
+    const bool m_dev = !a.matches || is_device_accessible(a.matches);
+    const bool s_dev = !a.sorted || is_device_accessible(a.sorted);
+    const bool i_dev = !a.nn_idx || is_device_accessible(a.nn_idx);
+    const bool d_dev = !a.nn_dist || is_device_accessible(a.nn_dist);
+    const bool host_out = !(m_dev && s_dev && i_dev && d_dev);
+
+    Layout L;
+    const size_t o_qf = host_in ? L.take(static_cast<size_t>(q_n) * kDim * 4) : 0;
+    const size_t o_rf = host_in ? L.take(static_cast<size_t>(r_n) * kDim * 4 + 16) : 0;
+    const size_t o_qs = has_lo ? L.take(static_cast<size_t>(q_n) * 512) : 0;
+    const size_t o_rs = has_lo ? L.take(static_cast<size_t>(r_n) * 512 + 16) : 0;
+    const size_t o_brec = L.take(static_cast<size_t>(plan.base_tiles) * kRecInts * 4 + 16);
+    const size_t o_qnorm = L.take(static_cast<size_t>(plan.q_pad) * 4);
+    const size_t o_thr = L.take(static_cast<size_t>(plan.q_pad) * 4);
+    const size_t o_part = L.take(static_cast<size_t>(plan.max_splits) * plan.parts * plan.q_pad * sizeof(int4));
+    const size_t o_m = (a.matches && !m_dev) ? L.take(static_cast<size_t>(q_n) * 4) : 0;
+    const size_t o_s = (a.sorted && !s_dev) ? L.take(static_cast<size_t>(q_n) * 16) : 0;
+    const size_t o_i = (a.nn_idx && !i_dev) ? L.take(static_cast<size_t>(q_n) * 8) : 0;
+    const size_t o_d = (a.nn_dist && !d_dev) ? L.take(static_cast<size_t>(q_n) * 8) : 0;
+    SIFT_TRY(ensure_arena(c, L.off));
+    char* A = c.arena;
+
+    const void* q_src = a.q;
+    const void* r_src = a.r;
+    if (host_in) {
+        SIFT_CUDA(cudaMemcpyAsync(A + o_qf, a.q, static_cast<size_t>(q_n) * kDim * 4, cudaMemcpyHostToDevice, st));
+        if (r_n)
+            SIFT_CUDA(cudaMemcpyAsync(A + o_rf, a.r, static_cast<size_t>(r_n) * kDim * 4, cudaMemcpyHostToDevice, st));
+        q_src = A + o_qf;
+        r_src = A + o_rf;
+    }
+    // Largest |value| of both sets (and a finiteness check) for the scale.
+    SIFT_CUDA(cudaMemsetAsync(c.d_status + 1, 0, 2 * sizeof(int), st));
+    SIFT_CUDA(launch_abs_stats(q_src, half, q_n, c.d_status + 1, c.num_sms, st));
+    SIFT_CUDA(launch_abs_stats(r_src, half, r_n, c.d_status + 1, c.num_sms, st));
+    SIFT_CUDA(cudaMemcpyAsync(c.h_status + 1, c.d_status + 1, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    SIFT_CUDA(cudaStreamSynchronize(st));
+    if (c.h_status[1] != 0) return SIFT_ERR_INVALID_ARG;  // infinite or NaN values
+    float mx = 0.0f;
+    std::memcpy(&mx, &c.h_status[2], sizeof(float));
+    int e = 0;
+    if (has_lo && mx > 0.0f) {
+        int ex = 0;
+        std::frexp(mx, &ex);  // mx in [2^(ex-1), 2^ex)
+        e = 15 - ex;          // mx * 2^e in [2^14, 2^15)
+    }
+    const float mul = ldexpf(1.0f, e);
+    g_launches += (r_n > 0 ? 2 : 1);
+
+    const void* q_rows = q_src;
+    const void* r_rows = r_src;
+    if (has_lo) {
+        SIFT_CUDA(launch_pack_split_f16(static_cast<const float*>(q_src), q_n, mul, A + o_qs, c.num_sms, st));
+        SIFT_CUDA(launch_pack_split_f16(static_cast<const float*>(r_src), r_n, mul, A + o_rs, c.num_sms, st));
+        q_rows = A + o_qs;
+        r_rows = A + o_rs;
+        g_launches += (r_n > 0 ? 2 : 1);
+    }
+    int32_t* brec = reinterpret_cast<int32_t*>(A + o_brec);
+    int32_t* qnorm = reinterpret_cast<int32_t*>(A + o_qnorm);
+    int32_t* thresh = reinterpret_cast<int32_t*>(A + o_thr);
+    SIFT_CUDA(launch_row_norms_float(r_src, half, r_n, plan.r_pad, mul, a.metric, nullptr, brec, nullptr, st));
+    SIFT_CUDA(launch_row_norms_float(q_src, half, q_n, plan.q_pad, mul, kMetricL2, qnorm, nullptr, thresh, st));
+    g_launches += (plan.r_pad > 0 ? 1 : 0) + 1;
+    int4* partial = reinterpret_cast<int4*>(A + o_part);
+    if (r_n > 0) {
+        const uint64_t width = has_lo ? 2 * kDim : kDim;
+        CUtensorMap qmap, bmap;
+        SIFT_TRY(encode_f16_rows(&qmap, q_rows, q_n, kBM, width));
+        SIFT_TRY(encode_f16_rows(&bmap, r_rows, r_n, kBN / 2, width));
+        SIFT_CUDA(maybe_inject_wait_expiry(c.d_status, st));
+        SIFT_CUDA(launch_exact2nn_float_pair(qmap, bmap, brec, plan, partial, thresh, c.d_status, has_lo, st));
+        ++g_launches;
+    }
+    uint32_t* m_out = (a.matches && !m_dev) ? reinterpret_cast<uint32_t*>(A + o_m) : a.matches;
+    float4* s_out = (a.sorted && !s_dev) ? reinterpret_cast<float4*>(A + o_s) : reinterpret_cast<float4*>(a.sorted);
+    int32_t* i_out = (a.nn_idx && !i_dev) ? reinterpret_cast<int32_t*>(A + o_i) : a.nn_idx;
+    float* d_out = (a.nn_dist && !d_dev) ? reinterpret_cast<float*>(A + o_d) : a.nn_dist;
+    SIFT_CUDA(launch_merge2nn_float(partial, plan, kGroupTiles * kBM, qnorm, a.metric, a.threshold,
+                                    ldexpf(1.0f, -2 * e), m_out, s_out, i_out, d_out, st));
+    ++g_launches;
+    if (a.matches && !m_dev)
+        SIFT_CUDA(cudaMemcpyAsync(a.matches, m_out, static_cast<size_t>(q_n) * 4, cudaMemcpyDeviceToHost, st));
+    if (a.sorted && !s_dev)
+        SIFT_CUDA(cudaMemcpyAsync(a.sorted, s_out, static_cast<size_t>(q_n) * 16, cudaMemcpyDeviceToHost, st));
+    if (a.nn_idx && !i_dev)
+        SIFT_CUDA(cudaMemcpyAsync(a.nn_idx, i_out, static_cast<size_t>(q_n) * 8, cudaMemcpyDeviceToHost, st));
+    if (a.nn_dist && !d_dev)
+        SIFT_CUDA(cudaMemcpyAsync(a.nn_dist, d_out, static_cast<size_t>(q_n) * 8, cudaMemcpyDeviceToHost, st));
+    if (a.sync || host_out || host_in) {
+        SIFT_CUDA(cudaStreamSynchronize(st));
+        return collect_device_status(c, st);
+    }
+    return SIFT_OK;
+}
+
 // Core of every exact entry point.
 int exact_match(const MatchArgs& a) {
     if (a.q_n > 0 && !a.q) return SIFT_ERR_INVALID_ARG;
@@ -455,11 +571,18 @@ int exact_match(const MatchArgs& a) {
     const uint8_t* qd = nullptr;
     const uint8_t* rd = nullptr;
     int shift = 0;
+    // Values that are not integers times one power of two take the general
+    // float path (float keys on the FP16 tensor cores).
     if (use_f16) {
-        SIFT_TRY(common_shift(c, a.q, a.r, true, q_n, r_n, st, shift));
+        const int rc = common_shift(c, a.q, a.r, true, q_n, r_n, st, shift);
         g_launches += r_n > 0 ? 2 : 1;
+        if (rc == SIFT_ERR_NOT_INTEGER) return exact_match_float(a, c, st);
+        SIFT_TRY(rc);
     } else {
-        SIFT_TRY(stage_inputs(c, A, ip, a.type, a.q, a.r, q_n, r_n, st, qd, rd, shift));
+        const int rc = stage_inputs(c, A, ip, a.type, a.q, a.r, q_n, r_n, st, qd, rd, shift);
+        if (rc == SIFT_ERR_NOT_INTEGER && a.type != SIFT_U8_DEVICE && a.type != SIFT_U8_HOST)
+            return exact_match_float(a, c, st);
+        SIFT_TRY(rc);
     }
 
     // ---- norms

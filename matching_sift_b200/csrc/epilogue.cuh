@@ -95,5 +95,55 @@ __device__ __forceinline__ void scan_group(const uint32_t (&v)[32], int row0, co
     }
 }
 
+// The same pruned scan for general float rows: v[c] = q.b(row0 + c) as f32
+// accumulators (any sign), nrm / gm8 the record's float norms and 8-row
+// minima (bit patterns). Keys are fma(-2, q.b, |b|^2) mapped by float_key;
+// the bound of a subgroup fma(-2, max q.b, min |b|^2) is computed with the same
+// single rounding, and rounding to nearest is monotone, so the bound never
+// exceeds a computed key of its rows: pruning drops no candidate.
+__device__ __forceinline__ void scan_group_float(const uint32_t (&v)[32], int row0, const int32_t* nrm,
+                                                 const int32_t* gm8, Top2& s) {
+    float mx[4];
+    #pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        float m = __uint_as_float(v[8 * k]);
+        #pragma unroll
+        for (int e = 1; e < 8; ++e) m = fmaxf(m, __uint_as_float(v[8 * k + e]));
+        mx[k] = m;
+    }
+    const int4 g8 = *reinterpret_cast<const int4*>(gm8);
+    const int bnd[4] = {float_key(fmaf(-2.0f, mx[0], __int_as_float(g8.x))),
+                        float_key(fmaf(-2.0f, mx[1], __int_as_float(g8.y))),
+                        float_key(fmaf(-2.0f, mx[2], __int_as_float(g8.z))),
+                        float_key(fmaf(-2.0f, mx[3], __int_as_float(g8.w)))};
+    const int bmin = min(__vimin3_s32(bnd[0], bnd[1], bnd[2]), bnd[3]);
+    if (__any_sync(0xffffffffu, bmin <= s.thr)) {
+        #pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const bool ps = bnd[k] <= s.thr;
+            if (__any_sync(0xffffffffu, ps)) {
+                if (ps) {
+                    const int4 na = *reinterpret_cast<const int4*>(nrm + 8 * k);
+                    const int4 nb = *reinterpret_cast<const int4*>(nrm + 8 * k + 4);
+                    const int nr[8] = {na.x, na.y, na.z, na.w, nb.x, nb.y, nb.z, nb.w};
+                    int key[8];
+                    #pragma unroll
+                    for (int e = 0; e < 8; ++e)
+                        key[e] = float_key(fmaf(-2.0f, __uint_as_float(v[8 * k + e]), __int_as_float(nr[e])));
+                    int mk = __vimin3_s32(key[0], key[1], key[2]);
+                    mk = __vimin3_s32(mk, key[3], key[4]);
+                    mk = __vimin3_s32(mk, key[5], key[6]);
+                    mk = min(mk, key[7]);
+                    if (mk <= s.thr) {
+                        const int base = row0 + 8 * k;
+                        #pragma unroll
+                        for (int e = 0; e < 8; ++e) top2_update(s, key[e], base + e);
+                    }
+                }
+            }
+        }
+    }
+}
+
 }  // namespace
 }  // namespace sift

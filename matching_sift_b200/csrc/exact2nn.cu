@@ -130,6 +130,73 @@ __global__ void __launch_bounds__(256) row_norms_kernel(const T* __restrict__ x,
     }
 }
 
+// 16 consecutive elements of a row, times mul, as floats.
+__device__ __forceinline__ void load16_f32(const float* x, int row, int sub, float mul, float (&f)[16]) {
+    const float4* p = reinterpret_cast<const float4*>(x + static_cast<size_t>(row) * kDim) + 4 * sub;
+    #pragma unroll
+    for (int h = 0; h < 4; ++h) {
+        const float4 v = p[h];
+        f[4 * h] = v.x * mul;
+        f[4 * h + 1] = v.y * mul;
+        f[4 * h + 2] = v.z * mul;
+        f[4 * h + 3] = v.w * mul;
+    }
+}
+__device__ __forceinline__ void load16_f32(const __half* x, int row, int sub, float mul, float (&f)[16]) {
+    const uint4* p = reinterpret_cast<const uint4*>(x + static_cast<size_t>(row) * kDim) + 2 * sub;
+    #pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const uint4 v = p[h];
+        const __half2* hv = reinterpret_cast<const __half2*>(&v);
+        #pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float2 a = __half22float2(hv[k]);
+            f[8 * h + 2 * k] = a.x * mul;
+            f[8 * h + 2 * k + 1] = a.y * mul;
+        }
+    }
+}
+
+// Squared norms of general (non-integer) float / half rows times mul, in FP32,
+// stored as float bit patterns in the int32 slots of the integer path (norm,
+// record norms and 8-row minima); padding rows get kFloatKeyPad. thresh is set
+// to INT_MAX (the largest ordered key, see float_key).
+template <typename T>
+__global__ void __launch_bounds__(256) row_norms_float_kernel(const T* __restrict__ x, int n, int n_pad, float mul,
+                                                              int metric, int32_t* __restrict__ norm,
+                                                              int32_t* __restrict__ rec,
+                                                              int32_t* __restrict__ thresh) {
+    const int row = blockIdx.x * 32 + (threadIdx.x >> 3);
+    const int sub = threadIdx.x & 7;
+    float s = 0.0f;
+    if (row < n) {
+        float f[16];
+        load16_f32(x, row, sub, mul, f);
+        #pragma unroll
+        for (int i = 0; i < 16; ++i) s = fmaf(f[i], f[i], s);
+    }
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    s += __shfl_xor_sync(0xffffffffu, s, 4);
+    const float v = row < n ? (metric == kMetricL2 ? s : 0.0f) : kFloatKeyPad;
+    __shared__ float nrm[32];
+    int32_t* r = rec ? rec + static_cast<size_t>(blockIdx.x / 4) * kRecInts : nullptr;
+    const int part = blockIdx.x & 3;
+    if (sub == 0) {
+        nrm[threadIdx.x >> 3] = v;
+        if (norm) norm[row] = __float_as_int(v);
+        if (r) r[part * 32 + (threadIdx.x >> 3)] = __float_as_int(v);
+        if (thresh) thresh[row] = INT_MAX;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4 && r) {
+        float m = nrm[8 * threadIdx.x];
+        #pragma unroll
+        for (int i = 1; i < 8; ++i) m = fminf(m, nrm[8 * threadIdx.x + i]);
+        r[128 + part * 4 + threadIdx.x] = __float_as_int(m);
+    }
+}
+
 // Largest k with key(items[k]) <= v over a non-decreasing key; empty
 // problems share the key of the problem after them, so the match is the
 // problem that owns v.
@@ -409,6 +476,9 @@ __device__ __forceinline__ bool lex_less(int ka, int ia, int kb, int ib) {
     return ka < kb || (ka == kb && ia < ib);
 }
 
+// FLOATKEY: the keys are ordered images of float keys (float_key) and the
+// query norms float bit patterns (the general float path); else integers.
+template <bool FLOATKEY>
 __global__ void __launch_bounds__(256) merge2nn_kernel(const int4* __restrict__ partial, const ExactPlan plan,
                                                        const WorkItem* __restrict__ items, int n_items,
                                                        const WorkItem single, int group_rows, int total_q,
@@ -444,11 +514,24 @@ __global__ void __launch_bounds__(256) merge2nn_kernel(const int4* __restrict__ 
     }
     // Rows past the problem's base set are padding (they may hold another
     // problem's rows, but only enter a top-2 when fewer real rows exist).
-    const bool v1 = j1 >= 0 && j1 < it.n_b && a1 < kKeyPad;
-    const bool v2 = j2 >= 0 && j2 < it.n_b && a2 < kKeyPad;
-    const int qn = metric == kMetricL2 ? qnorm[q] : 0;
-    const float d1 = v1 ? static_cast<float>(a1 + qn) * dscale : FLT_MAX;
-    const float d2 = v2 ? static_cast<float>(a2 + qn) * dscale : FLT_MAX;
+    bool v1, v2;
+    float d1, d2;
+    if constexpr (FLOATKEY) {
+        // Squared distances |b|^2 - 2 q.b + |q|^2 can round a little below
+        // zero for (near-)identical rows: clamped at 0.
+        v1 = j1 >= 0 && j1 < it.n_b;
+        v2 = j2 >= 0 && j2 < it.n_b;
+        const float qn = metric == kMetricL2 ? __int_as_float(qnorm[q]) : 0.0f;
+        const float lo = metric == kMetricL2 ? 0.0f : -FLT_MAX;
+        d1 = v1 ? fmaxf((key_float(a1) + qn) * dscale, lo) : FLT_MAX;
+        d2 = v2 ? fmaxf((key_float(a2) + qn) * dscale, lo) : FLT_MAX;
+    } else {
+        v1 = j1 >= 0 && j1 < it.n_b && a1 < kKeyPad;
+        v2 = j2 >= 0 && j2 < it.n_b && a2 < kKeyPad;
+        const int qn = metric == kMetricL2 ? qnorm[q] : 0;
+        d1 = v1 ? static_cast<float>(a1 + qn) * dscale : FLT_MAX;
+        d2 = v2 ? static_cast<float>(a2 + qn) * dscale : FLT_MAX;
+    }
     if (matches) {
         bool pass = false;
         if (v1) {
@@ -545,13 +628,13 @@ cudaError_t launch_merge2nn_chunks(const int4* partial, const ChunkSet& cs, int 
     return cudaGetLastError();
 }
 
-ExactPlan make_exact_plan(int q_n, int r_n, int num_sms, int parts) {
+ExactPlan make_exact_plan(int q_n, int r_n, int num_sms, int parts, int group_tiles) {
     ExactPlan p{};
     p.parts = parts;
     p.q_n = q_n;
     p.r_n = r_n;
     p.q_tiles = (q_n + kBM - 1) / kBM;
-    p.q_groups = (p.q_tiles + kQT - 1) / kQT;
+    p.q_groups = (p.q_tiles + group_tiles - 1) / group_tiles;
     p.q_pad = p.q_tiles * kBM;
     p.base_tiles = (r_n + kBN - 1) / kBN;
     p.r_pad = p.base_tiles * kBN;
@@ -587,6 +670,18 @@ cudaError_t launch_row_norms_f16(const void* x, int n, int n_pad, float mul, int
     return cudaGetLastError();
 }
 
+cudaError_t launch_row_norms_float(const void* x, bool half, int n, int n_pad, float mul, int metric, int32_t* norm,
+                                   int32_t* rec, int32_t* thresh, cudaStream_t stream) {
+    if (n_pad <= 0) return cudaSuccess;
+    if (half)
+        row_norms_float_kernel<__half><<<n_pad / 32, 256, 0, stream>>>(static_cast<const __half*>(x), n, n_pad, mul,
+                                                                       metric, norm, rec, thresh);
+    else
+        row_norms_float_kernel<float><<<n_pad / 32, 256, 0, stream>>>(static_cast<const float*>(x), n, n_pad, mul,
+                                                                      metric, norm, rec, thresh);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_exact2nn_u8(const CUtensorMap& qmap, const CUtensorMap& bmap, const int32_t* brec,
                                const ExactPlan& plan, int4* partial, int32_t* thresh, int* err, cudaStream_t stream) {
     // The shared-memory opt-in is per device; the host API serialises calls per device.
@@ -614,9 +709,24 @@ cudaError_t launch_merge2nn(const int4* partial, const ExactPlan& plan, const in
     single.n_b = plan.r_n;
     single.groups = plan.q_groups;
     single.tiles = plan.base_tiles;
-    merge2nn_kernel<<<(plan.q_n + 255) / 256, 256, 0, stream>>>(partial, plan, nullptr, 1, single, kQT * kBM, plan.q_n,
-                                                               qnorm, metric, threshold, dist_scale, matches, sorted,
-                                                               nn_idx, nn_dist);
+    merge2nn_kernel<false><<<(plan.q_n + 255) / 256, 256, 0, stream>>>(partial, plan, nullptr, 1, single, kQT * kBM,
+                                                                      plan.q_n, qnorm, metric, threshold, dist_scale,
+                                                                      matches, sorted, nn_idx, nn_dist);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_merge2nn_float(const int4* partial, const ExactPlan& plan, int group_rows, const int32_t* qnorm,
+                                  int metric, float threshold, float dist_scale, uint32_t* matches, float4* sorted,
+                                  int32_t* nn_idx, float* nn_dist, cudaStream_t stream) {
+    if (plan.q_n <= 0) return cudaSuccess;
+    WorkItem single{};
+    single.n_a = plan.q_n;
+    single.n_b = plan.r_n;
+    single.groups = plan.q_groups;
+    single.tiles = plan.base_tiles;
+    merge2nn_kernel<true><<<(plan.q_n + 255) / 256, 256, 0, stream>>>(partial, plan, nullptr, 1, single, group_rows,
+                                                                     plan.q_n, qnorm, metric, threshold, dist_scale,
+                                                                     matches, sorted, nn_idx, nn_dist);
     return cudaGetLastError();
 }
 
@@ -624,7 +734,7 @@ cudaError_t launch_merge2nn_batch(const int4* partial, const BatchPlan& bp, int 
                                   int metric, float threshold, float dist_scale, uint32_t* matches, float4* sorted,
                                   int32_t* nn_idx, float* nn_dist, cudaStream_t stream) {
     if (total_queries <= 0) return cudaSuccess;
-    merge2nn_kernel<<<(total_queries + 255) / 256, 256, 0, stream>>>(
+    merge2nn_kernel<false><<<(total_queries + 255) / 256, 256, 0, stream>>>(
         partial, bp.plan, bp.items, bp.n_items, WorkItem{}, bp.group_rows, total_queries, qnorm, metric, threshold,
         dist_scale, matches, sorted, nn_idx, nn_dist);
     return cudaGetLastError();

@@ -97,7 +97,38 @@ ExactPlan make_batch_plan(const WorkItem* items, int n_items, long long units, i
 
 // num_workers: persistent CTAs (or CTA pairs); parts: partial top-2 lists
 // each worker writes per query (one per disjoint column slice it scans).
-ExactPlan make_exact_plan(int q_n, int r_n, int num_workers, int parts);
+// group_tiles: 128-row query tiles per query group (kQT: groups of 512 rows
+// for the u8 / FP16 kernels; 2: groups of 256 for the general-float kernel).
+ExactPlan make_exact_plan(int q_n, int r_n, int num_workers, int parts, int group_tiles = kQT);
+
+// ---- general (non-integer) float / half descriptors
+// Keys of the float path are floats mapped to int32 so that signed integer
+// order is float order (the integer top-2, shared bounds and merge machinery
+// then apply unchanged): non-negative floats keep their bit pattern, negative
+// ones have their magnitude bits flipped. -0.0 is folded into +0.0.
+__device__ __forceinline__ int32_t float_key(float x) {
+    const int32_t i = __float_as_int(x + 0.0f);
+    return i >= 0 ? i : (i ^ 0x7fffffff);
+}
+__device__ __forceinline__ float key_float(int32_t k) { return __int_as_float(k >= 0 ? k : (k ^ 0x7fffffff)); }
+constexpr float kFloatKeyPad = 3.0e38f;  // norm of padding rows (never a real key)
+
+// Squared norms (float bit patterns) of n float or half rows times mul, laid
+// out as launch_row_norms_u8's outputs (norm / rec / thresh, each optional).
+cudaError_t launch_row_norms_float(const void* x, bool half, int n, int n_pad, float mul, int metric, int32_t* norm,
+                                   int32_t* rec, int32_t* thresh, cudaStream_t stream);
+// The CTA-pair search on FP16 rows with float keys: query and base rows are
+// [hi | lo] split rows of 256 halves (qmap / bmap_half: dims {256, rows}, box
+// {64, 128 / 64}) when has_lo, else plain FP16 rows of 128 halves (the lo
+// products are skipped). dot = hi.hi' + hi.lo' + lo.hi' in f32 (kind::f16).
+// Query groups of 256 rows (plan made with group_tiles = 2).
+cudaError_t launch_exact2nn_float_pair(const CUtensorMap& qmap, const CUtensorMap& bmap_half, const int32_t* brec,
+                                       const ExactPlan& plan, int4* partial, int32_t* thresh, int* err, bool has_lo,
+                                       cudaStream_t stream);
+// Merge of the float path (float keys, float query norms); group_rows = 256.
+cudaError_t launch_merge2nn_float(const int4* partial, const ExactPlan& plan, int group_rows, const int32_t* qnorm,
+                                  int metric, float threshold, float dist_scale, uint32_t* matches, float4* sorted,
+                                  int32_t* nn_idx, float* nn_dist, cudaStream_t stream);
 
 // Per-row squared norms of u8 descriptors (or zeros for kMetricDot), padded
 // to n_pad rows (a multiple of kBN) with kKeyPad. Outputs (each optional):

@@ -91,13 +91,22 @@ constexpr int kPRecBytes = kRecInts * 4;         // 640 B
 constexpr uint16_t kPairMask = 0x3;
 constexpr size_t kPSmemBudget = 225 * 1024;
 
+// Element formats of the instantiations.
+enum PairMode : int {
+    kModeU8 = 0,     // u8 rows, kind::i8, integer keys
+    kModeF16Int = 1, // FP16 rows holding integers x 2^-s, kind::f16, integer keys
+    kModeFloat = 2,  // split FP16 rows [hi | lo] (or plain FP16 rows), kind::f16, float keys
+};
+
 // Shapes of one instantiation. A row of 128 elements is kKBlocks blocks of
-// 128 bytes; each block of a tile is stored as its own SW128 K-major tile
-// (rows x 128 B), and every MMA consumes 32 bytes of K.
-template <bool F16, int QPT, int QB>
+// 128 bytes (split rows: 2 hi blocks then 2 lo blocks); each block of a tile
+// is stored as its own SW128 K-major tile (rows x 128 B), and every MMA
+// consumes 32 bytes of K.
+template <int MODE, int QPT, int QB>
 struct PairCfg {
+    static constexpr bool F16 = MODE != kModeU8;
     static constexpr int kElemBytes = F16 ? 2 : 1;
-    static constexpr int kKBlocks = F16 ? 2 : 1;
+    static constexpr int kKBlocks = MODE == kModeU8 ? 1 : (MODE == kModeFloat ? 4 : 2);
     static constexpr int kBoxElems = 128 / kElemBytes;       // TMA box width of one K block
     static constexpr int kQKBlock = kBM * 128;               // bytes of one K block of a query tile
     static constexpr int kBKBlock = kPHalf * 128;            // bytes of one K block of a base half
@@ -182,13 +191,18 @@ struct Cursor {
     }
 };
 
-template <bool F16, int QPT, int QB>
+// has_lo (kModeFloat only): the rows carry lo blocks (split float rows); when
+// false they are plain FP16 rows and only the hi.hi products are formed.
+template <int MODE, int QPT, int QB>
 __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtensorMap& bmap,
                                           const int32_t* __restrict__ brec, const ExactPlan& plan,
                                           const WorkItem* __restrict__ items, int n_items, const WorkItem& single,
                                           int4* __restrict__ partial, int32_t* __restrict__ thresh,
-                                          int* __restrict__ err, float dscale) {
-    using Cfg = PairCfg<F16, QPT, QB>;
+                                          int* __restrict__ err, float dscale, bool has_lo = false) {
+    using Cfg = PairCfg<MODE, QPT, QB>;
+    constexpr bool F16 = Cfg::F16;
+    // K blocks actually loaded per row (split rows without lo parts: the hi blocks only).
+    const int kb_load = (MODE == kModeFloat && !has_lo) ? 2 : Cfg::kKBlocks;
     constexpr int kPStages = Cfg::kStages;
     constexpr int kPQTileBytes = Cfg::kQTileBytes;
     constexpr int kPBHalfBytes = Cfg::kBHalfBytes;
@@ -275,25 +289,28 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                     if (ngroups >= QB && !ptx::mbar_wait_cluster(bar_qempty + 8 * qb, ((ngroups / QB) - 1) & 1,
                                                                  abort_flag, err, kErrWaitQuery))
                         break;
-                    if (leader) ptx::mbar_arrive_expect_tx(bar_qfull + 8 * qb, 2 * Cfg::kQBufBytes);
+                    if (leader) ptx::mbar_arrive_expect_tx(bar_qfull + 8 * qb, 2 * QPT * kb_load * Cfg::kQKBlock);
                     for (int t = 0; t < QPT; ++t) {
                         const int row = cur.it.a_off + ((cur.g * QPT + t) * 2 + static_cast<int>(rank)) * kBM;
                         #pragma unroll
                         for (int kb = 0; kb < Cfg::kKBlocks; ++kb)
-                            ptx::tma_load_2d_pair(q_s + qb * Cfg::kQBufBytes + t * kPQTileBytes + kb * Cfg::kQKBlock,
-                                                  &qmap, kb * Cfg::kBoxElems, row, lead_qfull + 8 * qb);
+                            if (kb < kb_load)
+                                ptx::tma_load_2d_pair(
+                                    q_s + qb * Cfg::kQBufBytes + t * kPQTileBytes + kb * Cfg::kQKBlock, &qmap,
+                                    kb * Cfg::kBoxElems, row, lead_qfull + 8 * qb);
                     }
                     ++ngroups;
                 }
                 const int s = n % kPStages;
                 if (!ptx::mbar_wait(bar_sfree + 8 * s, ((n / kPStages) & 1) ^ 1, abort_flag, err, kErrWaitProducer))
                     break;
-                if (leader) ptx::mbar_arrive_expect_tx(bar_full + 8 * s, 2 * kPBHalfBytes);
+                if (leader) ptx::mbar_arrive_expect_tx(bar_full + 8 * s, 2 * kb_load * Cfg::kBKBlock);
                 const int brow = cur.it.b_off + cur.j * kBN + static_cast<int>(rank) * kPHalf;
                 #pragma unroll
                 for (int kb = 0; kb < Cfg::kKBlocks; ++kb)
-                    ptx::tma_load_2d_pair(b_s + s * kPBHalfBytes + kb * Cfg::kBKBlock, &bmap, kb * Cfg::kBoxElems,
-                                          brow, lead_full + 8 * s);
+                    if (kb < kb_load)
+                        ptx::tma_load_2d_pair(b_s + s * kPBHalfBytes + kb * Cfg::kBKBlock, &bmap, kb * Cfg::kBoxElems,
+                                              brow, lead_full + 8 * s);
                 ptx::mbar_arrive_expect_tx(bar_rfull + 8 * s, kPRecBytes);
                 ptx::bulk_load(r_s + s * kPRecBytes, brec + static_cast<size_t>(cur.it.rec_off + cur.j) * kRecInts,
                                kPRecBytes, bar_rfull + 8 * s);
@@ -317,6 +334,8 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
             // buffer mt); both walk every unit to follow the query groups.
             const int mt = warp == 1 ? 0 : 1;
             constexpr uint32_t idesc = Cfg::kIdesc;
+            constexpr int kMaxProd = MODE == kModeFloat ? 6 : Cfg::kKBlocks;
+            const int n_prod = MODE == kModeFloat ? (has_lo ? 6 : 2) : Cfg::kKBlocks;
             const uint64_t b_desc0 = ptx::sdesc_sw128(b_s);
             int ngroups = 0;
             bool new_group = true;
@@ -352,14 +371,20 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                         }
                         ptx::tc_fence_after();
                         const uint32_t d = tmem + (t * 2 + mt) * kBN;
+                        // K-block products: (kb, kb) for every block of the row;
+                        // split float rows: hi.hi for both K halves, then (with lo
+                        // parts) hi.lo' and lo.hi'.
                         #pragma unroll
-                        for (int kb = 0; kb < Cfg::kKBlocks; ++kb) {
+                        for (int p = 0; p < kMaxProd; ++p) {
+                            if (p >= n_prod) break;
+                            const int ab = MODE == kModeFloat ? (p < 4 ? (p & 1) : 2 + (p & 1)) : p;
+                            const int bb = MODE == kModeFloat ? (p < 2 ? p : (p < 4 ? 2 + (p & 1) : (p & 1))) : p;
                             const uint64_t a_desc =
-                                a_desc0 + static_cast<uint64_t>((t * kPQTileBytes + kb * Cfg::kQKBlock) >> 4);
-                            const uint64_t b_kb = b_desc + static_cast<uint64_t>((kb * Cfg::kBKBlock) >> 4);
+                                a_desc0 + static_cast<uint64_t>((t * kPQTileBytes + ab * Cfg::kQKBlock) >> 4);
+                            const uint64_t b_kb = b_desc + static_cast<uint64_t>((bb * Cfg::kBKBlock) >> 4);
                             #pragma unroll
                             for (int kk = 0; kk < 4; ++kk) {
-                                const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
+                                const uint32_t acc = (p > 0 || kk > 0) ? 1u : 0u;
                                 if constexpr (F16)
                                     ptx::mma_f16_pair(d, a_desc + 2 * kk, b_kb + 2 * kk, idesc, acc);
                                 else
@@ -431,23 +456,29 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                 if (active) {
                     st.thr = min(st.thr, shared_thr);
                     const int32_t* rec = r_smem + s * kRecInts;
+                    auto scan = [&](const uint32_t (&v)[32], int r0, const int32_t* nrm, const int32_t* gm8) {
+                        if constexpr (MODE == kModeFloat)
+                            scan_group_float(v, r0, nrm, gm8, st);
+                        else
+                            scan_group<F16>(v, r0, nrm, gm8, st, dscale);
+                    };
                     const int row0 = cur.it.idx_base + j * kBN;
                     uint32_t va[32];
                     ptx::tmem_ld32(taddr, va);
                     ptx::tmem_ld_wait(va);
-                    scan_group<F16>(va, row0, rec, rec + 128, st, dscale);
+                    scan(va, row0, rec, rec + 128);
                     ptx::tmem_ld32(taddr + 32, va);
                     ptx::tmem_ld_wait(va);
-                    scan_group<F16>(va, row0 + 32, rec + 32, rec + 132, st, dscale);
+                    scan(va, row0 + 32, rec + 32, rec + 132);
                     ptx::tmem_ld32(taddr + 64, va);
                     ptx::tmem_ld_wait(va);
-                    scan_group<F16>(va, row0 + 64, rec + 64, rec + 136, st, dscale);
+                    scan(va, row0 + 64, rec + 64, rec + 136);
                     ptx::tmem_ld32(taddr + 96, va);
                     ptx::tmem_ld_wait(va);
                     ptx::tc_fence_before();
                     __syncwarp();
                     if (lane == 0) ptx::mbar_arrive_cluster_relaxed(lead_tempty);
-                    scan_group<F16>(va, row0 + 96, rec + 96, rec + 140, st, dscale);
+                    scan(va, row0 + 96, rec + 96, rec + 140);
                     if (valid && st.k2 < published) {
                         atomicMin(thresh + q, st.k2);
                         published = st.k2;
@@ -477,14 +508,17 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
     }
 }
 
-using CfgU8 = PairCfg<false, 2, 1>;
-using CfgF16 = PairCfg<true, 2, 1>;
+using CfgU8 = PairCfg<kModeU8, 2, 1>;
+using CfgF16 = PairCfg<kModeF16Int, 2, 1>;
+// Split float rows are 512 bytes: one query tile per CTA (groups of 256
+// queries) leaves room for 4 base stages.
+using CfgFloat = PairCfg<kModeFloat, 1, 1>;
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CfgU8::kThreads, 1)
     exact2nn_u8_pair_kernel(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap bmap,
                             const int32_t* __restrict__ brec, const ExactPlan plan, const WorkItem single,
                             int4* __restrict__ partial, int32_t* __restrict__ thresh, int* __restrict__ err) {
-    pair_body<false, 2, 1>(qmap, bmap, brec, plan, nullptr, 1, single, partial, thresh, err, 1.0f);
+    pair_body<kModeU8, 2, 1>(qmap, bmap, brec, plan, nullptr, 1, single, partial, thresh, err, 1.0f);
 }
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CfgF16::kThreads, 1)
@@ -492,16 +526,24 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CfgF16::kThreads, 1)
                              const int32_t* __restrict__ brec, const ExactPlan plan, const WorkItem single,
                              int4* __restrict__ partial, int32_t* __restrict__ thresh, int* __restrict__ err,
                              float dscale) {
-    pair_body<true, 2, 1>(qmap, bmap, brec, plan, nullptr, 1, single, partial, thresh, err, dscale);
+    pair_body<kModeF16Int, 2, 1>(qmap, bmap, brec, plan, nullptr, 1, single, partial, thresh, err, dscale);
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CfgFloat::kThreads, 1)
+    exact2nn_float_pair_kernel(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap bmap,
+                               const int32_t* __restrict__ brec, const ExactPlan plan, const WorkItem single,
+                               int4* __restrict__ partial, int32_t* __restrict__ thresh, int* __restrict__ err,
+                               int has_lo) {
+    pair_body<kModeFloat, 1, 1>(qmap, bmap, brec, plan, nullptr, 1, single, partial, thresh, err, 1.0f, has_lo != 0);
 }
 
 template <int QPT, int QB>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairCfg<false, QPT, QB>::kThreads, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairCfg<kModeU8, QPT, QB>::kThreads, 1)
     exact2nn_u8_pair_batch_kernel(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap bmap,
                                   const int32_t* __restrict__ brec, const ExactPlan plan,
                                   const WorkItem* __restrict__ items, int n_items, int4* __restrict__ partial,
                                   int32_t* __restrict__ thresh, int* __restrict__ err) {
-    pair_body<false, QPT, QB>(qmap, bmap, brec, plan, items, n_items, WorkItem{}, partial, thresh, err, 1.0f);
+    pair_body<kModeU8, QPT, QB>(qmap, bmap, brec, plan, items, n_items, WorkItem{}, partial, thresh, err, 1.0f);
 }
 
 template <typename K>
@@ -533,7 +575,7 @@ WorkItem single_item(const ExactPlan& plan) {
 template <int QPT, int QB>
 cudaError_t launch_batch_variant(const CUtensorMap& qmap, const CUtensorMap& bmap, const int32_t* brec,
                                  const BatchPlan& bp, int4* partial, int32_t* thresh, int* err, cudaStream_t stream) {
-    using Cfg = PairCfg<false, QPT, QB>;
+    using Cfg = PairCfg<kModeU8, QPT, QB>;
     static bool attr_set[64] = {};
     cudaError_t e = set_smem_once(exact2nn_u8_pair_batch_kernel<QPT, QB>, Cfg::kSmemBytes, attr_set);
     if (e != cudaSuccess) return e;
@@ -580,6 +622,18 @@ cudaError_t launch_exact2nn_f16_pair(const CUtensorMap& qmap, const CUtensorMap&
     if (plan.grid <= 0) return cudaSuccess;
     exact2nn_f16_pair_kernel<<<2 * plan.grid, CfgF16::kThreads, CfgF16::kSmemBytes, stream>>>(
         qmap, bmap_half, brec, plan, single_item(plan), partial, thresh, err, dscale);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_exact2nn_float_pair(const CUtensorMap& qmap, const CUtensorMap& bmap_half, const int32_t* brec,
+                                       const ExactPlan& plan, int4* partial, int32_t* thresh, int* err, bool has_lo,
+                                       cudaStream_t stream) {
+    static bool attr_set[64] = {};
+    cudaError_t e = set_smem_once(exact2nn_float_pair_kernel, CfgFloat::kSmemBytes, attr_set);
+    if (e != cudaSuccess) return e;
+    if (plan.grid <= 0) return cudaSuccess;
+    exact2nn_float_pair_kernel<<<2 * plan.grid, CfgFloat::kThreads, CfgFloat::kSmemBytes, stream>>>(
+        qmap, bmap_half, brec, plan, single_item(plan), partial, thresh, err, has_lo ? 1 : 0);
     return cudaGetLastError();
 }
 

@@ -128,6 +128,77 @@ __global__ void stats_f16_kernel(const uint4* __restrict__ x, size_t n8, int* __
     stats_flush(bad, sh, mx, stats);
 }
 
+// General (non-integer) descriptors: stats[0] |= 1 if a value is not finite,
+// stats[1] = bit pattern of the largest |value|.
+__device__ __forceinline__ void abs_one(float v, bool& bad, float& mx) {
+    const float a = fabsf(v);
+    bad |= !(a <= 3.0e38f);
+    if (a <= 3.0e38f) mx = fmaxf(mx, a);
+}
+
+__device__ __forceinline__ void abs_flush(bool bad, float mx, int* stats) {
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    bad = __any_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0) {
+        if (bad) atomicOr(stats, 1);
+        atomicMax(stats + 1, __float_as_int(mx));
+    }
+}
+
+__global__ void abs_stats_f32_kernel(const float4* __restrict__ x, size_t n4, int* __restrict__ stats) {
+    bool bad = false;
+    float mx = 0.0f;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n4;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const float4 v = x[i];
+        abs_one(v.x, bad, mx);
+        abs_one(v.y, bad, mx);
+        abs_one(v.z, bad, mx);
+        abs_one(v.w, bad, mx);
+    }
+    abs_flush(bad, mx, stats);
+}
+
+__global__ void abs_stats_f16_kernel(const uint4* __restrict__ x, size_t n8, int* __restrict__ stats) {
+    bool bad = false;
+    float mx = 0.0f;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n8;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const uint4 v = x[i];
+        const __half2* h = reinterpret_cast<const __half2*>(&v);
+        #pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float2 f = __half22float2(h[k]);
+            abs_one(f.x, bad, mx);
+            abs_one(f.y, bad, mx);
+        }
+    }
+    abs_flush(bad, mx, stats);
+}
+
+// Float rows -> split FP16 rows [n][256]: halves [0, 128) hold hi = fp16(x * mul)
+// and [128, 256) lo = fp16(x * mul - hi), so hi + lo carries 22 significant
+// bits of x * mul (mul a power of two: exact). Each thread converts 4
+// consecutive elements of one row.
+__global__ void pack_split_f16_kernel(const float4* __restrict__ x, size_t n4, float mul, __half* __restrict__ out) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n4;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const float4 v = x[i];
+        const size_t row = i >> 5, col = (i & 31) * 4;
+        const float s[4] = {v.x * mul, v.y * mul, v.z * mul, v.w * mul};
+        __half hi[4], lo[4];
+        #pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            hi[k] = __float2half_rn(s[k]);
+            lo[k] = __float2half_rn(s[k] - __half2float(hi[k]));
+        }
+        __half* o = out + row * 256 + col;
+        *reinterpret_cast<uint2*>(o) = *reinterpret_cast<const uint2*>(hi);
+        *reinterpret_cast<uint2*>(o + 128) = *reinterpret_cast<const uint2*>(lo);
+    }
+}
+
 unsigned grid_for(size_t items, int num_sms) {
     size_t blocks = (items + 255) / 256;
     const size_t cap = static_cast<size_t>(num_sms) * 8;
@@ -146,6 +217,27 @@ cudaError_t launch_value_stats(const void* x, bool half, size_t n_rows, int* sta
         const size_t n4 = n_rows * 32;
         stats_f32_kernel<<<grid_for(n4, num_sms), 256, 0, stream>>>(reinterpret_cast<const float4*>(x), n4, stats);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_abs_stats(const void* x, bool half, size_t n_rows, int* stats, int num_sms, cudaStream_t stream) {
+    if (n_rows == 0) return cudaSuccess;
+    if (half) {
+        const size_t n8 = n_rows * 16;
+        abs_stats_f16_kernel<<<grid_for(n8, num_sms), 256, 0, stream>>>(reinterpret_cast<const uint4*>(x), n8, stats);
+    } else {
+        const size_t n4 = n_rows * 32;
+        abs_stats_f32_kernel<<<grid_for(n4, num_sms), 256, 0, stream>>>(reinterpret_cast<const float4*>(x), n4, stats);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack_split_f16(const float* x, size_t n_rows, float mul, void* out, int num_sms,
+                                  cudaStream_t stream) {
+    const size_t n4 = n_rows * 32;
+    if (n4 == 0) return cudaSuccess;
+    pack_split_f16_kernel<<<grid_for(n4, num_sms), 256, 0, stream>>>(reinterpret_cast<const float4*>(x), n4, mul,
+                                                                     static_cast<__half*>(out));
     return cudaGetLastError();
 }
 

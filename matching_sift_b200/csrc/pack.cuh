@@ -23,4 +23,15 @@ cudaError_t launch_pack_f16_u8(const void* x, size_t n_rows, float mul, uint8_t*
 // stats[0] == 0 and (largest value) * 2^s <= 255.
 cudaError_t launch_value_stats(const void* x, bool half, size_t n_rows, int* stats, int num_sms, cudaStream_t stream);
 
+// General descriptors (any finite float / half values), accumulated into
+// stats[0..1] (caller zeroes them first): stats[0] |= 1 when a value is
+// infinite or NaN, stats[1] = bit pattern of the largest |value|.
+cudaError_t launch_abs_stats(const void* x, bool half, size_t n_rows, int* stats, int num_sms, cudaStream_t stream);
+
+// Float rows -> split FP16 rows out[n_rows][256] (16-byte aligned): halves
+// [0, 128) = hi = fp16(x * mul), [128, 256) = lo = fp16(x * mul - hi); mul is a
+// power of two chosen so that the largest |x * mul| stays below the FP16 range.
+cudaError_t launch_pack_split_f16(const float* x, size_t n_rows, float mul, void* out, int num_sms,
+                                  cudaStream_t stream);
+
 }  // namespace sift

@@ -149,14 +149,6 @@ def test_cublas_2nn_sift_all_memory_types(cuda_device):
     np.testing.assert_array_equal(m_host, want)
 
 
-def test_non_integer_input_is_rejected(cuda_device):
-    import torch
-
-    q = torch.rand((10, 128), device=cuda_device)
-    m = torch.zeros(10, dtype=torch.int32, device=cuda_device)
-    assert ms.cublas_2nn_sift(q, q, ms.FLOAT_DEVICE, 10, 10, m, 0.8) == ms.SIFT_ERR_NOT_INTEGER
-
-
 def test_device_brute_and_cublas_2nn_f(cuda_device):
     import torch
 

@@ -124,25 +124,24 @@ def test_reference_benchmark_scaling_through_cublas_2nn_sift(cuda_device):
     np.testing.assert_array_equal(got[:, :2], (d.astype(np.float64) / 2 ** 18).astype(np.float32))
 
 
-@pytest.mark.parametrize("bad", ["negative", "too_large", "not_dyadic", "nan"])
-def test_values_outside_the_contract_are_rejected(cuda_device, bad):
+@pytest.mark.parametrize("bad", ["negative", "too_large", "not_dyadic"])
+def test_values_outside_the_integer_contract_take_the_float_path(cuda_device, bad):
+    """One value that is not an integer in [0, 255] (times a power of two)
+    sends the whole search to the general float path; its results then
+    agree with the FP64 oracle within the float path's tolerance."""
     import torch
+
+    from test_float_gpu import check_2nn
 
     q, r = datagen.make_workload(20, 100, seed=13)
     qf = torch.from_numpy(q).to(cuda_device).float()
-    if bad == "negative":
-        qf[3, 7] = -1.0
-    elif bad == "too_large":
-        qf[3, 7] = 256.0
-    elif bad == "not_dyadic":
-        qf[3, 7] = 0.1
-    else:
-        qf[3, 7] = float("nan")
+    qf[3, 7] = {"negative": -1.0, "too_large": 256.0, "not_dyadic": 0.1}[bad]
     rf = torch.from_numpy(r).to(cuda_device).float()
-    for dt, typ in ((torch.float32, ms.FLOAT_DEVICE), (torch.float16, ms.HALF_DEVICE)):
-        m = torch.zeros(20, dtype=torch.int32, device=cuda_device)
-        rc = ms.cublas_2nn_sift(qf.to(dt), rf.to(dt), typ, 20, 100, m, 0.8)
-        assert rc == ms.SIFT_ERR_NOT_INTEGER, (dt, rc)
+    for dt in (torch.float32, torch.float16):
+        out = ms.match(qf.to(dt), rf.to(dt), outputs=("nn_idx", "nn_dist"))
+        assert ms.stream_status() == ms.SIFT_OK
+        check_2nn(qf.to(dt).float().cpu().numpy(), rf.to(dt).float().cpu().numpy(), out["nn_dist"].cpu().numpy(),
+                  out["nn_idx"].cpu().numpy())
 
 
 def test_fp16_scale_subset_vs_oracle(cuda_device):
