@@ -308,8 +308,13 @@ def main():
         variants["pairs"] = pairs_leg(args, ms, torch, dev, stream)
         variants["mutual"] = mutual_leg(args, ms, torch, dev, stream)
         truth = nn_idx[:, 0].cpu().numpy()
-        variants["learned"] = learned_leg(args, ms, torch, dev, stream, qd, rd, base, truth)
-        variants["lsh"] = lsh_leg(args, ms, torch, dev, stream, qd, rd, truth)
+        copies = datagen.query_copies(q_n, seed=rank)
+        hbm = _peaks()[0]["hbm_gbs"]
+        variants["lsh"] = lsh_leg(args, ms, torch, dev, stream, qd, rd, truth, copies, hbm)
+        variants["learned"] = learned_leg(args, ms, torch, dev, stream, qd, rd, base, truth, copies, hbm,
+                                          variants["lsh"]["grid"])
+        variants["cfg1"] = cfg1_leg(args, ms, torch, dev, stream)
+        variants["float"] = float_leg(args, ms, torch, dev, stream, q_n, _peaks()[0]["bf16_tflops"])
 
     # ---- end to end through the C ABI with host buffers
     e2e_ms = float("nan")
@@ -448,12 +453,13 @@ def main():
                 "call": "sift2nn_match_mutual_batch + sift_compact_matches (two batched searches, cross-check, "
                         "per-pair match lists), preallocated outputs",
                 "mutual_matches": v["mutual_matches"]}
-        for key in ("learned", "lsh"):
+        names = {"learned": "learned_hash", "lsh": "lsh", "cfg1": "cfg1_1000x10000", "float": "float32_general"}
+        for key, name in names.items():
             if key in variants:
                 v = dict(variants[key])
                 v.pop("step_ms", None)
                 v.pop("kernel_ms", None)
-                line.setdefault("variants", {})["learned_hash" if key == "learned" else "lsh"] = v
+                line.setdefault("variants", {})[name] = v
         if "fp16" in variants:
             v = variants["fp16"]
             f16_peak = peaks["bf16_tflops"]
@@ -614,60 +620,200 @@ def _time_calls(torch, stream, fn, steps):
     return a.elapsed_time(b) / steps, out
 
 
-def learned_leg(args, ms, torch, dev, stream, qd, rd, base, truth):
-    """Learned hash (MLP 128 -> 256 -> 16) trained on 100,000 synthetic
-    queries labelled by the exact kernel; 2-NN of the bench queries at
-    several operating points (probes, exact-fallback criteria), each call
-    rebuilding the base's buckets; recall@1 against the exact results."""
-    from matching_sift_b200 import datagen
+def _kernel_ms(lib, kind):
+    """Mean device time (ms) of the kernels of one kind timed by the library since the last collection."""
+    import ctypes
 
-    tq = torch.from_numpy(datagen.make_queries(100_000, base, seed=7)).to(dev)
-    t0 = time.perf_counter()
-    model = ms.MlpHash.train(rd, tq, k=16, steps=1500, batch=2048, lr=2e-3, seed=1)
-    train_s = time.perf_counter() - t0
+    t, n = ctypes.c_double(0.0), ctypes.c_int(0)
+    lib.sift_profile_collect_kernel(kind, ctypes.byref(t), ctypes.byref(n))
+    return t.value / n.value if n.value else None
+
+
+def _search_points(ms, torch, stream, idx, qd, truth, copies, settings, steps, hbm, L, k):
+    """Times idx.search at each (probes, min_candidates, max_dist) setting: queries/s,
+    recall@1 (all queries, noisy-copy and fresh halves), candidates, and the
+    hash / scan kernels' algorithmic bytes over their CUDA-event times."""
+    lib = ms.lib()
     q_n = qd.shape[0]
     points = []
-    steps = max(3, args.steps // 2)
-    for probes, min_cand, max_dist in ((1, 0, 0.0), (4, 0, 0.0), (16, 0, 0.0), (1, 64, 0.0), (4, 64, 30000.0),
-                                       (1, 64, 30000.0), (1, 0, 20000.0)):
-        ms_call, out = _time_calls(torch, stream, lambda: model.match(qd, rd, n_probes=probes, min_candidates=min_cand,
+    for probes, min_cand, max_dist in settings:
+        lib.sift_profile_enable(1)
+        ms_call, out = _time_calls(torch, stream, lambda: idx.search(qd, probes=probes, min_candidates=min_cand,
                                                                      max_dist=max_dist, stream=stream), steps)
+        lib.sift_profile_enable(0)
+        hash_ms, scan_ms = _kernel_ms(lib, 1), _kernel_ms(lib, 2)
+        _kernel_ms(lib, 0)
         got = out["nn_idx"][:, 0].cpu().numpy()
-        points.append({"probes": probes, "min_candidates": min_cand, "max_dist": max_dist,
-                       "ms_per_call": round(ms_call, 4), "value": round(q_n / (ms_call * 1e-3), 1),
-                       "recall1": round(float((got == truth).mean()), 4),
-                       "candidates_mean": round(float(out["candidates"].float().mean().item()), 1),
+        hit = got == truth
+        cand = float(out["candidates"].double().sum().item())
+        # algorithmic bytes: query rows + codes (+ margins for probes) for the hash;
+        # for the scan, query rows, two bucket bounds per probe and per compared
+        # candidate its id (and code for k > 16) and its 128-byte row
+        hash_bytes = q_n * 128 + L * q_n * 4 + (L * q_n * k * 4 if probes > 1 else 0)
+        scan_bytes = q_n * 128 + L * probes * q_n * 8 + cand * (128 + (8 if k > 16 else 4))
+        pt = {"probes": probes, "ms_per_call": round(ms_call, 4), "value": round(q_n / (ms_call * 1e-3), 1),
+              "recall1": round(float(hit.mean()), 4), "recall1_copies": round(float(hit[copies].mean()), 4),
+              "recall1_fresh": round(float(hit[~copies].mean()), 4),
+              "candidates_mean": round(cand / q_n, 1)}
+        if min_cand or max_dist:
+            pt.update({"min_candidates": min_cand, "max_dist": max_dist,
                        "exact_fallback_queries": int(out["fallback"])})
-    ok = [p for p in points if p["recall1"] >= 0.8]
-    best = max(ok, key=lambda p: p["value"]) if ok else None
-    return {"value": best["value"] if best else None, "unit": "queries/s",
-            "recall1": best["recall1"] if best else None, "operating_point": best,
-            "at": "fastest point with recall@1 >= 0.8 against the exact results (null if none)",
-            "workload": "same queries and base as the exact leg; every call hashes the base on the tensor cores "
-                        "and rebuilds its buckets",
-            "model": "MLP 128->256->16, BF16 weights, trained 1500 Adam steps x 2048 pairs "
-                     f"({train_s:.2f} s incl. exact labels of 100,000 training queries)",
-            "points": points}
+        if hash_ms:
+            pt["hash_kernel"] = {"ms": round(hash_ms, 4), "GB/s": round(hash_bytes / (hash_ms * 1e-3) / 1e9, 1),
+                                 "frac_hbm": round(hash_bytes / (hash_ms * 1e-3) / 1e9 / hbm, 4)}
+        if scan_ms:
+            pt["scan_kernel"] = {"ms": round(scan_ms, 4), "GB/s": round(scan_bytes / (scan_ms * 1e-3) / 1e9, 1),
+                                 "frac_hbm": round(scan_bytes / (scan_ms * 1e-3) / 1e9 / hbm, 4)}
+        points.append(pt)
+    return points
 
 
-def lsh_leg(args, ms, torch, dev, stream, qd, rd, truth):
-    """Random-hyperplane LSH (int8 N(0,1)*32 planes, seed 1) at several (k, L,
-    probes) settings: recall@1 against the exact results, queries/s per call
-    and mean candidates compared per query."""
+def _best_at(points, recall=0.8):
+    ok = [p for p in points if p["recall1"] >= recall]
+    return max(ok, key=lambda p: p["value"]) if ok else None
+
+
+def learned_leg(args, ms, torch, dev, stream, qd, rd, base, truth, copies, hbm, lsh_grid):
+    """Learned hash (MLP 128 -> 256 -> k, k in {16, 20, 24}) trained on 200,000
+    generator queries labelled by the exact kernel; the base hashed and
+    bucketed once per model (persistent index), then 2-NN of the bench queries
+    at several operating points (probes, exact-fallback criteria) with
+    recall@1 against the exact results, beside random-hyperplane LSH with the
+    same bits, one table and the same probes."""
     from matching_sift_b200 import datagen
 
-    q_n = qd.shape[0]
-    points = []
-    for k, L, probes in ((16, 8, 1), (16, 8, 8), (16, 8, 32), (8, 16, 1)):
-        planes = torch.from_numpy(datagen.quantize_planes(datagen.make_hyperplanes(k, L, seed=1))).to(dev)
-        ms_call, out = _time_calls(
-            torch, stream, lambda: ms.lsh_match(qd, rd, planes, stream=stream, probes=probes, candidates=True), 2)
-        got = out["nn_idx"][:, 0].cpu().numpy()
-        points.append({"k": k, "L": L, "probes": probes, "ms_per_call": round(ms_call, 3),
-                       "value": round(q_n / (ms_call * 1e-3), 1), "recall1": round(float((got == truth).mean()), 4),
-                       "candidates_mean": round(float(out["candidates"].double().mean().item()), 1)})
-    return {"unit": "queries/s", "call": "sift_lsh_match_probes (hash base + buckets + probe codes + scan per call)",
-            "points": points}
+    tq = torch.from_numpy(datagen.make_queries(200_000, base, seed=7)).to(dev)
+    steps = max(3, args.steps // 4)
+    per_k = []
+    for k in (16, 20, 24):
+        t0 = time.perf_counter()
+        model = ms.MlpHash.train(rd, tq, k=k, steps=1500, batch=2048, lr=2e-3, seed=1)
+        train_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        idx = ms.HashIndex.mlp(rd, model)
+        build_ms = (time.perf_counter() - t0) * 1e3
+        settings = [(p, 0, 0.0) for p in (1, 4, 16, 64)] + [(16, 64, 0.0), (64, 64, 0.0), (16, 0, 30000.0),
+                                                              (64, 0, 30000.0)]
+        pts = _search_points(ms, torch, stream, idx, qd, truth, copies, settings, steps, hbm, 1, k)
+        idx.close()
+        lsh_same = [g for g in lsh_grid if g["k"] == k and g["L"] == 1]
+        per_k.append({"k": k, "train_s": round(train_s, 2), "index_build_ms": round(build_ms, 2),
+                      "best_at_recall_0.8": _best_at(pts), "points": pts,
+                      "lsh_same_bits_L1": lsh_same[0]["points"] if lsh_same else None})
+        del model
+    best = [b for b in (x["best_at_recall_0.8"] for x in per_k) if b]
+    top = max(best, key=lambda p: p["value"]) if best else None
+    return {"value": top["value"] if top else None, "unit": "queries/s",
+            "at": "fastest operating point with recall@1 >= 0.8 against the exact results over k in {16, 20, 24}",
+            "operating_point": top,
+            "workload": "same queries and base as the exact leg; persistent index (base hashed and bucketed once "
+                        "per model); per call: query hash (tcgen05 MLP) + probe codes + candidate scan "
+                        "[+ exact fallback]",
+            "model": "MLP 128->256->k, BF16 weights, 1500 Adam steps x 2048 pairs, 200,000 training queries",
+            "per_k": per_k}
+
+
+def lsh_leg(args, ms, torch, dev, stream, qd, rd, truth, copies, hbm):
+    """Random-hyperplane LSH over k in {12, 16, 20, 24} bits x L in {1, 2, 4, 8}
+    tables (int8 hyperplanes = N(0,1) x 32 rounded, seed 1): the base hashed
+    and bucketed once per configuration (persistent index), then searched with
+    1 / 4 / 16 / 64 probes per table; recall@1 against the exact results,
+    queries/s per call and the hash / scan kernels' achieved GB/s."""
+    from matching_sift_b200 import datagen
+
+    grid = []
+    steps = 2
+    for k in (12, 16, 20, 24):
+        for L in (1, 2, 4, 8):
+            planes = torch.from_numpy(datagen.quantize_planes(datagen.make_hyperplanes(k, L, seed=1))).to(dev)
+            t0 = time.perf_counter()
+            idx = ms.HashIndex.lsh(rd, planes)
+            build_ms = (time.perf_counter() - t0) * 1e3
+            pts = []
+            for probes in (1, 4, 16, 64):
+                pts += _search_points(ms, torch, stream, idx, qd, truth, copies, [(probes, 0, 0.0)], steps, hbm, L,
+                                      k)
+                if pts[-1]["recall1"] >= 0.95 or pts[-1]["ms_per_call"] > 150.0:
+                    break
+            idx.close()
+            grid.append({"k": k, "L": L, "index_build_ms": round(build_ms, 2), "best_at_recall_0.8": _best_at(pts),
+                         "points": pts})
+    best = [g["best_at_recall_0.8"] | {"k": g["k"], "L": g["L"]} for g in grid if g["best_at_recall_0.8"]]
+    top = max(best, key=lambda p: p["value"]) if best else None
+    roof = None
+    if top and "scan_kernel" in top:
+        roof = {"bound": "hbm", "kernel": "lsh_scan_kernel", "achieved": top["scan_kernel"]["GB/s"], "peak": hbm,
+                "unit": "GB/s", "frac": top["scan_kernel"]["frac_hbm"],
+                "note": "algorithmic bytes (query rows, bucket bounds, per compared candidate its id and 128-byte "
+                        "row) over the kernel's CUDA-event time at the fastest recall>=0.8 point"}
+    return {"value": top["value"] if top else None, "unit": "queries/s", "operating_point": top,
+            "at": "fastest (k, L, probes) with recall@1 >= 0.8 against the exact results",
+            "call": "HashIndex.lsh / sift_index_search (base hashed and bucketed once per configuration)",
+            "roofline": roof, "grid": grid}
+
+
+def cfg1_leg(args, ms, torch, dev, stream):
+    """The reference's small configuration: 1,000 queries x 10,000 base rows,
+    u8 device rows (sift2nn_match) and float32 rows holding the integers
+    (cublas_2nn_sift, type FLOAT_DEVICE, as the reference benchmark calls it)."""
+    from matching_sift_b200 import datagen
+
+    q, r = datagen.make_workload(1000, 10000, seed=1)
+    qd, rd = torch.from_numpy(q).to(dev), torch.from_numpy(r).to(dev)
+    qf, rf = qd.float(), rd.float()
+    m = torch.empty(1000, dtype=torch.int32, device=dev)
+    lib = ms.lib()
+    steps = max(5, args.steps)
+    u8_ms, _ = _time_calls(torch, stream, lambda: lib.sift2nn_match(qd.data_ptr(), rd.data_ptr(), ms.U8_DEVICE, 1000,
+                                                                    10000, ms.METRIC_L2, THRESHOLD, m.data_ptr(),
+                                                                    None, None, None, stream.cuda_stream), steps)
+    f_ms, _ = _time_calls(torch, stream, lambda: lib.cublas_2nn_sift(qf.data_ptr(), rf.data_ptr(), ms.FLOAT_DEVICE,
+                                                                     1000, 10000, m.data_ptr(), THRESHOLD, None, 1,
+                                                                     0, 17), steps)
+    return {"value": round(1000 / (u8_ms * 1e-3), 1), "unit": "queries/s", "ms_per_call": round(u8_ms, 4),
+            "workload": "1,000 x 128 queries vs 10,000 x 128 base (seed 1), ratio test 0.8",
+            "call": "sift2nn_match (u8 device rows)",
+            "float32_call": {"ms_per_call": round(f_ms, 4), "value": round(1000 / (f_ms * 1e-3), 1),
+                             "call": "cublas_2nn_sift(type=FLOAT_DEVICE) on float32 rows holding the integers "
+                                     "(value check + u8 pack + search, synchronous)"}}
+
+
+def float_leg(args, ms, torch, dev, stream, q_n, bf16_peak):
+    """General float descriptors (the reference benchmark's default data:
+    unit-normalised vectors of rand()-range values, src/helper.cu:40-58), 10,000
+    x 1,000,000 float32: split FP16 rows, float keys (sift2nn_match FLOAT_DEVICE)."""
+    lib = ms.lib()
+    g = torch.Generator(device=dev)
+    g.manual_seed(3)
+    rf = torch.rand((R_N, DIM), device=dev, generator=g)
+    rf /= rf.norm(dim=1, keepdim=True)
+    qf = torch.rand((q_n, DIM), device=dev, generator=g)
+    qf /= qf.norm(dim=1, keepdim=True)
+    nn_idx = torch.empty((q_n, 2), dtype=torch.int32, device=dev)
+    steps = max(3, args.steps // 4)
+    lib.sift_profile_enable(1)
+    ms_call, _ = _time_calls(torch, stream, lambda: lib.sift2nn_match(qf.data_ptr(), rf.data_ptr(), ms.FLOAT_DEVICE,
+                                                                      q_n, R_N, ms.METRIC_L2, THRESHOLD, None, None,
+                                                                      nn_idx.data_ptr(), None, stream.cuda_stream),
+                             steps)
+    lib.sift_profile_enable(0)
+    k_ms = _kernel_ms(lib, 0)
+    if ms.stream_status(stream.cuda_stream) != 0:
+        raise RuntimeError("device status after the float steps")
+    flops = 3 * 2.0 * q_n * R_N * DIM
+    out = {"value": round(q_n / (ms_call * 1e-3), 1), "unit": "queries/s", "ms_per_call": round(ms_call, 4),
+           "dtype": "f32 (split into FP16 hi + lo)",
+           "workload": f"{q_n:,} x 128 float32 queries vs 1,000,000 x 128 float32 base, unit-normalised uniform "
+                       "values (general floats: not integers)",
+           "call": "sift2nn_match(type=SIFT_FLOAT_DEVICE): value check, split-FP16 pack, float norms, "
+                   "exact2nn_float_pair_kernel (three kind::f16 products per tile), merge"}
+    if k_ms:
+        ach = flops / (k_ms * 1e-3) / 1e12
+        out["roofline"] = {"bound": "tensor", "kernel": "exact2nn_float_pair_kernel", "kernel_ms": round(k_ms, 4),
+                           "achieved": round(ach, 1), "peak": round(bf16_peak, 1), "unit": "TFLOP/s",
+                           "frac": round(ach / bf16_peak, 4), "flops_per_launch": flops}
+    del qf, rf
+    return out
 
 
 def reference_arm(args, world, rank):

@@ -415,13 +415,20 @@ SIFT_API int sift_batch_describe(const sift_pair* pairs, int n_pairs, uint32_t r
 /* Number of kernels this library has launched in the process so far. */
 SIFT_API long long sift_launch_count(void);
 
-/* When enabled, the search kernel of every exact call is bracketed by CUDA
-   events recorded on the stream it is launched on. */
+/* When enabled, the timed kernels of every call are bracketed by CUDA events
+   recorded on the stream they are launched on: the exact search kernel
+   (SIFT_PROF_SEARCH), the query hash of the hash searches (SIFT_PROF_HASH)
+   and their candidate scan (SIFT_PROF_SCAN). */
+#define SIFT_PROF_SEARCH 0
+#define SIFT_PROF_HASH 1
+#define SIFT_PROF_SCAN 2
 SIFT_API void sift_profile_enable(int on);
 
 /* Synchronises the recorded events and returns (and clears) the summed search
    kernel time in milliseconds and the number of timed launches. */
 SIFT_API int sift_profile_collect(double* total_ms, int* launches);
+/* The same for one kernel kind (SIFT_PROF_*). */
+SIFT_API int sift_profile_collect_kernel(int kernel, double* total_ms, int* launches);
 
 /* Selects the exact-search kernel for subsequent calls in this process:
    0 (default) the CTA-pair kernels (tcgen05 cta_group::2; half inputs go to

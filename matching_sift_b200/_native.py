@@ -39,6 +39,8 @@ _PROTOS = {
     "sift_launch_count": (ctypes.c_longlong, []),
     "sift_profile_enable": (None, [ctypes.c_int]),
     "sift_profile_collect": (ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]),
+    "sift_profile_collect_kernel": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                                   ctypes.POINTER(ctypes.c_int)]),
     "sift_set_kernel_variant": (ctypes.c_int, [ctypes.c_int]),
     "lsh_gpu": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, _vp, ctypes.c_float, _vp,
                                ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),

@@ -37,7 +37,38 @@ std::atomic<long long> g_launches{0};  // kernels launched by this library
 std::atomic<int> g_variant{0};
 std::atomic<bool> g_profile{false};
 std::mutex g_prof_mu;
-std::vector<std::pair<cudaEvent_t, cudaEvent_t>> g_prof_events;
+struct ProfRecord {
+    int tag;
+    cudaEvent_t e0, e1;
+};
+std::vector<ProfRecord> g_prof_events;
+
+ProfSpan::ProfSpan(cudaStream_t st, int tag) : st_(st), tag_(tag) {
+    if (!g_profile.load()) return;
+    if (cudaEventCreate(&e0_) != cudaSuccess || cudaEventRecord(e0_, st) != cudaSuccess) {
+        cudaGetLastError();
+        if (e0_) cudaEventDestroy(e0_);
+        e0_ = nullptr;
+    }
+}
+
+void ProfSpan::end() {
+    if (!e0_) return;
+    cudaEvent_t e1 = nullptr;
+    if (cudaEventCreate(&e1) == cudaSuccess && cudaEventRecord(e1, st_) == cudaSuccess) {
+        std::lock_guard<std::mutex> pl(g_prof_mu);
+        g_prof_events.push_back({tag_, e0_, e1});
+    } else {
+        cudaGetLastError();
+        cudaEventDestroy(e0_);
+        if (e1) cudaEventDestroy(e1);
+    }
+    e0_ = nullptr;
+}
+
+ProfSpan::~ProfSpan() {
+    if (e0_) cudaEventDestroy(e0_);
+}
 
 
 int ensure_ready(DeviceCtx*& out, int& dev) {
@@ -376,6 +407,11 @@ int exact_match_chunked(const MatchArgs& a, DeviceCtx& c, cudaStream_t st) {
         SIFT_CUDA(cudaStreamWaitEvent(st, c.chunk_ev[ch], 0));
         SIFT_CUDA(launch_row_norms_u8(rd + static_cast<size_t>(off) * kDim, plans[ch].r_n, plans[ch].r_pad, a.metric,
                                       nullptr, brec + static_cast<size_t>(off / kBN) * kRecInts, nullptr, st));
+        // The first chunk's rows seed the pruning bounds of the whole search.
+        if (ch == 0) {
+            SIFT_CUDA(launch_seed_thresh(qd, rd, q_n, plans[0].r_n, brec, thresh, st));
+            ++g_launches;
+        }
         WorkItem it{};
         it.n_a = q_n;
         it.b_off = off;
@@ -497,7 +533,9 @@ int exact_match_float(const MatchArgs& a, DeviceCtx& c, cudaStream_t st) {
         SIFT_TRY(encode_f16_rows(&qmap, q_rows, q_n, kBM, width));
         SIFT_TRY(encode_f16_rows(&bmap, r_rows, r_n, kBN / 2, width));
         SIFT_CUDA(maybe_inject_wait_expiry(c.d_status, st));
+        ProfSpan span(st, kProfSearch);
         SIFT_CUDA(launch_exact2nn_float_pair(qmap, bmap, brec, plan, partial, thresh, c.d_status, has_lo, st));
+        span.end();
         ++g_launches;
     }
     uint32_t* m_out = (a.matches && !m_dev) ? reinterpret_cast<uint32_t*>(A + o_m) : a.matches;
@@ -596,6 +634,9 @@ int exact_match(const MatchArgs& a) {
     } else {
         SIFT_CUDA(launch_row_norms_u8(rd, r_n, plan.r_pad, a.metric, nullptr, brec, nullptr, st));
         SIFT_CUDA(launch_row_norms_u8(qd, q_n, plan.q_pad, kMetricL2, qnorm, nullptr, thresh, st));
+        // Start the pruning bounds from a sample of the base rather than INT_MAX.
+        SIFT_CUDA(launch_seed_thresh(qd, rd, q_n, r_n, brec, thresh, st));
+        g_launches += r_n >= 2 ? 1 : 0;
     }
     g_launches += (plan.r_pad > 0 ? 1 : 0) + 1;
 
@@ -611,13 +652,7 @@ int exact_match(const MatchArgs& a) {
             SIFT_TRY(encode_u8_rows(&bmap, rd, r_n, use_pair ? kBN / 2 : kBN));
         }
         SIFT_CUDA(maybe_inject_wait_expiry(c.d_status, st));
-        cudaEvent_t e0 = nullptr, e1 = nullptr;
-        const bool prof = g_profile.load();
-        if (prof) {
-            SIFT_CUDA(cudaEventCreate(&e0));
-            SIFT_CUDA(cudaEventCreate(&e1));
-            SIFT_CUDA(cudaEventRecord(e0, st));
-        }
+        ProfSpan span(st, kProfSearch);
         if (use_f16)
             SIFT_CUDA(launch_exact2nn_f16_pair(qmap, bmap, brec, plan, partial, thresh, c.d_status,
                                                ldexpf(1.0f, 2 * shift), st));
@@ -626,11 +661,7 @@ int exact_match(const MatchArgs& a) {
         else
             SIFT_CUDA(launch_exact2nn_u8(qmap, bmap, brec, plan, partial, thresh, c.d_status, st));
         ++g_launches;
-        if (prof) {
-            SIFT_CUDA(cudaEventRecord(e1, st));
-            std::lock_guard<std::mutex> pl(g_prof_mu);
-            g_prof_events.emplace_back(e0, e1);
-        }
+        span.end();
     }
 
     // ---- merge + outputs
@@ -840,21 +871,24 @@ int stream_status(void* stream) {
     return collect_device_status(*cp, st);
 }
 
-int profile_collect(double* total_ms, int* launches) {
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+int profile_collect(int tag, double* total_ms, int* launches) {
+    if (tag < 0 || tag >= kProfTags) return SIFT_ERR_INVALID_ARG;
+    std::vector<ProfRecord> ev;
     {
         std::lock_guard<std::mutex> pl(g_prof_mu);
-        ev.swap(g_prof_events);
+        std::vector<ProfRecord> keep;
+        for (auto& p : g_prof_events) (p.tag == tag ? ev : keep).push_back(p);
+        g_prof_events.swap(keep);
     }
     double tot = 0.0;
     int rc = SIFT_OK;
     for (auto& p : ev) {
         float ms = 0.f;
-        if (cudaEventSynchronize(p.second) != cudaSuccess || cudaEventElapsedTime(&ms, p.first, p.second) != cudaSuccess)
+        if (cudaEventSynchronize(p.e1) != cudaSuccess || cudaEventElapsedTime(&ms, p.e0, p.e1) != cudaSuccess)
             rc = SIFT_ERR_CUDA;
         tot += ms;
-        cudaEventDestroy(p.first);
-        cudaEventDestroy(p.second);
+        cudaEventDestroy(p.e0);
+        cudaEventDestroy(p.e1);
     }
     if (total_ms) *total_ms = tot;
     if (launches) *launches = static_cast<int>(ev.size());
@@ -1010,6 +1044,9 @@ const char* sift_version(void) { return "sift2nn-b200 0.1.0 (sm_100a)"; }
 long long sift_launch_count(void) { return sift::launch_count(); }
 void sift_profile_enable(int on) { sift::profile_enable(on != 0); }
 int sift_set_kernel_variant(int variant) { return sift::set_variant(variant); }
-int sift_profile_collect(double* total_ms, int* launches) { return sift::profile_collect(total_ms, launches); }
+int sift_profile_collect(double* total_ms, int* launches) { return sift::profile_collect(0, total_ms, launches); }
+int sift_profile_collect_kernel(int kernel, double* total_ms, int* launches) {
+    return sift::profile_collect(kernel, total_ms, launches);
+}
 
 }  // extern "C"

@@ -49,7 +49,7 @@ int lsh_buckets(const uint32_t* codes, uint32_t n, int L, int k, int* start, int
 void reference_planes(int L, int nbits, int8_t* out);
 int stream_status(void* stream);
 void set_last_status(int s);
-int profile_collect(double* total_ms, int* launches);
+int profile_collect(int tag, double* total_ms, int* launches);
 long long launch_count();
 void profile_enable(bool on);
 int set_variant(int v);

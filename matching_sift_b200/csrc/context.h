@@ -93,6 +93,23 @@ int encode_bf16_2d(CUtensorMap* m, const void* base, uint64_t inner, uint64_t ro
 int map_cuda(cudaError_t e);
 // Reads and clears the device status words. Caller has synchronised `st`.
 int collect_device_status(DeviceCtx& c, cudaStream_t st);
+// Benchmark timing of one kernel launch on `st` (CUDA events recorded on the
+// launching stream when profiling is enabled; collected by tag).
+enum ProfTag : int { kProfSearch = 0, kProfHash = 1, kProfScan = 2, kProfTags = 3 };
+class ProfSpan {
+public:
+    ProfSpan(cudaStream_t st, int tag);
+    void end();
+    ~ProfSpan();
+    ProfSpan(const ProfSpan&) = delete;
+    ProfSpan& operator=(const ProfSpan&) = delete;
+
+private:
+    cudaStream_t st_;
+    int tag_;
+    cudaEvent_t e0_ = nullptr;
+};
+
 // Fault injection for the failure-detection tests (faults.cu): launches the
 // wait-expiry probe on `st` when armed, recording into *err.
 cudaError_t maybe_inject_wait_expiry(int* err, cudaStream_t st);

@@ -456,29 +456,32 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                 if (active) {
                     st.thr = min(st.thr, shared_thr);
                     const int32_t* rec = r_smem + s * kRecInts;
-                    auto scan = [&](const uint32_t (&v)[32], int r0, const int32_t* nrm, const int32_t* gm8) {
-                        if constexpr (MODE == kModeFloat)
-                            scan_group_float(v, r0, nrm, gm8, st);
-                        else
-                            scan_group<F16>(v, r0, nrm, gm8, st, dscale);
-                    };
+                    constexpr int kKind = MODE == kModeFloat ? kAccFloat : (F16 ? kAccF32Int : kAccS32);
                     const int row0 = cur.it.idx_base + j * kBN;
-                    uint32_t va[32];
-                    ptx::tmem_ld32(taddr, va);
+                    // The slot's 128 columns in 8 chunks of 16: chunk c + 1 loads
+                    // while chunk c is scanned, so the slot is handed back as soon
+                    // as the last chunk is in registers.
+                    uint32_t va[16], vb[16];
+                    auto scan = [&](const uint32_t (&v)[16], int c) {
+                        scan16<kKind>(v, row0 + 16 * c, rec + 16 * c, rec + 128 + 2 * c, st, dscale);
+                    };
+                    ptx::tmem_ld16(taddr, va);
                     ptx::tmem_ld_wait(va);
-                    scan(va, row0, rec, rec + 128);
-                    ptx::tmem_ld32(taddr + 32, va);
-                    ptx::tmem_ld_wait(va);
-                    scan(va, row0 + 32, rec + 32, rec + 132);
-                    ptx::tmem_ld32(taddr + 64, va);
-                    ptx::tmem_ld_wait(va);
-                    scan(va, row0 + 64, rec + 64, rec + 136);
-                    ptx::tmem_ld32(taddr + 96, va);
-                    ptx::tmem_ld_wait(va);
+                    #pragma unroll
+                    for (int c = 1; c < 8; c += 2) {
+                        ptx::tmem_ld16(taddr + 16 * c, vb);
+                        scan(va, c - 1);
+                        ptx::tmem_ld_wait(vb);
+                        if (c + 1 < 8) {
+                            ptx::tmem_ld16(taddr + 16 * (c + 1), va);
+                            scan(vb, c);
+                            ptx::tmem_ld_wait(va);
+                        }
+                    }
                     ptx::tc_fence_before();
                     __syncwarp();
                     if (lane == 0) ptx::mbar_arrive_cluster_relaxed(lead_tempty);
-                    scan(va, row0 + 96, rec + 96, rec + 140);
+                    scan(vb, 7);
                     if (valid && st.k2 < published) {
                         atomicMin(thresh + q, st.k2);
                         published = st.k2;

@@ -373,7 +373,11 @@ int index_search(const sift_code_index* ix, const uint8_t* q, uint32_t q_n_, int
     uint32_t* counts = candidates ? candidates : reinterpret_cast<uint32_t*>(A + o_cnt);
     float* dist = nn_dist ? nn_dist : reinterpret_cast<float*>(A + o_dist);
 
-    SIFT_TRY(index_hash(c, *ix, q, q_n, codes_q, z, st));
+    {
+        detail::ProfSpan span(st, detail::kProfHash);
+        SIFT_TRY(index_hash(c, *ix, q, q_n, codes_q, z, st));
+        span.end();
+    }
     const uint32_t* probe_codes = codes_q;
     if (multi) {
         uint32_t* pc = reinterpret_cast<uint32_t*>(A + o_pc);
@@ -383,9 +387,13 @@ int index_search(const sift_code_index* ix, const uint8_t* q, uint32_t q_n_, int
         detail::g_launches += L_;
         probe_codes = pc;
     }
-    SIFT_CUDA(launch_lsh_scan(q, ix->r, q_n, ix->r_n, L_, probes, ix->shift, ix->nbins, probe_codes, ix->start,
-                              ix->order, ix->ocode, threshold, threshold > 0.0f ? 1 : 0, 1.0f, matches, counts, nn_idx,
-                              dist, st));
+    {
+        detail::ProfSpan span(st, detail::kProfScan);
+        SIFT_CUDA(launch_lsh_scan(q, ix->r, q_n, ix->r_n, L_, probes, ix->shift, ix->nbins, probe_codes, ix->start,
+                                  ix->order, ix->ocode, threshold, threshold > 0.0f ? 1 : 0, 1.0f, matches, counts,
+                                  nn_idx, dist, st));
+        span.end();
+    }
     ++detail::g_launches;
     if (!fallback) return SIFT_OK;
     SIFT_TRY(exact_fallback(c, A, fs, q, ix->r, q_n, ix->r_n, ix->brec, counts, dist, min_cand, max_dist, threshold,

@@ -60,6 +60,17 @@ def make_queries(n: int, base: np.ndarray, seed: int = 0, copy_frac: float = 0.5
     return out
 
 
+def query_copies(n: int, seed: int = 0, copy_frac: float = 0.5) -> np.ndarray:
+    """Boolean mask of the queries of ``make_queries(n, ..., seed, copy_frac)``
+    that are noisy copies of base rows (the rest are fresh draws)."""
+    rng = np.random.default_rng([seed, 1])
+    n_copy = int(round(n * copy_frac))
+    perm = rng.permutation(n)
+    mask = np.zeros(n, bool)
+    mask[perm[:n_copy]] = True
+    return mask
+
+
 def make_workload(n_query: int, n_base: int, seed: int = 0):
     """(queries, base) as uint8 arrays from the recipe above."""
     base = make_base(n_base, seed)

@@ -48,39 +48,106 @@ def test_lsh_match_vs_oracle(cuda_device, L, k):
     np.testing.assert_array_equal(out["matches"].cpu().numpy().view(np.uint32), want)
 
 
-def test_buckets_equal_reference_lsh_thread_sort_reduce(cuda_device):
-    """The reference's own code + bucket grouping (FP16 hash GEMM, set_bit_h,
-    thrust sort, host run-length) for the same hyperplanes."""
+def _groups(codes, ids):
+    """(code, id) pairs sorted lexicographically: the grouping as sets of ids per code."""
+    o = np.lexsort((ids, codes))
+    return np.stack([codes[o].astype(np.int64), ids[o].astype(np.int64)])
+
+
+# Unit roundoff of FP16 and the worst-case bound of a 128-term FP16 sum
+# (products and partial sums each rounded): |fl(sum) - sum| <= gamma_128 * sum |x_i p_i|.
+_U16 = 2.0 ** -11
+_GAMMA128 = 128 * _U16 / (1 - 128 * _U16)
+
+
+@pytest.mark.parametrize("family", ["pm1", "gauss"])
+@pytest.mark.parametrize("k", [12, 16, 20, 24])
+def test_buckets_equal_reference_lsh_thread_sort_reduce(cuda_device, family, k):
+    """Bucket contents against the reference's own bucketing given the same
+    hyperplanes (lsh_thread_sort_reduce, src/lsh_h.cu:565-629: cublasHgemm hash
+    dots as at :909, set_bit_h, thrust sort by code, host run-length into
+    {first id, count} runs), 100,000 generator points.
+
+    Hyperplane families: the reference's own +/-1 planes (pm1), and N(0,1)
+    planes rounded to multiples of 1/32 (gauss: exact in FP16 for the
+    reference, int8 x 1/32 here), so both sides hash with identical planes.
+    The library's dot products are exact integers; the reference's are FP16
+    sums. Every point whose code differs is listed, and each of its differing
+    bits must have |exact dot| within the FP16 bound gamma_128 * sum|x_i p_i|.
+    Apart from those points the two groupings are identical as sets of ids per
+    code, and the reference's runs are checked to be its groups."""
     import torch
 
     if not oracle.ref_available():
         pytest.skip("reference library not built")
     ref = oracle.ref()
-    n, nbits = 4000, 16
+    n = 100_000
     x = datagen.make_base(n, seed=77)
-    rng = np.random.default_rng(3)
-    planes = np.where(rng.random((nbits, 128)) >= 0.5, 1, -1).astype(np.int8)  # the reference's +/-1 family
-    ours = ms.lsh_hash(torch.from_numpy(x).to(cuda_device), torch.from_numpy(planes[None]).to(cuda_device))
-    ours = ours.cpu().numpy().view(np.uint32)[0]
+    rng = np.random.default_rng(1000 + k)
+    if family == "pm1":
+        planes = np.where(rng.random((k, 128)) >= 0.5, 1, -1).astype(np.int8)
+        pl16 = planes.astype(np.float16)
+    else:
+        planes = datagen.quantize_planes(datagen.make_hyperplanes(k, 1, seed=k), 32.0)[0]
+        pl16 = (planes.astype(np.float32) / 32.0).astype(np.float16)
+        assert np.array_equal(pl16.astype(np.float32) * 32.0, planes.astype(np.float32))
+    xd = torch.from_numpy(x).to(cuda_device)
+    codes = ms.lsh_hash(xd, torch.from_numpy(planes[None]).to(cuda_device))
+    start, order, ocode = ms.lsh_buckets(codes, k)
+    ours = codes.cpu().numpy().view(np.uint32)[0]
+    start, order, ocode = start.cpu().numpy()[0], order.cpu().numpy()[0], ocode.cpu().numpy().view(np.uint32)[0]
+
     code = np.zeros(n, np.int32)
     index = np.zeros(n, np.int32)
     buckets = np.zeros(2 * n, np.int32)
     nb = ctypes.c_int(0)
-    pts16 = x.astype(np.float16)
-    pl16 = planes.astype(np.float16)
-    rc = ref.ref_lsh_buckets(pts16.ctypes.data, n, pl16.ctypes.data, nbits, code.ctypes.data, index.ctypes.data,
-                             buckets.ctypes.data, ctypes.byref(nb))
+    rc = ref.ref_lsh_buckets(x.astype(np.float16).ctypes.data, n, pl16.ctypes.data, k, code.ctypes.data,
+                             index.ctypes.data, buckets.ctypes.data, ctypes.byref(nb))
     assert rc == 0
     ref_code = code.view(np.uint32)
+    runs = buckets[:2 * nb.value].reshape(-1, 2)
+
+    # The library: exact codes, and its table groups every point by its code.
     dots = x.astype(np.int64) @ planes.astype(np.int64).T
-    differ = ref_code != ours
-    # The reference accumulates the hash GEMM in FP16: only points with a dot
-    # product close to zero may land in another bucket.
-    assert (np.abs(dots[differ]).min(axis=1) <= 64).all() if differ.any() else True
-    assert differ.mean() < 0.01
-    # identical grouping wherever the codes agree: the reference's sorted index
-    # order groups equal codes contiguously
-    assert (np.diff(ref_code[index].astype(np.int64)) >= 0).all()
+    exact = ((dots < 0).astype(np.uint64) << np.arange(k, dtype=np.uint64)).sum(1).astype(np.uint32)
+    np.testing.assert_array_equal(ours, exact)
+    top = min(k, 16)
+    assert start[0] == 0 and start[-1] == n and (np.diff(start) >= 0).all()
+    np.testing.assert_array_equal(ocode, ours[order])
+    np.testing.assert_array_equal(np.repeat(np.arange(1 << top), np.diff(start)), ocode >> (k - top))
+
+    # The reference: its runs partition its sorted index into groups of one code.
+    assert runs[:, 1].sum() == n and (runs[:, 1] > 0).all()
+    pos = np.concatenate([[0], np.cumsum(runs[:, 1])[:-1]])
+    np.testing.assert_array_equal(index[pos], runs[:, 0])  # each run starts at its first id
+    run_code = ref_code[runs[:, 0]]
+    np.testing.assert_array_equal(ref_code[index], np.repeat(run_code, runs[:, 1]))
+    assert len(np.unique(run_code)) == len(run_code)
+    assert sorted(index.tolist()) == list(range(n))
+
+    # Differences: points whose FP16 code differs, every differing bit within the bound.
+    differ = np.nonzero(ref_code != ours)[0]
+    bound = _GAMMA128 * (x.astype(np.float64) @ np.abs(planes.astype(np.float64)).T)
+    for i in differ:
+        bits = np.nonzero((int(ref_code[i]) ^ int(ours[i])) >> np.arange(k) & 1)[0]
+        assert (np.abs(dots[i, bits]) <= bound[i, bits]).all(), (i, bits, dots[i, bits], bound[i, bits])
+    near = (np.abs(dots) <= bound).any(1)
+    assert len(differ) <= int(near.sum())
+    print(f"{family} k={k}: {len(differ)} of {n} points hashed differently by the FP16 reference "
+          f"(points with a bit inside the FP16 bound: {int(near.sum())}); buckets {nb.value}")
+
+    # Identical groupings apart from those points.
+    keep = np.ones(n, bool)
+    keep[differ] = False
+    ids = np.arange(n)
+    np.testing.assert_array_equal(_groups(ref_code[keep], ids[keep]), _groups(ours[keep], ids[keep]))
+    # ... and each differing point sits in the group of its own code on each side.
+    in_ours = np.zeros(n, np.uint32)
+    in_ours[order] = ocode
+    in_ref = np.zeros(n, np.uint32)
+    in_ref[index] = np.repeat(run_code, runs[:, 1])
+    np.testing.assert_array_equal(in_ours[differ], ours[differ])
+    np.testing.assert_array_equal(in_ref[differ], ref_code[differ])
 
 
 def test_lsh_gpu_reference_entry_point(cuda_device):

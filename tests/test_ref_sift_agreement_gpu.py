@@ -1,0 +1,126 @@
+"""Agreement of the drop-in cublas_2nn_sift with the reference's own
+cublas_2nn_sift (src/knn_brute.cu:24-209, built from its sources), with every
+disagreement classified.
+
+The reference is run as its benchmark runs it: float inputs divided by 512
+(src/test.cu:103), type FLOAT_DEVICE, stream_n 1, a 383-query batch budget and
+17 warps (src/test.cu:210). It ranks base rows by -2 q.r (no norms) computed
+in FP16 by cublasHgemm (:244), and tests sqrt(d1 + 2) / sqrt(d2 + 2) < thr
+(:430-442). The drop-in ranks by the exact squared distance and tests
+sqrt(D1) / sqrt(D2) < thr. A query on which the two differ must fall in one of
+these classes (anything else fails the test):
+
+  fp16      the reference's nearest row is not the exact -2 q.r nearest, but
+            its exact dot product is within the FP16 error bound of the best
+            one: dot(ref) >= dot(best) (1 - g) / (1 + g), g = gamma_129 of
+            unit roundoff 2^-11 (products, 128-term sum and the final store
+            each rounded; all terms are non-negative);
+  metric    the exact -2 q.r nearest row differs from the exact L2 nearest
+            row (norms are not all equal), and the reference picked the
+            former (up to an fp16 tie);
+  ratio     same nearest row, different ratio-test outcome, and either the
+            two formulas straddle the threshold on exact values, or the
+            reference's exact-value ratio lies within its FP16 error interval
+            of the threshold, or the reference passes a query its own
+            formula on exact values rejects (its running second-best keeps
+            only the smaller of two candidates' seconds and can drop the true
+            second, src/knn_brute.cu:451-482 -- which only ever makes it pass
+            more, never less).
+"""
+import numpy as np
+import pytest
+
+import matching_sift_b200 as ms
+import oracle
+from matching_sift_b200 import datagen
+
+pytestmark = pytest.mark.gpu
+U32_MAX = np.uint32(0xFFFFFFFF)
+G = 129 * 2.0 ** -11 / (1 - 129 * 2.0 ** -11)
+SCALE = 512.0 ** 2
+
+
+def _ref_sift(ref, qd, rd, q_n, r_n, thr, dev):
+    import torch
+
+    m = torch.zeros(q_n, dtype=torch.int32, device=dev)
+    assert ref.ref_cublas_2nn_sift(qd.data_ptr(), rd.data_ptr(), q_n, r_n, m.data_ptr(), thr, 1, 2 * r_n * 383,
+                                   17) == 0
+    return m.cpu().numpy().view(np.uint32)
+
+
+def _classify(q, r, ref2, ref8, ours2, ours8):
+    d, i = oracle.brute_2nn_u8(q, r)
+    dd, di = oracle.brute_2nn_u8(q, r, metric=1)
+    qi = q.astype(np.int64)
+
+    def dot(k, j):
+        return int(qi[k] @ r[j].astype(np.int64))
+
+    counts = {"agree": 0, "fp16": 0, "metric": 0, "ratio": 0}
+    unexplained = []
+    lo_f = (1 - G) / (1 + G)
+    for k in range(q.shape[0]):
+        a, b = int(ref2[k]), int(ours2[k])
+        assert b == i[k, 0]
+        near_ok = a == b
+        if not near_ok:
+            c = int(di[k, 0])
+            tie = dot(k, a) >= dot(k, c) * lo_f
+            if c != b and (a == c or tie):
+                counts["metric"] += 1
+            elif c == b and tie:
+                counts["fp16"] += 1
+            else:
+                unexplained.append((k, "nearest", a, b, c, dot(k, a), dot(k, c)))
+            continue
+        rp, op = ref8[k] != U32_MAX, ours8[k] != U32_MAX
+        if rp == op:
+            counts["agree"] += 1
+            continue
+        # ratio-test disagreement on the same nearest row
+        c1, c2 = int(di[k, 0]), int(di[k, 1])
+        x1, x2 = dot(k, c1) / SCALE, dot(k, c2) / SCALE
+        r_ref = np.sqrt((2 - 2 * x1) / (2 - 2 * x2))
+        r_ours = np.sqrt(d[k, 0] / d[k, 1])
+        e1, e2 = 2 * G * x1, 2 * G * x2
+        r_lo = np.sqrt(max(2 - 2 * x1 - e1, 0.0) / (2 - 2 * x2 + e2))
+        r_hi = np.sqrt((2 - 2 * x1 + e1) / max(2 - 2 * x2 - e2, 1e-30))
+        straddle = (r_ref < 0.8) != (r_ours < 0.8)
+        within = r_lo < 0.8 < r_hi
+        second_defect = rp and r_lo >= 0.8
+        if straddle or within or second_defect:
+            counts["ratio"] += 1
+        else:
+            unexplained.append((k, "ratio", bool(rp), bool(op), float(r_ref), float(r_ours)))
+    return counts, unexplained
+
+
+@pytest.mark.parametrize("case", ["cfg1_1000x10000", "cfg2_1000x1000000"])
+def test_agreement_with_reference_cublas_2nn_sift(cuda_device, case):
+    import torch
+
+    if not oracle.ref_available():
+        pytest.skip("reference library not built")
+    ref = oracle.ref()
+    if case.startswith("cfg1"):
+        q, r = datagen.make_workload(1000, 10000, seed=1)
+    else:
+        r = datagen.make_base(1_000_000, seed=0)
+        q = datagen.make_queries(10_000, r, seed=0)[:1000]
+    q_n, r_n = q.shape[0], r.shape[0]
+    qd = torch.from_numpy(q.astype(np.float32) / 512.0).to(cuda_device)
+    rd = torch.from_numpy(r.astype(np.float32) / 512.0).to(cuda_device)
+    ref2 = _ref_sift(ref, qd, rd, q_n, r_n, 2.0, cuda_device)
+    ref8 = _ref_sift(ref, qd, rd, q_n, r_n, 0.8, cuda_device)
+    ours = {}
+    for thr in (2.0, 0.8):
+        m = torch.zeros(q_n, dtype=torch.int32, device=cuda_device)
+        assert ms.cublas_2nn_sift(qd, rd, ms.FLOAT_DEVICE, q_n, r_n, m, thr) == ms.SIFT_OK
+        ours[thr] = m.cpu().numpy().view(np.uint32)
+    counts, unexplained = _classify(q, r, ref2, ref8, ours[2.0], ours[0.8])
+    total = q_n
+    print(f"{case}: nearest agrees {float((ref2 == ours[2.0]).mean()):.4f}, matches at 0.8 agree "
+          f"{float((ref8 == ours[0.8]).mean()):.4f}; classes {counts}")
+    assert not unexplained, unexplained[:10]
+    assert sum(counts.values()) == total
