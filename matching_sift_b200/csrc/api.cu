@@ -631,6 +631,8 @@ int exact_match(const MatchArgs& a) {
         const float mul = ldexpf(1.0f, shift);
         SIFT_CUDA(launch_row_norms_f16(a.r, r_n, plan.r_pad, mul, a.metric, nullptr, brec, nullptr, st));
         SIFT_CUDA(launch_row_norms_f16(a.q, q_n, plan.q_pad, mul, kMetricL2, qnorm, nullptr, thresh, st));
+        SIFT_CUDA(launch_seed_thresh_f16(a.q, a.r, q_n, r_n, mul, brec, thresh, st));
+        g_launches += r_n >= 2 ? 1 : 0;
     } else {
         SIFT_CUDA(launch_row_norms_u8(rd, r_n, plan.r_pad, a.metric, nullptr, brec, nullptr, st));
         SIFT_CUDA(launch_row_norms_u8(qd, q_n, plan.q_pad, kMetricL2, qnorm, nullptr, thresh, st));
