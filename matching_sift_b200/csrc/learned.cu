@@ -12,7 +12,10 @@
 // Warps: 0 = weight and input-tile TMA, TMEM allocation, MMA issue (one
 //            thread); the u8 input tiles stream through a 2-stage ring,
 //            loaded two tiles ahead;
-//        1..4 = conversion and epilogue, thread = tile row (TMEM lane).
+//        1..8 = conversion and epilogue, two warps per TMEM lane quarter:
+//            thread = tile row (TMEM lane), warp half h converts K block h of
+//            the input row and applies layer 1's epilogue to hidden columns
+//            [128 h, 128 h + 128); half 0 also forms the codes.
 // Per tile i (epilogue threads):
 //   convert x(i) -> x_s      [x_ready]     MMA1: TMEM[0,256) = x W1^T
 //   epi1: h = bf16(relu(acc / 64 + b1)) -> h_s   [h_ready]   MMA2: TMEM[256,288) = h W2^T
@@ -28,7 +31,8 @@
 namespace sift {
 namespace {
 
-constexpr int kLThreads = 32 * 5;
+constexpr int kLEpiWarps = 8;  // two per TMEM lane quarter
+constexpr int kLThreads = 32 * (1 + kLEpiWarps);
 constexpr int kXKBlock = 128 * 128;                     // bytes of one K block of a 128-row BF16 tile
 constexpr int kW1Bytes = kMlpHidden * kMlpIn * 2;       // 64 KB
 constexpr int kW2Bytes = kMlpOutRows * kMlpHidden * 2;  // 16 KB
@@ -61,11 +65,11 @@ __device__ __forceinline__ uint32_t bf16x2(float a, float b) {
     return *reinterpret_cast<const uint32_t*>(&h);
 }
 
-// Row r of a u8 tile in shared memory (TMA, 128-byte swizzle; rows past the
-// end of the input are zeros) -> BF16 K blocks of x_s.
-__device__ __forceinline__ void convert_row(const uint8_t* u8_tile, int r, uint8_t* x_s) {
+// Half h of row r of a u8 tile in shared memory (TMA, 128-byte swizzle; rows
+// past the end of the input are zeros) -> BF16 K block h of x_s.
+__device__ __forceinline__ void convert_row(const uint8_t* u8_tile, int r, uint8_t* x_s, int h) {
     #pragma unroll
-    for (int c = 0; c < 8; ++c) {
+    for (int c = 4 * h; c < 4 * h + 4; ++c) {
         const uint4 v = *reinterpret_cast<const uint4*>(u8_tile + sw128_off(r, c));
         const uint32_t w[4] = {v.x, v.y, v.z, v.w};
         uint32_t o[8];
@@ -106,8 +110,8 @@ __global__ void __launch_bounds__(kLThreads, 1)
     const uint32_t bar_m2 = ptx::smem_u32(&ctl->m2), bar_drain = ptx::smem_u32(&ctl->drain);
     if (threadIdx.x == 0) {
         ptx::mbar_init(bar_w, 1);
-        ptx::mbar_init(bar_x, 128);
-        ptx::mbar_init(bar_h, 128);
+        ptx::mbar_init(bar_x, 32 * kLEpiWarps);
+        ptx::mbar_init(bar_h, 32 * kLEpiWarps);
         ptx::mbar_init(bar_m1, 1);
         ptx::mbar_init(bar_m2, 1);
         ptx::mbar_init(bar_drain, 1);
@@ -190,12 +194,13 @@ __global__ void __launch_bounds__(kLThreads, 1)
         __syncwarp();
     } else {
         const int quarter = warp & 3;
+        const int half = (warp - 1) >> 2;   // which K block / hidden half this warp handles
         const int r = quarter * 32 + lane;  // tile row = TMEM lane
         const uint32_t lane_base = static_cast<uint32_t>(quarter * 32) << 16;
         bool conv_ok = true;
         if (my_tiles > 0) {
             conv_ok = ptx::mbar_wait(bar_xf, 0, abort_flag, err, kErrWaitEpilogue);
-            if (conv_ok) convert_row(xr_s, r, x_s);
+            if (conv_ok) convert_row(xr_s, r, x_s, half);
             ptx::fence_proxy_async();
             ptx::mbar_arrive(bar_x);
         }
@@ -205,7 +210,7 @@ __global__ void __launch_bounds__(kLThreads, 1)
             if (!__all_sync(0xffffffffu, waited)) break;
             ptx::tc_fence_after();
             #pragma unroll 1
-            for (int m = 0; m < kMlpHidden / 32; ++m) {
+            for (int m = 4 * half; m < 4 * half + 4; ++m) {
                 uint32_t v[32];
                 ptx::tmem_ld32(tmem + lane_base + m * 32, v);
                 ptx::tmem_ld_wait(v);
@@ -230,10 +235,11 @@ __global__ void __launch_bounds__(kLThreads, 1)
             if (i + 1 < my_tiles) {
                 const int st = (i + 1) % kXStages;
                 conv_ok = ptx::mbar_wait(bar_xf + 8 * st, ((i + 1) / kXStages) & 1, abort_flag, err, kErrWaitEpilogue);
-                if (conv_ok) convert_row(xr_s + st * kXTileBytes, r, x_s);
+                if (conv_ok) convert_row(xr_s + st * kXTileBytes, r, x_s, half);
                 ptx::fence_proxy_async();
                 ptx::mbar_arrive(bar_x);
             }
+            if (half) continue;  // layer 2's 32 columns: half 0
             waited = ptx::mbar_wait(bar_m2, i & 1, abort_flag, err, kErrWaitEpilogue);
             if (!__all_sync(0xffffffffu, waited)) break;
             ptx::tc_fence_after();

@@ -22,10 +22,10 @@
 //
 // Candidate scan. One warp per query over its L buckets (L x P with P probe
 // codes per table: multi-probe); candidate rows are fetched by groups of 8
-// lanes with coalesced 16-byte loads (4 rows per warp-wide load) and scored as
-// |q - b|^2 = |q|^2 + |b|^2 - 2 q.b with dp4a; the per-query top-2 is
-// lexicographic in (distance, index) and counts a base point found in several
-// tables once.
+// lanes with coalesced 16-byte loads (4 rows per warp-wide load) and scored
+// as the exact |q - b|^2 (byte-wise absolute differences squared and summed
+// by dp4a); the per-query top-2 is lexicographic in (distance, index) and
+// counts a base point found in several tables once.
 #include <climits>
 #include <cfloat>
 #include <cstdint>
@@ -45,7 +45,7 @@ constexpr int kHThreads = 64 + 4 * 32;  // producer, MMA, 4 epilogue warps
 struct __align__(8) HashCtl {
     uint64_t full[kHStages], empty[kHStages];
     uint64_t pfull;
-    uint64_t tfull[2], tempty[2];
+    uint64_t tfull[4], tempty[4];
     uint64_t drain;
     uint32_t tmem_base;
     int abort_flag, no_abort;
@@ -56,11 +56,14 @@ __host__ __device__ constexpr size_t hash_smem_bytes(int P) {
 }
 
 // P = number of hyperplane rows padded to a multiple of 32 (<= 256). TMEM:
-// two accumulator buffers of P columns (rounded up to a power of two >= 32).
+// nbuf accumulator buffers of slot_cols columns (P rounded up to a power of
+// two; nbuf = 4 for P <= 128, else 2), so the MMA of tile i + nbuf - 1 can run
+// while the epilogue still reads tile i.
 __global__ void __launch_bounds__(kHThreads, 1)
     lsh_hash_kernel(const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap pmap, int n, int P,
-                    int L, int k, uint32_t tmem_cols, uint32_t* __restrict__ codes, float* __restrict__ z,
-                    int* __restrict__ err) {
+                    int L, int k, int nbuf, uint32_t slot_cols, uint32_t* __restrict__ codes,
+                    float* __restrict__ z, int* __restrict__ err) {
+    const uint32_t tmem_cols = static_cast<uint32_t>(nbuf) * slot_cols;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = ptx::smem_u32(smem_raw);
     uint8_t* smem = smem_raw + ((1024u - (raw & 1023u)) & 1023u);
@@ -81,7 +84,7 @@ __global__ void __launch_bounds__(kHThreads, 1)
             ptx::mbar_init(bar_empty + 8 * s, 1);
         }
         ptx::mbar_init(bar_pfull, 1);
-        for (int b = 0; b < 2; ++b) {
+        for (int b = 0; b < nbuf; ++b) {
             ptx::mbar_init(bar_tfull + 8 * b, 1);
             ptx::mbar_init(bar_tempty + 8 * b, 4);
         }
@@ -132,11 +135,12 @@ __global__ void __launch_bounds__(kHThreads, 1)
             const uint32_t idesc = ptx::idesc_make(2 /*S32*/, 0 /*u8*/, 1 /*s8*/, 128, nc);
             bool ok = ptx::mbar_wait(bar_pfull, 0, abort_flag, err, kErrWaitMmaFull);
             for (int i = 0; i < my_tiles && ok; ++i) {
-                const int s = i % kHStages, b = i & 1;
+                const int s = i % kHStages, b = i % nbuf;
                 if (!ptx::mbar_wait(bar_full + 8 * s, (i / kHStages) & 1, abort_flag, err, kErrWaitMmaFull)) break;
-                if (!ptx::mbar_wait(bar_tempty + 8 * b, ((i >> 1) & 1) ^ 1, abort_flag, err, kErrWaitMmaTmem)) break;
+                if (!ptx::mbar_wait(bar_tempty + 8 * b, ((i / nbuf) & 1) ^ 1, abort_flag, err, kErrWaitMmaTmem))
+                    break;
                 ptx::tc_fence_after();
-                const uint32_t d = tmem + b * (tmem_cols / 2);
+                const uint32_t d = tmem + b * slot_cols;
                 for (int ch = 0; ch < nchunk; ++ch) {
                     #pragma unroll
                     for (int kk = 0; kk < 4; ++kk)
@@ -153,11 +157,11 @@ __global__ void __launch_bounds__(kHThreads, 1)
     } else {
         const int quarter = warp & 3;
         for (int i = 0; i < my_tiles; ++i) {
-            const int b = i & 1;
-            const bool waited = ptx::mbar_wait(bar_tfull + 8 * b, (i >> 1) & 1, abort_flag, err, kErrWaitEpilogue);
+            const int b = i % nbuf;
+            const bool waited = ptx::mbar_wait(bar_tfull + 8 * b, (i / nbuf) & 1, abort_flag, err, kErrWaitEpilogue);
             if (!__all_sync(0xffffffffu, waited)) break;
             ptx::tc_fence_after();
-            const uint32_t taddr = tmem + (static_cast<uint32_t>(quarter * 32) << 16) + b * (tmem_cols / 2);
+            const uint32_t taddr = tmem + (static_cast<uint32_t>(quarter * 32) << 16) + b * slot_cols;
             const int point = (blockIdx.x + i * gridDim.x) * 128 + quarter * 32 + lane;
             uint32_t mask[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             #pragma unroll
@@ -429,11 +433,12 @@ cudaError_t launch_lsh_hash(const CUtensorMap& xmap, const CUtensorMap& pmap, in
     cudaError_t e = cudaFuncSetAttribute(lsh_hash_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    uint32_t cols = 32;
-    while (cols < static_cast<uint32_t>(2 * P)) cols <<= 1;
+    uint32_t slot = 32;
+    while (slot < static_cast<uint32_t>(P)) slot <<= 1;
+    const int nbuf = slot <= 128 ? 4 : 2;  // 512 TMEM columns
     const int tiles = (n + 127) / 128;
     const int grid = tiles < num_sms ? tiles : num_sms;
-    lsh_hash_kernel<<<grid, kHThreads, smem, stream>>>(xmap, pmap, n, P, L, k, cols, codes, z, err);
+    lsh_hash_kernel<<<grid, kHThreads, smem, stream>>>(xmap, pmap, n, P, L, k, nbuf, slot, codes, z, err);
     return cudaGetLastError();
 }
 
