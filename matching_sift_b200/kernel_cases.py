@@ -9,7 +9,10 @@ times, synchronises and exits 0. Cases and the kernel they exercise:
   pairs      exact2nn_u8_pair_batch_kernel  128 uneven image pairs, one batch plan
   lsh_hash   lsh_hash_kernel                1,000,000 rows, 8 tables x 16 bits
   lsh_scan   lsh_scan_kernel                2,560 queries, 1,000,000 rows, 4 x 16 bits
+  lsh_probe  lsh_scan_kernel                2,560 queries, 1,000,000 rows, 8 x 16 bits, 8 probes
+                                            per table (persistent index: the scan without the base hash)
   mlp_hash   mlp_hash_kernel                1,000,000 rows, MLP 128 -> 256 -> 16
+  float      exact2nn_float_pair_kernel     2,560 x 1,000,000 general float32 rows (split FP16)
 """
 from __future__ import annotations
 
@@ -20,7 +23,7 @@ import numpy as np
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=("fp16", "pairs", "lsh_hash", "lsh_scan", "mlp_hash"))
+    ap.add_argument("case", choices=("fp16", "pairs", "lsh_hash", "lsh_scan", "lsh_probe", "mlp_hash", "float"))
     ap.add_argument("--reps", type=int, default=3)
     args = ap.parse_args()
 
@@ -51,6 +54,20 @@ def main():
         qd, rd = torch.from_numpy(q).to(dev), torch.from_numpy(r).to(dev)
         planes = torch.from_numpy(datagen.quantize_planes(datagen.make_hyperplanes(16, L, seed=1))).to(dev)
         run = (lambda: ms.lsh_hash(rd, planes)) if args.case == "lsh_hash" else (lambda: ms.lsh_match(qd, rd, planes))
+    elif args.case == "lsh_probe":
+        q, r = datagen.make_workload(2560, 1_000_000, seed=0)
+        qd, rd = torch.from_numpy(q).to(dev), torch.from_numpy(r).to(dev)
+        planes = torch.from_numpy(datagen.quantize_planes(datagen.make_hyperplanes(16, 8, seed=1))).to(dev)
+        index = ms.HashIndex.lsh(rd, planes)
+        run = lambda: index.search(qd, probes=8)
+    elif args.case == "float":
+        g = torch.Generator(device=dev)
+        g.manual_seed(3)
+        rf = torch.rand((1_000_000, 128), device=dev, generator=g)
+        rf /= rf.norm(dim=1, keepdim=True)
+        qf = torch.rand((2560, 128), device=dev, generator=g)
+        qf /= qf.norm(dim=1, keepdim=True)
+        run = lambda: ms.match(qf, rf, outputs=("nn_idx",))
     else:
         # random parameters in the flat SIFT_MLP_PARAMS layout: W1, b1, W2 (32 rows), b2 (32)
         g = np.random.default_rng(1)
