@@ -697,6 +697,98 @@ int encode_i8_rows(CUtensorMap* m, const void* base, uint64_t rows, uint32_t box
     return encode_u8_rows(m, base, rows, box_rows);
 }
 
+// LSH of general float / half rows (values that are not integers times one
+// power of two): FP32 hash and scan on the CUDA cores over the caller's rows
+// (host float rows are copied to the device first); the bucketing is the u8
+// path's. Caller holds the arena lock and has checked the arguments.
+int lsh_match_float(const LshArgs& a, DeviceCtx& c, cudaStream_t st) {
+    const int q_n = static_cast<int>(a.q_n), r_n = static_cast<int>(a.r_n);
+    const int L_ = a.L, k = a.k;
+    const int top = k < kLshMaxTopBits ? k : kLshMaxTopBits;
+    const int shift = k - top, nbins = 1 << top;
+    const int flip = k < 6 ? k : 6;
+    const bool half = a.type == SIFT_HALF_DEVICE;
+    const bool host_in = a.type == SIFT_FLOAT_HOST;
+    if (!host_in && ((reinterpret_cast<uintptr_t>(a.q) & 15) || (r_n && (reinterpret_cast<uintptr_t>(a.r) & 15))))
+        return SIFT_ERR_INVALID_ARG;
+    const bool m_dev = !a.matches || is_device_accessible(a.matches);
+    const bool i_dev = !a.nn_idx || is_device_accessible(a.nn_idx);
+    const bool d_dev = !a.nn_dist || is_device_accessible(a.nn_dist);
+    const bool host_out = !(m_dev && i_dev && d_dev);
+    const bool multi = a.probes > 1;
+    Layout L;
+    const size_t o_qf = host_in ? L.take(static_cast<size_t>(q_n) * kDim * 4) : 0;
+    const size_t o_rf = host_in ? L.take(static_cast<size_t>(r_n) * kDim * 4 + 16) : 0;
+    const size_t o_pl = L.take(static_cast<size_t>(L_) * k * kDim);
+    const size_t o_cr = L.take(static_cast<size_t>(L_) * r_n * 4 + 16);
+    const size_t o_cq = L.take(static_cast<size_t>(L_) * q_n * 4);
+    const size_t o_z = multi ? L.take(static_cast<size_t>(L_) * q_n * k * 4) : 0;
+    const size_t o_pc = multi ? L.take(static_cast<size_t>(L_) * a.probes * q_n * 4) : 0;
+    const size_t o_hist = L.take(static_cast<size_t>(L_) * nbins * 4);
+    const size_t o_start = L.take(static_cast<size_t>(L_) * (nbins + 1) * 4);
+    const size_t o_order = L.take(static_cast<size_t>(L_) * r_n * 4 + 16);
+    const size_t o_ocode = L.take(static_cast<size_t>(L_) * r_n * 4 + 16);
+    const size_t o_m = (a.matches && !m_dev) ? L.take(static_cast<size_t>(q_n) * 4) : 0;
+    const size_t o_i = (a.nn_idx && !i_dev) ? L.take(static_cast<size_t>(q_n) * 8) : 0;
+    const size_t o_d = (a.nn_dist && !d_dev) ? L.take(static_cast<size_t>(q_n) * 8) : 0;
+    SIFT_TRY(ensure_arena(c, L.off));
+    char* A = c.arena;
+    const void* q_src = a.q;
+    const void* r_src = a.r;
+    if (host_in) {
+        SIFT_CUDA(cudaMemcpyAsync(A + o_qf, a.q, static_cast<size_t>(q_n) * kDim * 4, cudaMemcpyHostToDevice, st));
+        if (r_n)
+            SIFT_CUDA(cudaMemcpyAsync(A + o_rf, a.r, static_cast<size_t>(r_n) * kDim * 4, cudaMemcpyHostToDevice, st));
+        q_src = A + o_qf;
+        r_src = A + o_rf;
+    }
+    // Finite values only (the same check as the exact float path).
+    SIFT_CUDA(cudaMemsetAsync(c.d_status + 1, 0, 2 * sizeof(int), st));
+    SIFT_CUDA(launch_abs_stats(q_src, half, q_n, c.d_status + 1, c.num_sms, st));
+    SIFT_CUDA(launch_abs_stats(r_src, half, r_n, c.d_status + 1, c.num_sms, st));
+    SIFT_CUDA(cudaMemcpyAsync(c.h_status + 1, c.d_status + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SIFT_CUDA(cudaStreamSynchronize(st));
+    if (c.h_status[1] != 0) return SIFT_ERR_INVALID_ARG;
+    int8_t* pl = reinterpret_cast<int8_t*>(A + o_pl);
+    SIFT_CUDA(cudaMemcpyAsync(pl, a.planes, static_cast<size_t>(L_) * k * kDim, cudaMemcpyDefault, st));
+    uint32_t* codes_r = reinterpret_cast<uint32_t*>(A + o_cr);
+    uint32_t* codes_q = reinterpret_cast<uint32_t*>(A + o_cq);
+    float* zq = multi ? reinterpret_cast<float*>(A + o_z) : nullptr;
+    SIFT_CUDA(launch_lsh_hash_float(r_src, half, r_n, pl, L_, k, codes_r, nullptr, st));
+    SIFT_CUDA(launch_lsh_hash_float(q_src, half, q_n, pl, L_, k, codes_q, zq, st));
+    const uint32_t* probe_codes = codes_q;
+    if (multi) {
+        uint32_t* pc = reinterpret_cast<uint32_t*>(A + o_pc);
+        for (int t = 0; t < L_; ++t)
+            SIFT_CUDA(launch_probe_codes(codes_q + static_cast<size_t>(t) * q_n, zq + static_cast<size_t>(t) * q_n * k,
+                                         q_n, k, flip, a.probes, pc + static_cast<size_t>(t) * a.probes * q_n, st));
+        g_launches += L_;
+        probe_codes = pc;
+    }
+    int* start = reinterpret_cast<int*>(A + o_start);
+    int* order = reinterpret_cast<int*>(A + o_order);
+    uint32_t* ocode = reinterpret_cast<uint32_t*>(A + o_ocode);
+    SIFT_CUDA(launch_lsh_buckets(codes_r, r_n, L_, shift, nbins, reinterpret_cast<int*>(A + o_hist), start, order,
+                                 ocode, c.num_sms, st));
+    uint32_t* m_out = (a.matches && !m_dev) ? reinterpret_cast<uint32_t*>(A + o_m) : a.matches;
+    int32_t* i_out = (a.nn_idx && !i_dev) ? reinterpret_cast<int32_t*>(A + o_i) : a.nn_idx;
+    float* d_out = (a.nn_dist && !d_dev) ? reinterpret_cast<float*>(A + o_d) : a.nn_dist;
+    SIFT_CUDA(launch_lsh_scan_float(q_src, r_src, half, q_n, r_n, L_, a.probes, shift, nbins, probe_codes, start,
+                                    order, ocode, a.threshold, a.ratio ? 1 : 0, m_out, a.candidates, i_out, d_out, st));
+    g_launches += 2 + (r_n > 0 ? 1 : 0) + (r_n > 0 ? 3 : 0) + 1;
+    if (a.matches && !m_dev)
+        SIFT_CUDA(cudaMemcpyAsync(a.matches, m_out, static_cast<size_t>(q_n) * 4, cudaMemcpyDeviceToHost, st));
+    if (a.nn_idx && !i_dev)
+        SIFT_CUDA(cudaMemcpyAsync(a.nn_idx, i_out, static_cast<size_t>(q_n) * 8, cudaMemcpyDeviceToHost, st));
+    if (a.nn_dist && !d_dev)
+        SIFT_CUDA(cudaMemcpyAsync(a.nn_dist, d_out, static_cast<size_t>(q_n) * 8, cudaMemcpyDeviceToHost, st));
+    if (a.sync || host_out || host_in) {
+        SIFT_CUDA(cudaStreamSynchronize(st));
+        return collect_device_status(c, st);
+    }
+    return SIFT_OK;
+}
+
 int lsh_match(const LshArgs& a) {
     if (a.L < 1 || a.k < 1 || a.k > 32 || a.L * a.k > kLshMaxPlanes || !a.planes) return SIFT_ERR_INVALID_ARG;
     if (a.q_n > 0x7fffffffu / 32 || a.r_n > 0x7fffffffu / 32) return SIFT_ERR_INVALID_ARG;
@@ -745,7 +837,13 @@ int lsh_match(const LshArgs& a) {
     const uint8_t* qd = nullptr;
     const uint8_t* rd = nullptr;
     int vshift = 0;  // inputs were integers times 2^-vshift
-    SIFT_TRY(stage_inputs(c, A, ip, a.type, a.q, a.r, q_n, r_n, st, qd, rd, vshift));
+    {
+        const int rc = stage_inputs(c, A, ip, a.type, a.q, a.r, q_n, r_n, st, qd, rd, vshift);
+        // General float values: the same hash and scan in FP32 on the caller's rows.
+        if (rc == SIFT_ERR_NOT_INTEGER && a.type != SIFT_U8_DEVICE && a.type != SIFT_U8_HOST)
+            return lsh_match_float(a, c, st);
+        SIFT_TRY(rc);
+    }
     const int8_t* pl = a.planes;
     if (!planes_dev) {
         SIFT_CUDA(cudaMemcpyAsync(A + o_pl, a.planes, static_cast<size_t>(L_) * k * kDim, cudaMemcpyDefault, st));

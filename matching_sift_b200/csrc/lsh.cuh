@@ -38,4 +38,17 @@ cudaError_t launch_lsh_scan(const uint8_t* q, const uint8_t* r, int q_n, int r_n
                             const uint32_t* ocode, float thr, int ratio, float dist_scale, uint32_t* matches,
                             uint32_t* counts, int32_t* nn_idx, float* nn_dist, cudaStream_t stream);
 
+// General float (half = false) or half rows (lsh_float.cu): codes[t][i] bit j
+// set when the FP32 dot product of row i with planes[t * k + j] (int8,
+// [L * k][128] device, 16-byte aligned) is negative; z (optional) the dot
+// products [t][i][j].
+cudaError_t launch_lsh_hash_float(const void* x, bool half, int n, const int8_t* planes, int L, int k,
+                                  uint32_t* codes, float* z, cudaStream_t stream);
+// The candidate scan of launch_lsh_scan on float / half rows (FP32 squared
+// distances).
+cudaError_t launch_lsh_scan_float(const void* q, const void* r, bool half, int q_n, int r_n, int L, int probes,
+                                  int shift, int nbins, const uint32_t* qcodes, const int* start, const int* order,
+                                  const uint32_t* ocode, float thr, int ratio, uint32_t* matches, uint32_t* counts,
+                                  int32_t* nn_idx, float* nn_dist, cudaStream_t stream);
+
 }  // namespace sift

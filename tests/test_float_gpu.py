@@ -192,3 +192,64 @@ def test_integer_data_still_takes_the_exact_path(cuda_device):
         np.testing.assert_array_equal(out["nn_idx"].cpu().numpy().astype(np.int64), i)
         np.testing.assert_array_equal(out["nn_dist"].cpu().numpy().astype(np.float64),
                                       d.astype(np.float64) * scale * scale)
+
+
+def _fp64_lsh(q, r, planes):
+    """FP64 restatement of the LSH search on float rows: codes (bit j when the
+    dot product with plane j is negative), the members of the query's bucket
+    in each table, nearest by FP64 squared distance. Also flags, per point,
+    whether any of its dot products is so close to 0 that FP32 and FP64 may
+    disagree on the sign."""
+    L, k = planes.shape[:2]
+    q64, r64 = q.astype(np.float64), r.astype(np.float64)
+    qc, rc, amb_q, amb_r = [], [], np.zeros(len(q), bool), np.zeros(len(r), bool)
+    for t in range(L):
+        p = planes[t].astype(np.float64)
+        for x, codes, amb in ((q64, qc, amb_q), (r64, rc, amb_r)):
+            d = x @ p.T
+            bound = 1e-5 * (np.abs(x) @ np.abs(p).T)
+            amb |= (np.abs(d) <= bound).any(1)
+            codes.append(((d < 0).astype(np.int64) << np.arange(k)).sum(1))
+    nn = np.full(len(q), -1, np.int64)
+    nd = np.full(len(q), np.inf)
+    for i in range(len(q)):
+        member = np.zeros(len(r), bool)
+        for t in range(L):
+            member |= rc[t] == qc[t][i]
+        idx = np.nonzero(member)[0]
+        if len(idx):
+            d = ((r64[idx] - q64[i]) ** 2).sum(1)
+            j = np.lexsort((idx, d))[0]
+            nn[i], nd[i] = idx[j], d[j]
+    return nn, nd, amb_q, amb_r
+
+
+def test_lsh_on_general_floats(cuda_device):
+    """lsh_match / lsh_gpu on the reference benchmark's kind of data: the
+    nearest bucket member equals the FP64 restatement's, except for queries
+    whose buckets involve a point with a dot product at the FP32/FP64 sign
+    boundary; distances within the float tolerance."""
+    import torch
+
+    from matching_sift_b200 import datagen
+
+    q, r = rand_unit(400, 12), rand_unit(20000, 13)
+    L, k = 2, 10
+    planes = datagen.quantize_planes(datagen.make_hyperplanes(k, L, seed=14), 32.0)
+    qd, rd = torch.from_numpy(q).to(cuda_device), torch.from_numpy(r).to(cuda_device)
+    out = ms.lsh_match(qd, rd, torch.from_numpy(planes).to(cuda_device), threshold=0.0, candidates=True)
+    assert ms.stream_status() == ms.SIFT_OK
+    nn, nd, amb_q, amb_r = _fp64_lsh(q, r, planes)
+    got = out["nn_idx"][:, 0].cpu().numpy().astype(np.int64)
+    gd = out["nn_dist"][:, 0].cpu().numpy().astype(np.float64)
+    clear = ~amb_q & ~amb_r[np.where(nn >= 0, nn, 0)] & ~amb_r[np.where(got >= 0, got, 0)]
+    assert clear.mean() > 0.9
+    np.testing.assert_array_equal(got[clear], nn[clear])
+    ok = clear & (nn >= 0)
+    qn = (q.astype(np.float64) ** 2).sum(1)
+    assert (np.abs(gd[ok] - nd[ok]) <= TOL * 2 * qn[ok] + 1e-6).all()
+    # the reference-named entry point with rand() +/-1 planes on float rows
+    m = torch.zeros(400, dtype=torch.int32, device=cuda_device)
+    assert ms.lsh_gpu(qd, rd, ms.FLOAT_DEVICE, 400, 20000, m, 0.8, None, 2, 3, 0, 12) == ms.SIFT_OK
+    mm = m.cpu().numpy().view(np.uint32)
+    assert ((mm < 20000) | (mm == 0xFFFFFFFF)).all() and (mm < 20000).mean() > 0.5
