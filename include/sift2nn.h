@@ -130,13 +130,18 @@ SIFT_API int sift_last_status(void);
      sorted[q_n]     {d1, d2, i1, i2} as floats, FLT_MAX where absent
      nn_idx[2*q_n]   int32 nearest / second indices, -1 where absent
      nn_dist[2*q_n]  float distances under `metric`, FLT_MAX where absent
-   Float and half values must be integers in [0, 255] times one common power
+   Float and half values that are integers in [0, 255] times one common power
    of two 2^-s, s <= 24 (raw SIFT components, or the reference benchmark's
-   components / 512, src/test.cu:99-103); distances are then in the caller's
-   units (the integer results times 2^-2s), else SIFT_ERR_NOT_INTEGER.
-   SIFT_HALF_DEVICE rows are searched in place by the FP16 tensor-core kernel
-   (kind::f16, f32 accumulation, exact for such values); float rows are packed
-   to u8 for the u8 kernel.
+   components / 512, src/test.cu:99-103) are searched exactly, distances in
+   the caller's units (the integer results times 2^-2s): SIFT_HALF_DEVICE
+   rows in place by the FP16 tensor-core kernel (kind::f16, f32
+   accumulation, exact for such values), float rows packed to u8 for the u8
+   kernel. Any other finite values (e.g. the reference benchmark's default
+   unit-normalised rand() vectors) take the general float path: float rows
+   split into FP16 hi + lo parts, half rows in place, f32 accumulation on the
+   tensor cores; distances within 2^-16 (|q|^2 + |r|^2) of FP64 and index
+   swaps only among rows that close. Infinite or NaN values return
+   SIFT_ERR_INVALID_ARG.
    stream: a cudaStream_t (NULL = legacy default stream). With u8 device
    inputs and device outputs the call is asynchronous on `stream`; device-side
    problems are then reported by sift_stream_status(stream). Float / half
@@ -168,7 +173,11 @@ SIFT_API int sift_lsh_buckets(const uint32_t* codes, uint32_t n, int L, int k, i
    memory): each query is compared exactly with the base rows that share its
    code in at least one table. Outputs as sift2nn_match (nn_dist = squared
    distances; -1 / FLT_MAX where fewer than 1 / 2 candidates); matches applies
-   the ratio test when threshold > 0, else holds the nearest candidate. */
+   the ratio test when threshold > 0, else holds the nearest candidate.
+   Integer-valued rows (as sift2nn_match) are hashed and scanned exactly;
+   other finite float / half rows are hashed and scanned in FP32 on the
+   CUDA cores (a point whose dot product with a plane lies within FP32
+   rounding of 0 may land in the neighbouring bucket). */
 SIFT_API int sift_lsh_match(const void* q, const void* r, int type, uint32_t q_n, uint32_t r_n, const int8_t* planes,
                             int L, int k, float threshold, uint32_t* matches, int32_t* nn_idx, float* nn_dist,
                             void* stream);
