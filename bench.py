@@ -434,14 +434,14 @@ def main():
                 "ms_per_step": round(pk_ms, 4), "steps": v["steps"], "dtype": "u8",
                 "workload": f"{v['pairs']} image pairs, 500..8000 keypoints per side (log-uniform, seed 0), "
                             f"{v['queries']:,} query rows vs their pair's base rows, ratio test 0.8",
-                "call": "sift_batch_plan_run: one CUDA graph (norms, records, bound seeds, one persistent "
+                "call": "sift_batch_plan_run: one CUDA graph (norms, records, one persistent "
                         "exact2nn_u8_pair_batch_kernel launch over the device work list, merge)",
                 "inputs": "q + r = %.0f MB device-resident (> L2)" % (v["bytes"] / 1e6),
                 "shape": v["shape"], "tuned_ms": v["tuned_ms"],
                 "roofline": {"bound": "tensor", "achieved": round(ach, 1), "peak": round(peak_int8, 1),
                              "unit": "TFLOP/s", "frac": round(ach / peak_int8, 4), "ops_per_step": v["ops"],
-                             "note": "whole graph time (5 launches: norms, records, bound seeds, search, "
-                                     "merge), 2 ops per MAC"},
+                             "note": "whole graph time (4 launches: norms, records, search, merge), 2 ops per "
+                                     "MAC"},
                 "gpu_launches": v["launches"]}
         if "mutual" in variants:
             v = variants["mutual"]
@@ -560,8 +560,8 @@ def pairs_leg(args, ms, torch, dev, stream):
             "ops": float(ops), "bytes": float(q.nbytes + r.nbytes),
             "shape": {"qpt": info["qpt"], "qbuf": info["qbuf"]},
             "tuned_ms": [round(x, 4) for x in info["tuned_ms"]],
-            # graph replays are not counted by the library's launch counter; 5 kernels per replay
-            "launches": int(ms.lib().sift_launch_count() - launches0) + 5 * steps}
+            # graph replays are not counted by the library's launch counter; 4 kernels per replay
+            "launches": int(ms.lib().sift_launch_count() - launches0) + 4 * steps}
 
 
 def mutual_leg(args, ms, torch, dev, stream):

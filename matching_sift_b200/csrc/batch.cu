@@ -132,14 +132,12 @@ int enqueue(DeviceCtx& c, const uint8_t* q, const uint8_t* r, uint32_t r_rows, c
     int launches = 2;
     if (b.units > 0) {
         SIFT_CUDA(launch_batch_records(r, static_cast<int>(r_rows), bp, kMetricL2, m.rec, st));
-        // Each query's bound starts from a sample of its own problem's base set.
-        SIFT_CUDA(launch_seed_thresh_batch(q, r, bp, b.total_q, m.rec, m.thresh, st));
         CUtensorMap qmap, rmap;
         SIFT_TRY(detail::encode_u8_rows(&qmap, q, static_cast<uint64_t>(b.total_q), kBM));
         SIFT_TRY(detail::encode_u8_rows(&rmap, r, r_rows, kBN / 2));
         SIFT_CUDA(launch_exact2nn_u8_pair_batch(qmap, rmap, m.rec, bp, m.partial, m.thresh, c.d_status, sh.qpt,
                                                 sh.qbuf, st));
-        launches += 3;
+        launches += 2;
     }
     SIFT_CUDA(launch_merge2nn_batch(m.partial, bp, b.total_q, m.qnorm, kMetricL2, thr, 1.0f, matches, nullptr, nn_idx,
                                     nn_dist, st));

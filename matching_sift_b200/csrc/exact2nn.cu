@@ -258,55 +258,6 @@ __device__ __forceinline__ int find_item(int n_items, long long v, F key) {
     return lo;
 }
 
-// seed_thresh_kernel for the query rows of a batch: row q of problem p is
-// seeded from min(n_b, 256) sampled rows of p's own base set (records of the
-// problem's tiles from rec_off on).
-__global__ void __launch_bounds__(256) seed_thresh_batch_kernel(const uint8_t* __restrict__ q,
-                                                                const uint8_t* __restrict__ r,
-                                                                const WorkItem* __restrict__ items, int n_items,
-                                                                int total_q, const int32_t* __restrict__ rec,
-                                                                int32_t* __restrict__ thresh) {
-    const int wq = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (wq >= total_q) return;
-    const WorkItem it = items[find_item(n_items, wq, [&](int k) { return static_cast<long long>(items[k].a_off); })];
-    if (it.n_b < 2 || it.tiles <= 0) return;  // the bound stays INT_MAX
-    uint4 qv[8];
-    #pragma unroll
-    for (int c = 0; c < 8; ++c) qv[c] = __ldg(reinterpret_cast<const uint4*>(q + static_cast<size_t>(wq) * kDim) + c);
-    const int S = it.n_b < kSeedRows ? it.n_b : kSeedRows;
-    int a1 = INT_MAX, a2 = INT_MAX;
-    for (int i = lane; i < S; i += 32) {
-        const int local = static_cast<int>((static_cast<long long>(i) * it.n_b) / S);
-        const uint4* rr = reinterpret_cast<const uint4*>(r + static_cast<size_t>(it.b_off + local) * kDim);
-        uint32_t dot = 0;
-        #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const uint4 b = __ldg(rr + c);
-            dot = __dp4a(qv[c].x, b.x, dot);
-            dot = __dp4a(qv[c].y, b.y, dot);
-            dot = __dp4a(qv[c].z, b.z, dot);
-            dot = __dp4a(qv[c].w, b.w, dot);
-        }
-        const int key =
-            rec[static_cast<size_t>(it.rec_off + local / kBN) * kRecInts + local % kBN] - 2 * static_cast<int>(dot);
-        if (key < a1) {
-            a2 = a1;
-            a1 = key;
-        } else if (key < a2) {
-            a2 = key;
-        }
-    }
-    #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const int b1 = __shfl_xor_sync(0xffffffffu, a1, o), b2 = __shfl_xor_sync(0xffffffffu, a2, o);
-        const int lo = min(a1, b1);
-        a2 = min(max(a1, b1), min(a2, b2));
-        a1 = lo;
-    }
-    if (lane == 0) thresh[wq] = a2;
-}
-
 // Base-tile records of a batch: block b fills quarter b % 4 of record b / 4;
 // the record belongs to the problem whose record range holds it, and rows of
 // its base set past n_b are padding (norm kKeyPad).
@@ -756,14 +707,6 @@ cudaError_t launch_seed_thresh(const uint8_t* q, const uint8_t* r, int q_n, int 
                                int32_t* thresh, cudaStream_t stream) {
     if (q_n <= 0 || r_n < 2) return cudaSuccess;
     seed_thresh_kernel<uint8_t><<<(q_n + 7) / 8, 256, 0, stream>>>(q, r, q_n, r_n, 1.0f, rec, thresh);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_seed_thresh_batch(const uint8_t* q, const uint8_t* r, const BatchPlan& bp, int total_queries,
-                                     const int32_t* rec, int32_t* thresh, cudaStream_t stream) {
-    if (total_queries <= 0) return cudaSuccess;
-    seed_thresh_batch_kernel<<<(total_queries + 7) / 8, 256, 0, stream>>>(q, r, bp.items, bp.n_items, total_queries,
-                                                                          rec, thresh);
     return cudaGetLastError();
 }
 

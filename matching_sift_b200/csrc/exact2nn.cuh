@@ -144,10 +144,6 @@ cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, 
 // starting pruning bound for the search kernels (u8 rows; keys exact).
 cudaError_t launch_seed_thresh(const uint8_t* q, const uint8_t* r, int q_n, int r_n, const int32_t* rec,
                                int32_t* thresh, cudaStream_t stream);
-// The same for the query rows of a batch (each from its own problem's base
-// set; records as launch_batch_records writes them).
-cudaError_t launch_seed_thresh_batch(const uint8_t* q, const uint8_t* r, const BatchPlan& bp, int total_queries,
-                                     const int32_t* rec, int32_t* thresh, cudaStream_t stream);
 // The same for FP16 rows whose values times mul are integers in [0, 255].
 cudaError_t launch_seed_thresh_f16(const void* q, const void* r, int q_n, int r_n, float mul, const int32_t* rec,
                                    int32_t* thresh, cudaStream_t stream);

@@ -133,8 +133,15 @@ def test_buckets_equal_reference_lsh_thread_sort_reduce(cuda_device, family, k):
         assert (np.abs(dots[i, bits]) <= bound[i, bits]).all(), (i, bits, dots[i, bits], bound[i, bits])
     near = (np.abs(dots) <= bound).any(1)
     assert len(differ) <= int(near.sum())
+    # How tight the explanation is: the largest |dot| / sum|x_i p_i| of a
+    # differing bit, and how many points have some bit at least that close to 0.
+    rel = np.abs(dots) / np.maximum(x.astype(np.float64) @ np.abs(planes.astype(np.float64)).T, 1.0)
+    worst = max((rel[i][(int(ref_code[i]) ^ int(ours[i])) >> np.arange(k) & 1 == 1].max() for i in differ),
+                default=0.0)
+    close = int((rel <= worst).any(1).sum()) if len(differ) else 0
     print(f"{family} k={k}: {len(differ)} of {n} points hashed differently by the FP16 reference "
-          f"(points with a bit inside the FP16 bound: {int(near.sum())}); buckets {nb.value}")
+          f"(points with a bit inside the FP16 bound: {int(near.sum())}); largest |dot| / sum|x p| of a differing "
+          f"bit {worst:.2e}, points with a bit that close to 0: {close}; buckets {nb.value}")
 
     # Identical groupings apart from those points.
     keep = np.ones(n, bool)
