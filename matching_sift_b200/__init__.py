@@ -164,7 +164,9 @@ def lsh_buckets(codes, k: int, stream=None):
 
 
 def lsh_match(q, r, planes, threshold: float = 0.0, stream=None, probes: int = 1, candidates: bool = False):
-    """LSH 2-NN of uint8 CUDA tensors with int8 hyperplanes planes [L, k, 128].
+    """LSH 2-NN of CUDA tensors (uint8, float16 or float32; float values that
+    are not integers times a power of two take the FP32 hash and scan) with
+    int8 hyperplanes planes [L, k, 128].
 
     Returns {"matches", "nn_idx", "nn_dist"} like match(); only base rows
     sharing a code with the query in some table are candidates. probes > 1
@@ -175,6 +177,9 @@ def lsh_match(q, r, planes, threshold: float = 0.0, stream=None, probes: int = 1
     """
     import torch
 
+    types = {torch.uint8: U8_DEVICE, torch.float16: HALF_DEVICE, torch.float32: FLOAT_DEVICE}
+    if q.dtype != r.dtype or q.dtype not in types or not q.is_cuda or not r.is_cuda:
+        raise TypeError("lsh_match() expects two CUDA tensors of one dtype: uint8, float16 or float32")
     L, k = planes.shape[0], planes.shape[1]
     q, r, planes = q.contiguous(), r.contiguous(), planes.contiguous()
     n = q.shape[0]
@@ -184,7 +189,7 @@ def lsh_match(q, r, planes, threshold: float = 0.0, stream=None, probes: int = 1
     if candidates:
         out["candidates"] = torch.empty(n, dtype=torch.int32, device=q.device)
     s = stream if stream is not None else torch.cuda.current_stream(q.device)
-    check(lib().sift_lsh_match_probes(q.data_ptr(), r.data_ptr(), U8_DEVICE, n, r.shape[0], planes.data_ptr(), L, k,
+    check(lib().sift_lsh_match_probes(q.data_ptr(), r.data_ptr(), types[q.dtype], n, r.shape[0], planes.data_ptr(), L, k,
                                       probes, threshold, out["matches"].data_ptr(), out["nn_idx"].data_ptr(),
                                       out["nn_dist"].data_ptr(), _ptr(out.get("candidates")), s.cuda_stream),
           "sift_lsh_match_probes")

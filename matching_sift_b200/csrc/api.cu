@@ -407,11 +407,6 @@ int exact_match_chunked(const MatchArgs& a, DeviceCtx& c, cudaStream_t st) {
         SIFT_CUDA(cudaStreamWaitEvent(st, c.chunk_ev[ch], 0));
         SIFT_CUDA(launch_row_norms_u8(rd + static_cast<size_t>(off) * kDim, plans[ch].r_n, plans[ch].r_pad, a.metric,
                                       nullptr, brec + static_cast<size_t>(off / kBN) * kRecInts, nullptr, st));
-        // The first chunk's rows seed the pruning bounds of the whole search.
-        if (ch == 0) {
-            SIFT_CUDA(launch_seed_thresh(qd, rd, q_n, plans[0].r_n, brec, thresh, st));
-            ++g_launches;
-        }
         WorkItem it{};
         it.n_a = q_n;
         it.b_off = off;
@@ -631,14 +626,9 @@ int exact_match(const MatchArgs& a) {
         const float mul = ldexpf(1.0f, shift);
         SIFT_CUDA(launch_row_norms_f16(a.r, r_n, plan.r_pad, mul, a.metric, nullptr, brec, nullptr, st));
         SIFT_CUDA(launch_row_norms_f16(a.q, q_n, plan.q_pad, mul, kMetricL2, qnorm, nullptr, thresh, st));
-        SIFT_CUDA(launch_seed_thresh_f16(a.q, a.r, q_n, r_n, mul, brec, thresh, st));
-        g_launches += r_n >= 2 ? 1 : 0;
     } else {
         SIFT_CUDA(launch_row_norms_u8(rd, r_n, plan.r_pad, a.metric, nullptr, brec, nullptr, st));
         SIFT_CUDA(launch_row_norms_u8(qd, q_n, plan.q_pad, kMetricL2, qnorm, nullptr, thresh, st));
-        // Start the pruning bounds from a sample of the base rather than INT_MAX.
-        SIFT_CUDA(launch_seed_thresh(qd, rd, q_n, r_n, brec, thresh, st));
-        g_launches += r_n >= 2 ? 1 : 0;
     }
     g_launches += (plan.r_pad > 0 ? 1 : 0) + 1;
 

@@ -197,54 +197,6 @@ __global__ void __launch_bounds__(256) row_norms_float_kernel(const T* __restric
     }
 }
 
-// Seeds each query's shared pruning bound with the second-smallest key
-// (norm(b) - 2 q.b, exact integers, the search kernel's own keys) over a
-// fixed sample of base rows: an upper bound of the query's final
-// second-best key, so the search prunes from its first base tile instead of
-// starting from INT_MAX. One warp per query; lane l scores the sample rows
-// l, l + 32, ... (sample i is base row floor(i * r_n / S), S = min(r_n, 256)).
-constexpr int kSeedRows = 256;
-template <typename T>
-__global__ void __launch_bounds__(256) seed_thresh_kernel(const T* __restrict__ q, const T* __restrict__ r, int q_n,
-                                                          int r_n, float mul, const int32_t* __restrict__ rec,
-                                                          int32_t* __restrict__ thresh) {
-    const int wq = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (wq >= q_n) return;
-    uint4 qv[8];
-    #pragma unroll
-    for (int c = 0; c < 8; ++c) qv[c] = load16_u8(q, wq, c, mul);
-    const int S = r_n < kSeedRows ? r_n : kSeedRows;
-    int a1 = INT_MAX, a2 = INT_MAX;  // two smallest keys of this lane's samples
-    for (int i = lane; i < S; i += 32) {
-        const int row = static_cast<int>((static_cast<long long>(i) * r_n) / S);
-        uint32_t dot = 0;
-        #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const uint4 b = load16_u8(r, row, c, mul);
-            dot = __dp4a(qv[c].x, b.x, dot);
-            dot = __dp4a(qv[c].y, b.y, dot);
-            dot = __dp4a(qv[c].z, b.z, dot);
-            dot = __dp4a(qv[c].w, b.w, dot);
-        }
-        const int key = rec[static_cast<size_t>(row / kBN) * kRecInts + row % kBN] - 2 * static_cast<int>(dot);
-        if (key < a1) {
-            a2 = a1;
-            a1 = key;
-        } else if (key < a2) {
-            a2 = key;
-        }
-    }
-    #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const int b1 = __shfl_xor_sync(0xffffffffu, a1, o), b2 = __shfl_xor_sync(0xffffffffu, a2, o);
-        const int lo = min(a1, b1);
-        a2 = min(max(a1, b1), min(a2, b2));
-        a1 = lo;
-    }
-    if (lane == 0) thresh[wq] = a2;  // INT_MAX when fewer than two samples
-}
-
 // Largest k with key(items[k]) <= v over a non-decreasing key; empty
 // problems share the key of the problem after them, so the match is the
 // problem that owns v.
@@ -702,22 +654,6 @@ ExactPlan make_exact_plan(int q_n, int r_n, int num_sms, int parts, int group_ti
 }
 
 size_t exact2nn_smem_bytes() { return kSmemBytes; }
-
-cudaError_t launch_seed_thresh(const uint8_t* q, const uint8_t* r, int q_n, int r_n, const int32_t* rec,
-                               int32_t* thresh, cudaStream_t stream) {
-    if (q_n <= 0 || r_n < 2) return cudaSuccess;
-    seed_thresh_kernel<uint8_t><<<(q_n + 7) / 8, 256, 0, stream>>>(q, r, q_n, r_n, 1.0f, rec, thresh);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_seed_thresh_f16(const void* q, const void* r, int q_n, int r_n, float mul, const int32_t* rec,
-                                   int32_t* thresh, cudaStream_t stream) {
-    if (q_n <= 0 || r_n < 2) return cudaSuccess;
-    seed_thresh_kernel<__half><<<(q_n + 7) / 8, 256, 0, stream>>>(static_cast<const __half*>(q),
-                                                                  static_cast<const __half*>(r), q_n, r_n, mul, rec,
-                                                                  thresh);
-    return cudaGetLastError();
-}
 
 cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* norm, int32_t* rec,
                                 int32_t* thresh, cudaStream_t stream) {

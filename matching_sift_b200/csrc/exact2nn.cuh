@@ -139,14 +139,6 @@ cudaError_t launch_merge2nn_float(const int4* partial, const ExactPlan& plan, in
 //                                     pruning bound of the search kernel)
 cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* norm, int32_t* rec,
                                 int32_t* thresh, cudaStream_t stream);
-// Seeds thresh[q] (q < q_n) with the second-smallest search key of query q
-// over a fixed sample of min(r_n, 256) base rows (norms from rec): a valid
-// starting pruning bound for the search kernels (u8 rows; keys exact).
-cudaError_t launch_seed_thresh(const uint8_t* q, const uint8_t* r, int q_n, int r_n, const int32_t* rec,
-                               int32_t* thresh, cudaStream_t stream);
-// The same for FP16 rows whose values times mul are integers in [0, 255].
-cudaError_t launch_seed_thresh_f16(const void* q, const void* r, int q_n, int r_n, float mul, const int32_t* rec,
-                                   int32_t* thresh, cudaStream_t stream);
 // The same for FP16 rows whose values times mul (a power of two) are
 // integers in [0, 255].
 cudaError_t launch_row_norms_f16(const void* x, int n, int n_pad, float mul, int metric, int32_t* norm, int32_t* rec,

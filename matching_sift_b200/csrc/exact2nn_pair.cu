@@ -424,6 +424,11 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
         int split = 0, q = 0;
         bool active = false, valid = false, open = false;
         bool new_group = true;
+        // The query's shared bound is read one unit of this warp ahead: the
+        // value used for unit n was loaded while unit n - 2 was scanned, so
+        // the L2 round trip never waits in front of the first chunk. An older
+        // value is still a valid bound (bounds only decrease).
+        int next_thr = INT_MAX;
 
         for (int n = 0; n < n_units; ++n) {
             if (new_group) {
@@ -438,10 +443,12 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                 active = __any_sync(0xffffffffu, valid);
                 split = pair - plan_cta_of(cur.group_first_unit(), W, G);
                 q = cur.it.a_off + q_local;
+                next_thr = valid ? __ldcg(thresh + q) : INT_MAX;
             }
             const int j = cur.j;
             if ((n & 1) == buf) {
-                const int shared_thr = valid ? __ldcg(thresh + q) : INT_MAX;
+                const int shared_thr = next_thr;
+                next_thr = valid ? __ldcg(thresh + q) : INT_MAX;
                 const int s = n % kPStages;
                 const uint32_t rpar = (n / kPStages) & 1, tpar = (static_cast<uint32_t>(n) >> 1) & 1;
                 // Both tests are issued back to back so their latencies overlap.

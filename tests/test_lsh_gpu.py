@@ -101,7 +101,8 @@ def test_buckets_equal_reference_lsh_thread_sort_reduce(cuda_device, family, k):
     index = np.zeros(n, np.int32)
     buckets = np.zeros(2 * n, np.int32)
     nb = ctypes.c_int(0)
-    rc = ref.ref_lsh_buckets(x.astype(np.float16).ctypes.data, n, pl16.ctypes.data, k, code.ctypes.data,
+    x16 = np.ascontiguousarray(x.astype(np.float16))  # held for the call: a temporary would be freed first
+    rc = ref.ref_lsh_buckets(x16.ctypes.data, n, pl16.ctypes.data, k, code.ctypes.data,
                              index.ctypes.data, buckets.ctypes.data, ctypes.byref(nb))
     assert rc == 0
     ref_code = code.view(np.uint32)
