@@ -95,117 +95,71 @@ __device__ __forceinline__ void scan_group(const uint32_t (&v)[32], int row0, co
     }
 }
 
-// Accumulator kinds of scan16.
+// Accumulator kinds of bound16 / exact8.
 enum AccKind : int {
     kAccS32 = 0,    // s32 dot products (u8 kernel)
     kAccF32Int = 1, // f32 accumulators holding integer dot products / dscale (FP16 kernel)
     kAccFloat = 2,  // f32 dot products of general floats (float keys, float norms)
 };
 
-// The pruned scan of 16 consecutive base rows [row0, row0 + 16): the two
-// 8-row subgroups of scan_group (same bounds, same keys), so an epilogue can
-// work through a TMEM slot in 16-column chunks while the next chunk loads.
-// nrm: the 16 norms, gm8: the two 8-row minima (8-byte aligned).
+// The pruned scan of a TMEM slot in two passes, so that an epilogue can bound
+// every 8-row subgroup with no vote and no branch and form exact keys only
+// where a bound passes.
+//
+// bound16: the pass bits of the chunk's two 8-row subgroups (bit k set when
+// subgroup k's lower bound, the 8-row minimum gm8[k] minus twice the largest
+// q.b of its rows, is within thr; the same bound as scan_group). gm8: the two
+// 8-row minima (8-byte aligned).
 template <int KIND>
-__device__ __forceinline__ void scan16(const uint32_t (&v)[16], int row0, const int32_t* nrm, const int32_t* gm8,
-                                       Top2& s, float dscale) {
+__device__ __forceinline__ uint32_t bound16(const uint32_t (&v)[16], const int32_t* gm8, int thr, float dscale) {
     const int2 g8 = *reinterpret_cast<const int2*>(gm8);
-    int bnd[2];
+    uint32_t bits = 0;
     #pragma unroll
     for (int k = 0; k < 2; ++k) {
         const int g = k ? g8.y : g8.x;
+        int bnd;
         if constexpr (KIND == kAccFloat) {
             float m = __uint_as_float(v[8 * k]);
             #pragma unroll
             for (int e = 1; e < 8; ++e) m = fmaxf(m, __uint_as_float(v[8 * k + e]));
-            bnd[k] = float_key(fmaf(-2.0f, m, __int_as_float(g)));
+            bnd = float_key(fmaf(-2.0f, m, __int_as_float(g)));
         } else {
             int m = max8(v + 8 * k);
             if constexpr (KIND == kAccF32Int) m = f32_dot(static_cast<uint32_t>(m), dscale);
-            bnd[k] = g - 2 * m;
+            bnd = g - 2 * m;
         }
+        bits |= (bnd <= thr ? 1u : 0u) << k;
     }
-    if (__any_sync(0xffffffffu, min(bnd[0], bnd[1]) <= s.thr)) {
-        #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const bool ps = bnd[k] <= s.thr;
-            if (__any_sync(0xffffffffu, ps)) {
-                if (ps) {
-                    const int4 na = *reinterpret_cast<const int4*>(nrm + 8 * k);
-                    const int4 nb = *reinterpret_cast<const int4*>(nrm + 8 * k + 4);
-                    const int nr[8] = {na.x, na.y, na.z, na.w, nb.x, nb.y, nb.z, nb.w};
-                    int key[8];
-                    #pragma unroll
-                    for (int e = 0; e < 8; ++e) {
-                        if constexpr (KIND == kAccFloat)
-                            key[e] = float_key(fmaf(-2.0f, __uint_as_float(v[8 * k + e]), __int_as_float(nr[e])));
-                        else if constexpr (KIND == kAccF32Int)
-                            key[e] = nr[e] - 2 * f32_dot(v[8 * k + e], dscale);
-                        else
-                            key[e] = nr[e] - 2 * static_cast<int>(v[8 * k + e]);
-                    }
-                    int mk = __vimin3_s32(key[0], key[1], key[2]);
-                    mk = __vimin3_s32(mk, key[3], key[4]);
-                    mk = __vimin3_s32(mk, key[5], key[6]);
-                    mk = min(mk, key[7]);
-                    if (mk <= s.thr) {
-                        const int base = row0 + 8 * k;
-                        #pragma unroll
-                        for (int e = 0; e < 8; ++e) top2_update(s, key[e], base + e);
-                    }
-                }
-            }
-        }
-    }
+    return bits;
 }
 
-// The same pruned scan for general float rows: v[c] = q.b(row0 + c) as f32
-// accumulators (any sign), nrm / gm8 the record's float norms and 8-row
-// minima (bit patterns). Keys are fma(-2, q.b, |b|^2) mapped by float_key;
-// the bound of a subgroup fma(-2, max q.b, min |b|^2) is computed with the same
-// single rounding, and rounding to nearest is monotone, so the bound never
-// exceeds a computed key of its rows: pruning drops no candidate.
-__device__ __forceinline__ void scan_group_float(const uint32_t (&v)[32], int row0, const int32_t* nrm,
-                                                 const int32_t* gm8, Top2& s) {
-    float mx[4];
+// exact8: the exact keys of one 8-row subgroup [row0, row0 + 8) (v: its
+// accumulators, nrm: its 8 norms, 16-byte aligned); they update the running
+// top-2 only when their minimum is within the thread's current threshold (a
+// key above it cannot reach the final top-2).
+template <int KIND>
+__device__ __forceinline__ void exact8(const uint32_t (&v)[8], int row0, const int32_t* nrm, Top2& s,
+                                       float dscale) {
+    const int4 na = *reinterpret_cast<const int4*>(nrm);
+    const int4 nb = *reinterpret_cast<const int4*>(nrm + 4);
+    const int nr[8] = {na.x, na.y, na.z, na.w, nb.x, nb.y, nb.z, nb.w};
+    int key[8];
     #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        float m = __uint_as_float(v[8 * k]);
-        #pragma unroll
-        for (int e = 1; e < 8; ++e) m = fmaxf(m, __uint_as_float(v[8 * k + e]));
-        mx[k] = m;
+    for (int e = 0; e < 8; ++e) {
+        if constexpr (KIND == kAccFloat)
+            key[e] = float_key(fmaf(-2.0f, __uint_as_float(v[e]), __int_as_float(nr[e])));
+        else if constexpr (KIND == kAccF32Int)
+            key[e] = nr[e] - 2 * f32_dot(v[e], dscale);
+        else
+            key[e] = nr[e] - 2 * static_cast<int>(v[e]);
     }
-    const int4 g8 = *reinterpret_cast<const int4*>(gm8);
-    const int bnd[4] = {float_key(fmaf(-2.0f, mx[0], __int_as_float(g8.x))),
-                        float_key(fmaf(-2.0f, mx[1], __int_as_float(g8.y))),
-                        float_key(fmaf(-2.0f, mx[2], __int_as_float(g8.z))),
-                        float_key(fmaf(-2.0f, mx[3], __int_as_float(g8.w)))};
-    const int bmin = min(__vimin3_s32(bnd[0], bnd[1], bnd[2]), bnd[3]);
-    if (__any_sync(0xffffffffu, bmin <= s.thr)) {
+    int mk = __vimin3_s32(key[0], key[1], key[2]);
+    mk = __vimin3_s32(mk, key[3], key[4]);
+    mk = __vimin3_s32(mk, key[5], key[6]);
+    mk = min(mk, key[7]);
+    if (mk <= s.thr) {
         #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const bool ps = bnd[k] <= s.thr;
-            if (__any_sync(0xffffffffu, ps)) {
-                if (ps) {
-                    const int4 na = *reinterpret_cast<const int4*>(nrm + 8 * k);
-                    const int4 nb = *reinterpret_cast<const int4*>(nrm + 8 * k + 4);
-                    const int nr[8] = {na.x, na.y, na.z, na.w, nb.x, nb.y, nb.z, nb.w};
-                    int key[8];
-                    #pragma unroll
-                    for (int e = 0; e < 8; ++e)
-                        key[e] = float_key(fmaf(-2.0f, __uint_as_float(v[8 * k + e]), __int_as_float(nr[e])));
-                    int mk = __vimin3_s32(key[0], key[1], key[2]);
-                    mk = __vimin3_s32(mk, key[3], key[4]);
-                    mk = __vimin3_s32(mk, key[5], key[6]);
-                    mk = min(mk, key[7]);
-                    if (mk <= s.thr) {
-                        const int base = row0 + 8 * k;
-                        #pragma unroll
-                        for (int e = 0; e < 8; ++e) top2_update(s, key[e], base + e);
-                    }
-                }
-            }
-        }
+        for (int e = 0; e < 8; ++e) top2_update(s, key[e], row0 + e);
     }
 }
 

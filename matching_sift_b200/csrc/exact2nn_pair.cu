@@ -465,30 +465,44 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                     const int32_t* rec = r_smem + s * kRecInts;
                     constexpr int kKind = MODE == kModeFloat ? kAccFloat : (F16 ? kAccF32Int : kAccS32);
                     const int row0 = cur.it.idx_base + j * kBN;
-                    // The slot's 128 columns in 8 chunks of 16: chunk c + 1 loads
-                    // while chunk c is scanned, so the slot is handed back as soon
-                    // as the last chunk is in registers.
+                    // Two passes over the slot's 128 columns (8 chunks of 16).
+                    // The first bounds every 8-row subgroup against the
+                    // threshold held at its start, with no vote and no branch,
+                    // while chunk c + 1 loads; the second forms exact keys
+                    // only in chunks where some lane's bound passed, reading
+                    // them from the slot again (still held). Then the slot is
+                    // handed back.
                     uint32_t va[16], vb[16];
-                    auto scan = [&](const uint32_t (&v)[16], int c) {
-                        scan16<kKind>(v, row0 + 16 * c, rec + 16 * c, rec + 128 + 2 * c, st, dscale);
-                    };
+                    const int thr0 = st.thr;
+                    uint32_t pass = 0;  // bit 2 c + k: subgroup k of chunk c may hold a candidate
                     ptx::tmem_ld16(taddr, va);
                     ptx::tmem_ld_wait(va);
                     #pragma unroll
                     for (int c = 1; c < 8; c += 2) {
                         ptx::tmem_ld16(taddr + 16 * c, vb);
-                        scan(va, c - 1);
+                        pass |= bound16<kKind>(va, rec + kBN + 2 * (c - 1), thr0, dscale) << (2 * (c - 1));
                         ptx::tmem_ld_wait(vb);
                         if (c + 1 < 8) {
                             ptx::tmem_ld16(taddr + 16 * (c + 1), va);
-                            scan(vb, c);
+                            pass |= bound16<kKind>(vb, rec + kBN + 2 * c, thr0, dscale) << (2 * c);
                             ptx::tmem_ld_wait(va);
                         }
+                    }
+                    pass |= bound16<kKind>(vb, rec + kBN + 14, thr0, dscale) << 14;
+                    // Subgroups in increasing order, so the top-2 still sees
+                    // the rows in index order (ties keep the lower index).
+                    uint32_t todo = __reduce_or_sync(0xffffffffu, pass);
+                    while (todo) {
+                        const int g = __ffs(todo) - 1;
+                        todo &= todo - 1;
+                        uint32_t v8[8];
+                        ptx::tmem_ld8(taddr + 8 * g, v8);
+                        ptx::tmem_ld_wait(v8);
+                        if ((pass >> g) & 1u) exact8<kKind>(v8, row0 + 8 * g, rec + 8 * g, st, dscale);
                     }
                     ptx::tc_fence_before();
                     __syncwarp();
                     if (lane == 0) ptx::mbar_arrive_cluster_relaxed(lead_tempty);
-                    scan(vb, 7);
                     if (valid && st.k2 < published) {
                         atomicMin(thresh + q, st.k2);
                         published = st.k2;

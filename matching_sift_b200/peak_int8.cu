@@ -5,7 +5,10 @@
 // in shared memory, one thread issuing back-to-back tcgen05.mma.kind::i8 with
 // K = 32 into TMEM, then one commit + bounded wait. MODE adds, per group of 4
 // MMAs: 1 = a tcgen05.commit, 2 = + tcgen05.fence::after_thread_sync,
-// 3 = + an mbarrier.try_wait on an already completed phase.
+// 3 = + an mbarrier.try_wait on an already completed phase. ISSUERS = 2 splits
+// the same MMAs between two threads (lane 0 of warps 0 and 1, each with its
+// own half of TMEM and its own barriers): whether a second issuing thread
+// hides the first one's synchronisation.
 // The MAC/clk/SM figure of MODE 0 is the roofline denominator bench.py uses.
 //
 //   make -C matching_sift_b200 peak && matching_sift_b200/peak_int8
@@ -16,12 +19,12 @@
 
 using namespace sift;
 
-template <int M, int N, bool PAIR, int MODE>
+template <int M, int N, bool PAIR, int MODE, int ISSUERS>
 __global__ void __launch_bounds__(128, 1) bench_kernel(int iters, unsigned long long* cycles) {
     extern __shared__ __align__(1024) uint8_t sm[];
     uint8_t* base = sm + ((1024 - (ptx::smem_u32(sm) & 1023)) & 1023);
-    __shared__ uint64_t bar;
-    __shared__ uint64_t side[4];
+    __shared__ uint64_t bar[2];
+    __shared__ uint64_t side[2][4];
     __shared__ uint32_t tbase;
     __shared__ int flag_abort, flag_err;
     const int warp = threadIdx.x >> 5;
@@ -30,8 +33,10 @@ __global__ void __launch_bounds__(128, 1) bench_kernel(int iters, unsigned long 
         reinterpret_cast<uint4*>(base)[i] = make_uint4(0, 0, 0, 0);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (threadIdx.x == 0) {
-        ptx::mbar_init(ptx::smem_u32(&bar), 1);
-        for (int i = 0; i < 4; ++i) ptx::mbar_init(ptx::smem_u32(&side[i]), 1);
+        for (int w = 0; w < 2; ++w) {
+            ptx::mbar_init(ptx::smem_u32(&bar[w]), 1);
+            for (int i = 0; i < 4; ++i) ptx::mbar_init(ptx::smem_u32(&side[w][i]), 1);
+        }
         ptx::fence_mbar_init(); flag_abort = 0; flag_err = 0;
     }
     if (warp == 0) {
@@ -45,26 +50,29 @@ __global__ void __launch_bounds__(128, 1) bench_kernel(int iters, unsigned long 
     const uint32_t tmem = tbase;
     const uint32_t rank = PAIR ? ptx::cluster_ctarank() : 0;
     unsigned long long t0 = clock64();
-    if (threadIdx.x == 0 && rank == 0) {
+    if ((threadIdx.x & 31) == 0 && warp < ISSUERS && rank == 0) {
         const uint32_t a0 = ptx::smem_u32(base), b0 = a0 + 128 * 128;
         const uint64_t ad = ptx::sdesc_sw128(a0), bd = ptx::sdesc_sw128(b0);
         constexpr uint32_t idesc = ptx::idesc_make(2, 0, 0, M, N);
-        for (int i = 0; i < iters; ++i) {
+        constexpr uint32_t width = 512 / ISSUERS;  // TMEM columns of this issuer
+        static_assert(N <= width, "accumulator wider than the issuer's TMEM share");
+        const uint32_t col0 = warp * width;
+        for (int i = 0; i < iters / ISSUERS; ++i) {
             const uint32_t k = i & 3;
-            const uint32_t d = tmem + (((i >> 2) & 1) ? (512 - N) : 0);
-            if (MODE >= 3 && k == 0) (void)ptx::mbar_try_wait(ptx::smem_u32(&side[(i >> 2) & 3]), 1);  // a completed phase
+            const uint32_t d = tmem + col0 + (((i >> 2) & 1) ? (width - N) : 0);
+            if (MODE >= 3 && k == 0) (void)ptx::mbar_try_wait(ptx::smem_u32(&side[warp][(i >> 2) & 3]), 1);  // a completed phase
             if (MODE >= 2 && k == 0) ptx::tc_fence_after();
             if (PAIR) ptx::mma_i8_pair(d, ad + 2 * k, bd + 2 * k, idesc, k > 0);
             else ptx::mma_i8(d, ad + 2 * k, bd + 2 * k, idesc, k > 0);
             if (MODE >= 1 && k == 3) {
-                if (PAIR) ptx::tc_commit_pair(ptx::smem_u32(&side[(i >> 2) & 3]));
-                else ptx::tc_commit(ptx::smem_u32(&side[(i >> 2) & 3]));
+                if (PAIR) ptx::tc_commit_pair(ptx::smem_u32(&side[warp][(i >> 2) & 3]));
+                else ptx::tc_commit(ptx::smem_u32(&side[warp][(i >> 2) & 3]));
             }
         }
-        if (PAIR) ptx::tc_commit_pair(ptx::smem_u32(&bar)); else ptx::tc_commit(ptx::smem_u32(&bar));
-        ptx::mbar_wait(ptx::smem_u32(&bar), 0, &flag_abort, &flag_err, 1);
+        if (PAIR) ptx::tc_commit_pair(ptx::smem_u32(&bar[warp])); else ptx::tc_commit(ptx::smem_u32(&bar[warp]));
+        ptx::mbar_wait(ptx::smem_u32(&bar[warp]), 0, &flag_abort, &flag_err, 1);
     }
-    __syncwarp();
+    __syncthreads();
     unsigned long long t1 = clock64();
     if (threadIdx.x == 0 && rank == 0) atomicAdd(cycles, t1 - t0);
     ptx::tc_fence_before();
@@ -76,9 +84,9 @@ __global__ void __launch_bounds__(128, 1) bench_kernel(int iters, unsigned long 
     }
 }
 
-template <int M, int N, bool PAIR, int MODE = 0>
+template <int M, int N, bool PAIR, int MODE = 0, int ISSUERS = 1>
 void run(const char* name, int sms) {
-    auto k = bench_kernel<M, N, PAIR, MODE>;
+    auto k = bench_kernel<M, N, PAIR, MODE, ISSUERS>;
     size_t smem = 1024 + 128 * 128 + 256 * 128;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     unsigned long long* d; cudaMalloc(&d, 8);
@@ -118,5 +126,8 @@ int main() {
     run<128, 128, false, 3>("1cta N128 +trywait", sms);
     run<256, 128, true, 1>("pair N128 +commit", sms);
     run<256, 128, true, 3>("pair N128 +all", sms);
+    run<256, 128, true, 1, 2>("pair N128 +commit x2", sms);
+    run<256, 128, true, 3, 2>("pair N128 +all x2", sms);
+    run<128, 128, false, 3, 2>("1cta N128 +all x2", sms);
     return 0;
 }
