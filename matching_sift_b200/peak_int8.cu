@@ -11,6 +11,9 @@
 // hides the first one's synchronisation.
 // The MAC/clk/SM figure of MODE 0 is the roofline denominator bench.py uses.
 //
+// chain_kernel below measures the accumulator hand-off between the MMA issuer
+// and the epilogue warps.
+//
 //   make -C matching_sift_b200 peak && matching_sift_b200/peak_int8
 #include <cstdio>
 #include <cstdint>
@@ -114,6 +117,127 @@ void run(const char* name, int sms) {
     }
 }
 
+// Accumulator hand-off chain of the search kernels: one MMA issuer (lane 0
+// of warp 0 of the leader CTA) and EW epilogue warps in each CTA of a pair,
+// NB TMEM slots of 128 columns used round robin. Per step the issuer waits
+// for the slot's free barrier, issues 4 MMAs (M256 N128 K32, 256 cycles of
+// tensor work) and commits to the slot's ready barrier in both CTAs; each
+// epilogue warp waits for ready, reads its lane quarter of the slot (READ:
+// 8 loads of 16 columns) and arrives on the leader's free barrier. Cycles
+// per step = max(256, hand-off latency / NB). CTA_WAIT: waits with CTA scope
+// instead of cluster scope. ISSUERS = 2: lane 0 of warp 1 issues the odd
+// steps (slots of odd index). HOLD: cycles an epilogue warp spends after its
+// reads before handing the slot back (the scan of a search kernel).
+template <int NB, int EW, bool READ, bool CTA_WAIT, int ISSUERS = 1, int HOLD = 0>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
+    chain_kernel(int iters, unsigned long long* cycles, unsigned* sink) {
+    extern __shared__ __align__(1024) uint8_t sm[];
+    uint8_t* base = sm + ((1024 - (ptx::smem_u32(sm) & 1023)) & 1023);
+    __shared__ uint64_t ready[NB], freeb[NB], drain[2];
+    __shared__ uint32_t tbase;
+    __shared__ int flag_abort, flag_err;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = threadIdx.x; i < (128 * 128 + 64 * 128) / 16; i += blockDim.x)
+        reinterpret_cast<uint4*>(base)[i] = make_uint4(0, 0, 0, 0);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < NB; ++b) {
+            ptx::mbar_init(ptx::smem_u32(&ready[b]), 1);
+            ptx::mbar_init(ptx::smem_u32(&freeb[b]), 2 * EW);
+        }
+        ptx::mbar_init(ptx::smem_u32(&drain[0]), 1);
+        ptx::mbar_init(ptx::smem_u32(&drain[1]), 1);
+        ptx::fence_mbar_init();
+        flag_abort = 0;
+        flag_err = 0;
+    }
+    if (warp == 0) {
+        ptx::tmem_alloc_pair(ptx::smem_u32(&tbase), 512);
+        ptx::tmem_relinquish_pair();
+    }
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::cluster_sync();
+    ptx::tc_fence_after();
+    const uint32_t tmem = tbase;
+    const uint32_t rank = ptx::cluster_ctarank();
+    auto wait = [&](uint32_t bar, uint32_t par) {
+        return CTA_WAIT ? ptx::mbar_wait(bar, par, &flag_abort, &flag_err, 1)
+                        : ptx::mbar_wait_cluster(bar, par, &flag_abort, &flag_err, 1);
+    };
+    const unsigned long long t0 = clock64();
+    if (warp < ISSUERS && lane == 0 && rank == 0) {
+        const uint32_t a0 = ptx::smem_u32(base), b0 = a0 + 128 * 128;
+        const uint64_t ad = ptx::sdesc_sw128(a0), bd = ptx::sdesc_sw128(b0);
+        constexpr uint32_t idesc = ptx::idesc_make(2, 0, 0, 256, 128);
+        for (int i = warp; i < iters; i += ISSUERS) {
+            const int b = i % NB, k = i / NB;
+            if (k > 0 && !wait(ptx::smem_u32(&freeb[b]), (k - 1) & 1)) break;
+            ptx::tc_fence_after();
+            for (int kk = 0; kk < 4; ++kk) ptx::mma_i8_pair(tmem + b * 128, ad + 2 * kk, bd + 2 * kk, idesc, kk > 0);
+            ptx::tc_commit_pair_mc(ptx::smem_u32(&ready[b]), 0x3);
+        }
+        ptx::tc_commit_pair(ptx::smem_u32(&drain[warp]));
+        ptx::mbar_wait(ptx::smem_u32(&drain[warp]), 0, &flag_abort, &flag_err, 1);
+    } else if (warp >= 2 && warp < 2 + EW) {
+        const uint32_t quarter = warp & 3;
+        unsigned acc = 0;
+        for (int i = 0; i < iters; ++i) {
+            const int b = i % NB, k = i / NB;
+            if (!__all_sync(0xffffffffu, wait(ptx::smem_u32(&ready[b]), k & 1))) break;
+            ptx::tc_fence_after();
+            if (READ) {
+                uint32_t v[16];
+                for (int c = 0; c < 8; ++c) {
+                    ptx::tmem_ld16(tmem + (quarter * 32 << 16) + b * 128 + 16 * c, v);
+                    ptx::tmem_ld_wait(v);
+                    acc ^= v[0] ^ v[15];
+                }
+            }
+            if (HOLD > 0) {
+                const long long h0 = clock64();
+                while (clock64() - h0 < HOLD) {}
+            }
+            ptx::tc_fence_before();
+            __syncwarp();
+            if (lane == 0) ptx::mbar_arrive_cluster_relaxed(ptx::mapa(ptx::smem_u32(&freeb[b]), 0));
+        }
+        if (acc == 0x12345678u) sink[0] = acc;
+    }
+    ptx::tc_fence_before();
+    __syncthreads();
+    ptx::cluster_sync();
+    const unsigned long long t1 = clock64();
+    if (threadIdx.x == 0 && rank == 0) atomicAdd(cycles, t1 - t0);
+    if (threadIdx.x == 0 && flag_err) atomicAdd(cycles + 1, 1ull);
+    if (warp == 0) {
+        ptx::tc_fence_after();
+        ptx::tmem_dealloc_pair(tmem, 512);
+    }
+}
+
+template <int NB, int EW, bool READ, bool CTA_WAIT, int ISSUERS = 1, int HOLD = 0>
+void run_chain(const char* name, int sms) {
+    auto k = chain_kernel<NB, EW, READ, CTA_WAIT, ISSUERS, HOLD>;
+    const size_t smem = 1024 + 128 * 128 + 64 * 128;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    unsigned long long* d;
+    unsigned* sink;
+    cudaMalloc(&d, 16);
+    cudaMalloc(&sink, 4);
+    const int iters = 20000;
+    for (int rep = 0; rep < 2; ++rep) {
+        cudaMemset(d, 0, 16);
+        k<<<sms, 192, smem>>>(iters, d, sink);
+        if (cudaDeviceSynchronize() != cudaSuccess) { printf("%s launch error\n", name); return; }
+        unsigned long long c[2];
+        cudaMemcpy(c, d, 16, cudaMemcpyDeviceToHost);
+        printf("%-34s cycles/step %7.1f (MMA work 256)  timeouts %llu\n", name, (double)c[0] / (sms / 2) / iters, c[1]);
+    }
+    cudaFree(d);
+    cudaFree(sink);
+}
+
 int main() {
     int sms; cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
     run<128, 64, false, 0>("1cta M128 N64", sms);
@@ -129,5 +253,17 @@ int main() {
     run<256, 128, true, 1, 2>("pair N128 +commit x2", sms);
     run<256, 128, true, 3, 2>("pair N128 +all x2", sms);
     run<128, 128, false, 3, 2>("1cta N128 +all x2", sms);
+    run_chain<2, 1, false, false>("chain NB2 1 warp, no read", sms);
+    run_chain<2, 4, false, false>("chain NB2 4 warps, no read", sms);
+    run_chain<2, 4, false, true>("chain NB2 4 warps, no read, cta", sms);
+    run_chain<2, 4, true, false>("chain NB2 4 warps, read", sms);
+    run_chain<2, 4, true, true>("chain NB2 4 warps, read, cta", sms);
+    run_chain<4, 4, true, false>("chain NB4 4 warps, read", sms);
+    run_chain<3, 4, true, false>("chain NB3 4 warps, read", sms);
+    run_chain<2, 4, true, false, 2>("chain NB2 read, 2 issuers", sms);
+    run_chain<4, 4, true, false, 2>("chain NB4 read, 2 issuers", sms);
+    run_chain<4, 4, true, false, 2, 400>("chain NB4 read, 2 issuers, hold 400", sms);
+    run_chain<4, 4, true, false, 2, 800>("chain NB4 read, 2 issuers, hold 800", sms);
+    run_chain<4, 4, true, false, 2, 1200>("chain NB4 read, 2 issuers, hold 1200", sms);
     return 0;
 }
