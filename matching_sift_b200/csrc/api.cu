@@ -229,6 +229,12 @@ struct InputPlan {
 int plan_inputs(const void* q, const void* r, int type, int q_n, int r_n, Layout& L, InputPlan& ip) {
     if (q_n > 0 && !q) return SIFT_ERR_INVALID_ARG;
     if (r_n > 0 && !r) return SIFT_ERR_INVALID_ARG;
+    // Device types must be device (or managed) memory: a host pointer would
+    // reach a tensor map or a kernel and fault instead of being refused.
+    if (type == -1 || type == SIFT_FLOAT_DEVICE || type == SIFT_HALF_DEVICE || type == SIFT_U8_DEVICE) {
+        if ((q_n > 0 && !is_device_accessible(q)) || (r_n > 0 && !is_device_accessible(r)))
+            return SIFT_ERR_INVALID_ARG;
+    }
     if (type == -1)
         return ((reinterpret_cast<uintptr_t>(q) & 15) || (reinterpret_cast<uintptr_t>(r) & 15)) ? SIFT_ERR_INVALID_ARG
                                                                                                 : SIFT_OK;

@@ -95,12 +95,70 @@ __device__ __forceinline__ void scan_group(const uint32_t (&v)[32], int row0, co
     }
 }
 
-// Accumulator kinds of bound16 / exact8.
+// Accumulator kinds of scan16 / bound16 / exact8.
 enum AccKind : int {
     kAccS32 = 0,    // s32 dot products (u8 kernel)
     kAccF32Int = 1, // f32 accumulators holding integer dot products / dscale (FP16 kernel)
     kAccFloat = 2,  // f32 dot products of general floats (float keys, float norms)
 };
+
+// The pruned scan of 16 consecutive base rows [row0, row0 + 16) in one pass:
+// the two 8-row subgroups of scan_group (same bounds, same keys), a warp vote
+// per chunk, exact keys formed at once from the registers (the form for
+// batches of small problems, whose bounds pass often).
+// nrm: the 16 norms, gm8: the two 8-row minima (8-byte aligned).
+template <int KIND>
+__device__ __forceinline__ void scan16(const uint32_t (&v)[16], int row0, const int32_t* nrm, const int32_t* gm8,
+                                       Top2& s, float dscale) {
+    const int2 g8 = *reinterpret_cast<const int2*>(gm8);
+    int bnd[2];
+    #pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int g = k ? g8.y : g8.x;
+        if constexpr (KIND == kAccFloat) {
+            float m = __uint_as_float(v[8 * k]);
+            #pragma unroll
+            for (int e = 1; e < 8; ++e) m = fmaxf(m, __uint_as_float(v[8 * k + e]));
+            bnd[k] = float_key(fmaf(-2.0f, m, __int_as_float(g)));
+        } else {
+            int m = max8(v + 8 * k);
+            if constexpr (KIND == kAccF32Int) m = f32_dot(static_cast<uint32_t>(m), dscale);
+            bnd[k] = g - 2 * m;
+        }
+    }
+    if (__any_sync(0xffffffffu, min(bnd[0], bnd[1]) <= s.thr)) {
+        #pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const bool ps = bnd[k] <= s.thr;
+            if (__any_sync(0xffffffffu, ps)) {
+                if (ps) {
+                    const int4 na = *reinterpret_cast<const int4*>(nrm + 8 * k);
+                    const int4 nb = *reinterpret_cast<const int4*>(nrm + 8 * k + 4);
+                    const int nr[8] = {na.x, na.y, na.z, na.w, nb.x, nb.y, nb.z, nb.w};
+                    int key[8];
+                    #pragma unroll
+                    for (int e = 0; e < 8; ++e) {
+                        if constexpr (KIND == kAccFloat)
+                            key[e] = float_key(fmaf(-2.0f, __uint_as_float(v[8 * k + e]), __int_as_float(nr[e])));
+                        else if constexpr (KIND == kAccF32Int)
+                            key[e] = nr[e] - 2 * f32_dot(v[8 * k + e], dscale);
+                        else
+                            key[e] = nr[e] - 2 * static_cast<int>(v[8 * k + e]);
+                    }
+                    int mk = __vimin3_s32(key[0], key[1], key[2]);
+                    mk = __vimin3_s32(mk, key[3], key[4]);
+                    mk = __vimin3_s32(mk, key[5], key[6]);
+                    mk = min(mk, key[7]);
+                    if (mk <= s.thr) {
+                        const int base = row0 + 8 * k;
+                        #pragma unroll
+                        for (int e = 0; e < 8; ++e) top2_update(s, key[e], base + e);
+                    }
+                }
+            }
+        }
+    }
+}
 
 // The pruned scan of a TMEM slot in two passes, so that an epilogue can bound
 // every 8-row subgroup with no vote and no branch and form exact keys only

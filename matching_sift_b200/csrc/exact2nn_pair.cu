@@ -193,7 +193,9 @@ struct Cursor {
 
 // has_lo (kModeFloat only): the rows carry lo blocks (split float rows); when
 // false they are plain FP16 rows and only the hi.hi products are formed.
-template <int MODE, int QPT, int QB>
+// TWO_PASS: the two-pass epilogue (single searches) or the one-pass scan
+// (batches of small problems).
+template <int MODE, int QPT, int QB, bool TWO_PASS>
 __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtensorMap& bmap,
                                           const int32_t* __restrict__ brec, const ExactPlan& plan,
                                           const WorkItem* __restrict__ items, int n_items, const WorkItem& single,
@@ -465,44 +467,72 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                     const int32_t* rec = r_smem + s * kRecInts;
                     constexpr int kKind = MODE == kModeFloat ? kAccFloat : (F16 ? kAccF32Int : kAccS32);
                     const int row0 = cur.it.idx_base + j * kBN;
-                    // Two passes over the slot's 128 columns (8 chunks of 16).
-                    // The first bounds every 8-row subgroup against the
-                    // threshold held at its start, with no vote and no branch,
-                    // while chunk c + 1 loads; the second forms exact keys
-                    // only in chunks where some lane's bound passed, reading
-                    // them from the slot again (still held). Then the slot is
-                    // handed back.
-                    uint32_t va[16], vb[16];
-                    const int thr0 = st.thr;
-                    uint32_t pass = 0;  // bit 2 c + k: subgroup k of chunk c may hold a candidate
-                    ptx::tmem_ld16(taddr, va);
-                    ptx::tmem_ld_wait(va);
-                    #pragma unroll
-                    for (int c = 1; c < 8; c += 2) {
-                        ptx::tmem_ld16(taddr + 16 * c, vb);
-                        pass |= bound16<kKind>(va, rec + kBN + 2 * (c - 1), thr0, dscale) << (2 * (c - 1));
-                        ptx::tmem_ld_wait(vb);
-                        if (c + 1 < 8) {
-                            ptx::tmem_ld16(taddr + 16 * (c + 1), va);
-                            pass |= bound16<kKind>(vb, rec + kBN + 2 * c, thr0, dscale) << (2 * c);
-                            ptx::tmem_ld_wait(va);
+                    if constexpr (TWO_PASS) {
+                        // Two passes over the slot's 128 columns (8 chunks of 16).
+                        // The first bounds every 8-row subgroup against the
+                        // threshold held at its start, with no vote and no branch,
+                        // while chunk c + 1 loads; the second forms exact keys
+                        // only in chunks where some lane's bound passed, reading
+                        // them from the slot again (still held). Then the slot is
+                        // handed back.
+                        uint32_t va[16], vb[16];
+                        const int thr0 = st.thr;
+                        uint32_t pass = 0;  // bit 2 c + k: subgroup k of chunk c may hold a candidate
+                        ptx::tmem_ld16(taddr, va);
+                        ptx::tmem_ld_wait(va);
+                        #pragma unroll
+                        for (int c = 1; c < 8; c += 2) {
+                            ptx::tmem_ld16(taddr + 16 * c, vb);
+                            pass |= bound16<kKind>(va, rec + kBN + 2 * (c - 1), thr0, dscale) << (2 * (c - 1));
+                            ptx::tmem_ld_wait(vb);
+                            if (c + 1 < 8) {
+                                ptx::tmem_ld16(taddr + 16 * (c + 1), va);
+                                pass |= bound16<kKind>(vb, rec + kBN + 2 * c, thr0, dscale) << (2 * c);
+                                ptx::tmem_ld_wait(va);
+                            }
                         }
+                        pass |= bound16<kKind>(vb, rec + kBN + 14, thr0, dscale) << 14;
+                        // Subgroups in increasing order, so the top-2 still sees
+                        // the rows in index order (ties keep the lower index).
+                        uint32_t todo = __reduce_or_sync(0xffffffffu, pass);
+                        while (todo) {
+                            const int g = __ffs(todo) - 1;
+                            todo &= todo - 1;
+                            uint32_t v8[8];
+                            ptx::tmem_ld8(taddr + 8 * g, v8);
+                            ptx::tmem_ld_wait(v8);
+                            if ((pass >> g) & 1u) exact8<kKind>(v8, row0 + 8 * g, rec + 8 * g, st, dscale);
+                        }
+                        ptx::tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) ptx::mbar_arrive_cluster_relaxed(lead_tempty);
+                    } else {
+                        // One pass (batches: their bounds pass often, so exact
+                        // keys are formed at once from the registers): chunk c + 1
+                        // loads while chunk c is scanned, and the slot is handed
+                        // back as soon as the last chunk is in registers.
+                        uint32_t va[16], vb[16];
+                        auto scan = [&](const uint32_t (&v)[16], int c) {
+                            scan16<kKind>(v, row0 + 16 * c, rec + 16 * c, rec + kBN + 2 * c, st, dscale);
+                        };
+                        ptx::tmem_ld16(taddr, va);
+                        ptx::tmem_ld_wait(va);
+                        #pragma unroll
+                        for (int c = 1; c < 8; c += 2) {
+                            ptx::tmem_ld16(taddr + 16 * c, vb);
+                            scan(va, c - 1);
+                            ptx::tmem_ld_wait(vb);
+                            if (c + 1 < 8) {
+                                ptx::tmem_ld16(taddr + 16 * (c + 1), va);
+                                scan(vb, c);
+                                ptx::tmem_ld_wait(va);
+                            }
+                        }
+                        ptx::tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) ptx::mbar_arrive_cluster_relaxed(lead_tempty);
+                        scan(vb, 7);
                     }
-                    pass |= bound16<kKind>(vb, rec + kBN + 14, thr0, dscale) << 14;
-                    // Subgroups in increasing order, so the top-2 still sees
-                    // the rows in index order (ties keep the lower index).
-                    uint32_t todo = __reduce_or_sync(0xffffffffu, pass);
-                    while (todo) {
-                        const int g = __ffs(todo) - 1;
-                        todo &= todo - 1;
-                        uint32_t v8[8];
-                        ptx::tmem_ld8(taddr + 8 * g, v8);
-                        ptx::tmem_ld_wait(v8);
-                        if ((pass >> g) & 1u) exact8<kKind>(v8, row0 + 8 * g, rec + 8 * g, st, dscale);
-                    }
-                    ptx::tc_fence_before();
-                    __syncwarp();
-                    if (lane == 0) ptx::mbar_arrive_cluster_relaxed(lead_tempty);
                     if (valid && st.k2 < published) {
                         atomicMin(thresh + q, st.k2);
                         published = st.k2;
@@ -542,7 +572,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CfgU8::kThreads, 1)
     exact2nn_u8_pair_kernel(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap bmap,
                             const int32_t* __restrict__ brec, const ExactPlan plan, const WorkItem single,
                             int4* __restrict__ partial, int32_t* __restrict__ thresh, int* __restrict__ err) {
-    pair_body<kModeU8, 2, 1>(qmap, bmap, brec, plan, nullptr, 1, single, partial, thresh, err, 1.0f);
+    pair_body<kModeU8, 2, 1, true>(qmap, bmap, brec, plan, nullptr, 1, single, partial, thresh, err, 1.0f);
 }
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CfgF16::kThreads, 1)
@@ -550,7 +580,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CfgF16::kThreads, 1)
                              const int32_t* __restrict__ brec, const ExactPlan plan, const WorkItem single,
                              int4* __restrict__ partial, int32_t* __restrict__ thresh, int* __restrict__ err,
                              float dscale) {
-    pair_body<kModeF16Int, 2, 1>(qmap, bmap, brec, plan, nullptr, 1, single, partial, thresh, err, dscale);
+    pair_body<kModeF16Int, 2, 1, true>(qmap, bmap, brec, plan, nullptr, 1, single, partial, thresh, err, dscale);
 }
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CfgFloat::kThreads, 1)
@@ -558,7 +588,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CfgFloat::kThreads, 
                                const int32_t* __restrict__ brec, const ExactPlan plan, const WorkItem single,
                                int4* __restrict__ partial, int32_t* __restrict__ thresh, int* __restrict__ err,
                                int has_lo) {
-    pair_body<kModeFloat, 1, 1>(qmap, bmap, brec, plan, nullptr, 1, single, partial, thresh, err, 1.0f, has_lo != 0);
+    pair_body<kModeFloat, 1, 1, true>(qmap, bmap, brec, plan, nullptr, 1, single, partial, thresh, err, 1.0f,
+                                      has_lo != 0);
 }
 
 template <int QPT, int QB>
@@ -567,7 +598,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairCfg<kModeU8, QPT
                                   const int32_t* __restrict__ brec, const ExactPlan plan,
                                   const WorkItem* __restrict__ items, int n_items, int4* __restrict__ partial,
                                   int32_t* __restrict__ thresh, int* __restrict__ err) {
-    pair_body<kModeU8, QPT, QB>(qmap, bmap, brec, plan, items, n_items, WorkItem{}, partial, thresh, err, 1.0f);
+    pair_body<kModeU8, QPT, QB, false>(qmap, bmap, brec, plan, items, n_items, WorkItem{}, partial, thresh, err,
+                                       1.0f);
 }
 
 template <typename K>

@@ -94,6 +94,30 @@ def test_extreme_values(cuda_device, kernel):
     assert got["nn_dist"][0, 0] == 0 and got["nn_dist"][2, 0] == 128 * 127 ** 2
 
 
+def test_device_types_refuse_host_pointers(cuda_device):
+    """A host array passed as device memory is refused (SIFT_ERR_INVALID_ARG)
+    before it can reach a tensor map or a kernel."""
+    import torch
+
+    q, r = datagen.make_workload(64, 256, seed=5)
+    qd = torch.from_numpy(q).to(cuda_device)
+    rd = torch.from_numpy(r).to(cuda_device)
+    m = torch.empty(64, dtype=torch.int32, device=cuda_device)
+    st = torch.cuda.current_stream(cuda_device).cuda_stream
+    lib = ms.lib()
+    qh = np.ascontiguousarray(q)
+    rh = np.ascontiguousarray(r)
+    for qp, rp in ((qh.ctypes.data, rd.data_ptr()), (qd.data_ptr(), rh.ctypes.data)):
+        rc = lib.sift2nn_match(qp, rp, ms.U8_DEVICE, 64, 256, ms.METRIC_L2, 0.8, m.data_ptr(), None, None, None, st)
+        assert rc == ms.SIFT_ERR_INVALID_ARG
+    qf = np.ascontiguousarray(q.astype(np.float32))
+    rf = rd.float()
+    rc = lib.sift2nn_match(qf.ctypes.data, rf.data_ptr(), ms.FLOAT_DEVICE, 64, 256, ms.METRIC_L2, 0.8,
+                           m.data_ptr(), None, None, None, st)
+    assert rc == ms.SIFT_ERR_INVALID_ARG
+    assert ms.stream_status() == ms.SIFT_OK
+
+
 def test_no_base_rows(cuda_device):
     import torch
 
