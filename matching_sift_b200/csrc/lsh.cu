@@ -164,24 +164,37 @@ __global__ void __launch_bounds__(kHThreads, 1)
             const uint32_t taddr = tmem + (static_cast<uint32_t>(quarter * 32) << 16) + b * slot_cols;
             const int point = (blockIdx.x + i * gridDim.x) * 128 + quarter * 32 + lane;
             uint32_t mask[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            // Up to 4 loads of 32 columns in flight per wait (one TMEM round
+            // trip for P <= 128 hyperplanes instead of one per 32 columns).
             #pragma unroll
-            for (int w = 0; w < 8; ++w) {
-                if (w * 32 < P) {
-                    uint32_t v[32];
-                    ptx::tmem_ld32(taddr + w * 32, v);
-                    ptx::tmem_ld_wait(v);
-                    uint32_t m = 0;
+            for (int w0 = 0; w0 < 8; w0 += 4) {
+                if (w0 * 32 < P) {
+                    uint32_t v[4][32];
                     #pragma unroll
-                    for (int c = 0; c < 32; ++c) m |= (v[c] >> 31) << c;
-                    mask[w] = m;
-                    if (z && point < n) {
-                        // Dot products of the point with each hyperplane (multi-probe margins).
-                        #pragma unroll
-                        for (int c = 0; c < 32; ++c) {
-                            const int col = w * 32 + c;
-                            if (col < L * k)
-                                z[(static_cast<size_t>(col / k) * n + point) * k + col % k] =
-                                    static_cast<float>(static_cast<int>(v[c]));
+                    for (int u = 0; u < 4; ++u)
+                        if ((w0 + u) * 32 < P) ptx::tmem_ld32(taddr + (w0 + u) * 32, v[u]);
+                    ptx::tmem_ld_wait(v[0]);
+                    ptx::tmem_ld_wait(v[1]);
+                    ptx::tmem_ld_wait(v[2]);
+                    ptx::tmem_ld_wait(v[3]);
+                    #pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int w = w0 + u;
+                        if (w * 32 < P) {
+                            uint32_t m = 0;
+                            #pragma unroll
+                            for (int c = 0; c < 32; ++c) m |= (v[u][c] >> 31) << c;
+                            mask[w] = m;
+                            if (z && point < n) {
+                                // Dot products of the point with each hyperplane (multi-probe margins).
+                                #pragma unroll
+                                for (int c = 0; c < 32; ++c) {
+                                    const int col = w * 32 + c;
+                                    if (col < L * k)
+                                        z[(static_cast<size_t>(col / k) * n + point) * k + col % k] =
+                                            static_cast<float>(static_cast<int>(v[u][c]));
+                                }
+                            }
                         }
                     }
                 }
