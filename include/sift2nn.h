@@ -43,7 +43,8 @@ extern "C" {
 #endif
 
 /* Input memory types: 0..2 as in the reference (src/knn_brute.cu:15-19,
-   src/lsh_h.cu:710-714); 3 and 4 are extensions for u8 descriptors. */
+   src/lsh_h.cu:710-714); 3 and 4 are extensions for u8 descriptors. A host
+   pointer given with a device type returns SIFT_ERR_INVALID_ARG. */
 enum sift_mem_type {
     SIFT_FLOAT_HOST = 0,   /* float[n][128] in mapped pinned host memory (read zero-copy) */
     SIFT_FLOAT_DEVICE = 1, /* float[n][128] in device memory */
