@@ -393,12 +393,12 @@ int exact_match_chunked(const MatchArgs& a, DeviceCtx& c, cudaStream_t st) {
     int4* partial = reinterpret_cast<int4*>(A + o_part);
     const uint8_t* rh = static_cast<const uint8_t*>(a.r);
 
-    // Queries first, on the search stream; the base chunks on the copy stream
-    // once every earlier use of the arena on the search stream is done.
-    SIFT_CUDA(cudaMemcpyAsync(qd, a.q, static_cast<size_t>(q_n) * kDim, cudaMemcpyHostToDevice, st));
-    SIFT_CUDA(launch_row_norms_u8(qd, q_n, whole.q_pad, kMetricL2, qnorm, nullptr, thresh, st));
+    // The base chunks on the copy stream once every earlier use of the arena
+    // on the search stream is done; the queries meanwhile on the search stream.
     SIFT_CUDA(cudaEventRecord(c.chunk_ev[kMaxChunks], st));
     SIFT_CUDA(cudaStreamWaitEvent(c.copy_stream, c.chunk_ev[kMaxChunks], 0));
+    SIFT_CUDA(cudaMemcpyAsync(qd, a.q, static_cast<size_t>(q_n) * kDim, cudaMemcpyHostToDevice, st));
+    SIFT_CUDA(launch_row_norms_u8(qd, q_n, whole.q_pad, kMetricL2, qnorm, nullptr, thresh, st));
     for (int ch = 0; ch < n_chunks; ++ch) {
         const size_t off = static_cast<size_t>(ch) * chunk_rows;
         SIFT_CUDA(cudaMemcpyAsync(rd + off * kDim, rh + off * kDim, static_cast<size_t>(plans[ch].r_n) * kDim,
