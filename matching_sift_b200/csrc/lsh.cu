@@ -337,70 +337,88 @@ __global__ void __launch_bounds__(kScanThreads) lsh_scan_kernel(
     const bool whole_bins = shift == 0;  // a group holds exactly one code
     int d1 = INT_MAX, i1 = -1, d2 = INT_MAX, i2 = -1;
     uint32_t seen = 0;  // candidates compared (bucket members)
-    for (int c = 0; c < L * probes; ++c) {
-        const int t = c / probes;  // probe c of the query searches table t
-        const uint32_t code = qcodes[static_cast<size_t>(c) * q_n + wq];
-        // A repeated probe code (fewer distinct probes than requested) is skipped.
-        bool dup = false;
-        for (int c2 = t * probes; c2 < c; ++c2) dup |= qcodes[static_cast<size_t>(c2) * q_n + wq] == code;
-        if (dup) continue;
+    for (int t = 0; t < L; ++t) {
+        // The table's probe codes and their bucket bounds, one probe per lane
+        // (probes <= 64: two per lane), fetched in parallel: two round trips per
+        // table instead of two per probe.
         const int* st = start + static_cast<size_t>(t) * (nbins + 1);
-        const int bin = static_cast<int>(code >> shift);
-        const int s = st[bin], e = st[bin + 1];
-        const int* ord = order + static_cast<size_t>(t) * r_n;
-        const uint32_t* oc = ocode + static_cast<size_t>(t) * r_n;
-        int nid = -1;
-        uint32_t ncode = ~code;
-        if (s + lane < e) {
-            nid = ord[s + lane];
-            ncode = whole_bins ? code : oc[s + lane];
+        const uint32_t* tq = qcodes + static_cast<size_t>(t) * probes * q_n + wq;
+        uint32_t pc0 = 0, pc1 = 0;
+        int ps0 = 0, pe0 = 0, ps1 = 0, pe1 = 0;
+        if (lane < probes) pc0 = tq[static_cast<size_t>(lane) * q_n];
+        if (lane + 32 < probes) pc1 = tq[static_cast<size_t>(lane + 32) * q_n];
+        if (lane < probes) {
+            const int b = static_cast<int>(pc0 >> shift);
+            ps0 = st[b];
+            pe0 = st[b + 1];
         }
-        for (int p0 = s; p0 < e; p0 += 32) {
-            const int id = nid;
-            const bool hit = id >= 0 && ncode == code;
-            const int pn = p0 + 32 + lane;
-            nid = -1;
-            ncode = ~code;
-            if (pn < e) {
-                nid = ord[pn];
-                ncode = whole_bins ? code : oc[pn];
+        if (lane + 32 < probes) {
+            const int b = static_cast<int>(pc1 >> shift);
+            ps1 = st[b];
+            pe1 = st[b + 1];
+        }
+        for (int pi = 0; pi < probes; ++pi) {
+            const bool lo = pi < 32;
+            const uint32_t code = __shfl_sync(0xffffffffu, lo ? pc0 : pc1, pi & 31);
+            // A repeated probe code (fewer distinct probes than requested) is skipped.
+            if (__any_sync(0xffffffffu, (lane < pi && pc0 == code) || (lane + 32 < pi && pc1 == code))) continue;
+            const int s = __shfl_sync(0xffffffffu, lo ? ps0 : ps1, pi & 31);
+            const int e = __shfl_sync(0xffffffffu, lo ? pe0 : pe1, pi & 31);
+            const int* ord = order + static_cast<size_t>(t) * r_n;
+            const uint32_t* oc = ocode + static_cast<size_t>(t) * r_n;
+            int nid = -1;
+            uint32_t ncode = ~code;
+            if (s + lane < e) {
+                nid = ord[s + lane];
+                ncode = whole_bins ? code : oc[s + lane];
             }
-            const uint32_t mask = __ballot_sync(0xffffffffu, hit);
-            const int nm = __popc(mask);
-            if (nm == 0) continue;
-            seen += nm;
-            if (hit) ids[__popc(mask & ((1u << lane) - 1u))] = id;
-            __syncwarp();
-            uint4 rv[8];
-            int cid[8];
-            #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const int rank = 4 * j + sub;
-                cid[j] = rank < nm ? ids[rank] : -1;
-                if (cid[j] >= 0)
-                    rv[j] = __ldg(reinterpret_cast<const uint4*>(r + static_cast<size_t>(cid[j]) * 128) + part);
-            }
-            __syncwarp();
-            #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                if (4 * j >= nm) break;
-                // |q - b|^2 of this lane's 16 bytes: byte-wise |q - b| (SIMD
-                // absolute difference), then the sum of their squares by dp4a.
-                uint32_t dist = 0;
-                if (cid[j] >= 0) {
-                    uint32_t a = __vabsdiffu4(qv.x, rv[j].x);
-                    dist = __dp4a(a, a, dist);
-                    a = __vabsdiffu4(qv.y, rv[j].y);
-                    dist = __dp4a(a, a, dist);
-                    a = __vabsdiffu4(qv.z, rv[j].z);
-                    dist = __dp4a(a, a, dist);
-                    a = __vabsdiffu4(qv.w, rv[j].w);
-                    dist = __dp4a(a, a, dist);
+            for (int p0 = s; p0 < e; p0 += 32) {
+                const int id = nid;
+                const bool hit = id >= 0 && ncode == code;
+                const int pn = p0 + 32 + lane;
+                nid = -1;
+                ncode = ~code;
+                if (pn < e) {
+                    nid = ord[pn];
+                    ncode = whole_bins ? code : oc[pn];
                 }
-                dist += __shfl_xor_sync(0xffffffffu, dist, 1);
-                dist += __shfl_xor_sync(0xffffffffu, dist, 2);
-                dist += __shfl_xor_sync(0xffffffffu, dist, 4);
-                if (part == 0 && cid[j] >= 0) push_dedup(static_cast<int>(dist), cid[j], d1, i1, d2, i2);
+                const uint32_t mask = __ballot_sync(0xffffffffu, hit);
+                const int nm = __popc(mask);
+                if (nm == 0) continue;
+                seen += nm;
+                if (hit) ids[__popc(mask & ((1u << lane) - 1u))] = id;
+                __syncwarp();
+                uint4 rv[8];
+                int cid[8];
+                #pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int rank = 4 * j + sub;
+                    cid[j] = rank < nm ? ids[rank] : -1;
+                    if (cid[j] >= 0)
+                        rv[j] = __ldg(reinterpret_cast<const uint4*>(r + static_cast<size_t>(cid[j]) * 128) + part);
+                }
+                __syncwarp();
+                #pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    if (4 * j >= nm) break;
+                    // |q - b|^2 of this lane's 16 bytes: byte-wise |q - b| (SIMD
+                    // absolute difference), then the sum of their squares by dp4a.
+                    uint32_t dist = 0;
+                    if (cid[j] >= 0) {
+                        uint32_t a = __vabsdiffu4(qv.x, rv[j].x);
+                        dist = __dp4a(a, a, dist);
+                        a = __vabsdiffu4(qv.y, rv[j].y);
+                        dist = __dp4a(a, a, dist);
+                        a = __vabsdiffu4(qv.z, rv[j].z);
+                        dist = __dp4a(a, a, dist);
+                        a = __vabsdiffu4(qv.w, rv[j].w);
+                        dist = __dp4a(a, a, dist);
+                    }
+                    dist += __shfl_xor_sync(0xffffffffu, dist, 1);
+                    dist += __shfl_xor_sync(0xffffffffu, dist, 2);
+                    dist += __shfl_xor_sync(0xffffffffu, dist, 4);
+                    if (part == 0 && cid[j] >= 0) push_dedup(static_cast<int>(dist), cid[j], d1, i1, d2, i2);
+                }
             }
         }
     }
