@@ -388,37 +388,44 @@ __global__ void __launch_bounds__(kScanThreads) lsh_scan_kernel(
                 seen += nm;
                 if (hit) ids[__popc(mask & ((1u << lane) - 1u))] = id;
                 __syncwarp();
-                uint4 rv[8];
-                int cid[8];
+                // The hits in two rounds of 16 (4 rows per lane in flight):
+                // fewer registers than one round of 32, so more queries (warps)
+                // share an SM and hide each other's load latency.
                 #pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const int rank = 4 * j + sub;
-                    cid[j] = rank < nm ? ids[rank] : -1;
-                    if (cid[j] >= 0)
-                        rv[j] = __ldg(reinterpret_cast<const uint4*>(r + static_cast<size_t>(cid[j]) * 128) + part);
-                }
-                __syncwarp();
-                #pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    if (4 * j >= nm) break;
-                    // |q - b|^2 of this lane's 16 bytes: byte-wise |q - b| (SIMD
-                    // absolute difference), then the sum of their squares by dp4a.
-                    uint32_t dist = 0;
-                    if (cid[j] >= 0) {
-                        uint32_t a = __vabsdiffu4(qv.x, rv[j].x);
-                        dist = __dp4a(a, a, dist);
-                        a = __vabsdiffu4(qv.y, rv[j].y);
-                        dist = __dp4a(a, a, dist);
-                        a = __vabsdiffu4(qv.z, rv[j].z);
-                        dist = __dp4a(a, a, dist);
-                        a = __vabsdiffu4(qv.w, rv[j].w);
-                        dist = __dp4a(a, a, dist);
+                for (int h = 0; h < 2; ++h) {
+                    if (16 * h >= nm) break;
+                    uint4 rv[4];
+                    int cid[4];
+                    #pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int rank = 16 * h + 4 * j + sub;
+                        cid[j] = rank < nm ? ids[rank] : -1;
+                        if (cid[j] >= 0)
+                            rv[j] = __ldg(reinterpret_cast<const uint4*>(r + static_cast<size_t>(cid[j]) * 128) + part);
                     }
-                    dist += __shfl_xor_sync(0xffffffffu, dist, 1);
-                    dist += __shfl_xor_sync(0xffffffffu, dist, 2);
-                    dist += __shfl_xor_sync(0xffffffffu, dist, 4);
-                    if (part == 0 && cid[j] >= 0) push_dedup(static_cast<int>(dist), cid[j], d1, i1, d2, i2);
+                    #pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        if (16 * h + 4 * j >= nm) break;
+                        // |q - b|^2 of this lane's 16 bytes: byte-wise |q - b| (SIMD
+                        // absolute difference), then the sum of their squares by dp4a.
+                        uint32_t dist = 0;
+                        if (cid[j] >= 0) {
+                            uint32_t a = __vabsdiffu4(qv.x, rv[j].x);
+                            dist = __dp4a(a, a, dist);
+                            a = __vabsdiffu4(qv.y, rv[j].y);
+                            dist = __dp4a(a, a, dist);
+                            a = __vabsdiffu4(qv.z, rv[j].z);
+                            dist = __dp4a(a, a, dist);
+                            a = __vabsdiffu4(qv.w, rv[j].w);
+                            dist = __dp4a(a, a, dist);
+                        }
+                        dist += __shfl_xor_sync(0xffffffffu, dist, 1);
+                        dist += __shfl_xor_sync(0xffffffffu, dist, 2);
+                        dist += __shfl_xor_sync(0xffffffffu, dist, 4);
+                        if (part == 0 && cid[j] >= 0) push_dedup(static_cast<int>(dist), cid[j], d1, i1, d2, i2);
+                    }
                 }
+                __syncwarp();  // ids is rewritten by the next 32 positions
             }
         }
     }
