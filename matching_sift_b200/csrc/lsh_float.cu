@@ -112,48 +112,66 @@ __global__ void __launch_bounds__(256) lsh_scan_float_kernel(
     const bool whole_bins = shift == 0;
     int d1 = INT_MAX, i1 = -1, d2 = INT_MAX, i2 = -1;
     uint32_t seen = 0;
-    for (int c = 0; c < L * probes; ++c) {
-        const int t = c / probes;
-        const uint32_t code = qcodes[static_cast<size_t>(c) * q_n + wq];
-        bool dup = false;
-        for (int c2 = t * probes; c2 < c; ++c2) dup |= qcodes[static_cast<size_t>(c2) * q_n + wq] == code;
-        if (dup) continue;
+    for (int t = 0; t < L; ++t) {
+        // The table's probe codes and bucket bounds, one probe per lane
+        // (probes <= 64: two per lane), fetched in parallel.
         const int* st = start + static_cast<size_t>(t) * (nbins + 1);
-        const int bin = static_cast<int>(code >> shift);
-        const int s = st[bin], e = st[bin + 1];
-        const int* ord = order + static_cast<size_t>(t) * r_n;
-        const uint32_t* oc = ocode + static_cast<size_t>(t) * r_n;
-        for (int p0 = s; p0 < e; p0 += 32) {
-            const int p = p0 + lane;
-            const bool hit = p < e && (whole_bins || oc[p] == code);
-            const uint32_t mask = __ballot_sync(0xffffffffu, hit);
-            const int nm = __popc(mask);
-            if (nm == 0) continue;
-            seen += nm;
-            if (hit) ids[__popc(mask & ((1u << lane) - 1u))] = ord[p];
-            __syncwarp();
-            for (int j = 0; 4 * j < nm; ++j) {
-                const int rank = 4 * j + sub;
-                const int cid = rank < nm ? ids[rank] : -1;
-                float dist = 0.0f;
-                if (cid >= 0) {
-                    #pragma unroll
-                    for (int cc = 0; cc < 4; ++cc) {
-                        float b4[4];
-                        load4(r, static_cast<size_t>(cid) * kDim + 16 * part + 4 * cc, b4);
+        const uint32_t* tq = qcodes + static_cast<size_t>(t) * probes * q_n + wq;
+        uint32_t pc0 = 0, pc1 = 0;
+        int ps0 = 0, pe0 = 0, ps1 = 0, pe1 = 0;
+        if (lane < probes) pc0 = tq[static_cast<size_t>(lane) * q_n];
+        if (lane + 32 < probes) pc1 = tq[static_cast<size_t>(lane + 32) * q_n];
+        if (lane < probes) {
+            const int b = static_cast<int>(pc0 >> shift);
+            ps0 = st[b];
+            pe0 = st[b + 1];
+        }
+        if (lane + 32 < probes) {
+            const int b = static_cast<int>(pc1 >> shift);
+            ps1 = st[b];
+            pe1 = st[b + 1];
+        }
+        for (int pi = 0; pi < probes; ++pi) {
+            const bool lo = pi < 32;
+            const uint32_t code = __shfl_sync(0xffffffffu, lo ? pc0 : pc1, pi & 31);
+            // A repeated probe code (fewer distinct probes than requested) is skipped.
+            if (__any_sync(0xffffffffu, (lane < pi && pc0 == code) || (lane + 32 < pi && pc1 == code))) continue;
+            const int s = __shfl_sync(0xffffffffu, lo ? ps0 : ps1, pi & 31);
+            const int e = __shfl_sync(0xffffffffu, lo ? pe0 : pe1, pi & 31);
+            const int* ord = order + static_cast<size_t>(t) * r_n;
+            const uint32_t* oc = ocode + static_cast<size_t>(t) * r_n;
+            for (int p0 = s; p0 < e; p0 += 32) {
+                const int p = p0 + lane;
+                const bool hit = p < e && (whole_bins || oc[p] == code);
+                const uint32_t mask = __ballot_sync(0xffffffffu, hit);
+                const int nm = __popc(mask);
+                if (nm == 0) continue;
+                seen += nm;
+                if (hit) ids[__popc(mask & ((1u << lane) - 1u))] = ord[p];
+                __syncwarp();
+                for (int j = 0; 4 * j < nm; ++j) {
+                    const int rank = 4 * j + sub;
+                    const int cid = rank < nm ? ids[rank] : -1;
+                    float dist = 0.0f;
+                    if (cid >= 0) {
                         #pragma unroll
-                        for (int ee = 0; ee < 4; ++ee) {
-                            const float df = qv[4 * cc + ee] - b4[ee];
-                            dist = fmaf(df, df, dist);
+                        for (int cc = 0; cc < 4; ++cc) {
+                            float b4[4];
+                            load4(r, static_cast<size_t>(cid) * kDim + 16 * part + 4 * cc, b4);
+                            #pragma unroll
+                            for (int ee = 0; ee < 4; ++ee) {
+                                const float df = qv[4 * cc + ee] - b4[ee];
+                                dist = fmaf(df, df, dist);
+                            }
                         }
                     }
+                    dist += __shfl_xor_sync(0xffffffffu, dist, 1);
+                    dist += __shfl_xor_sync(0xffffffffu, dist, 2);
+                    dist += __shfl_xor_sync(0xffffffffu, dist, 4);
+                    if (part == 0 && cid >= 0) push_dedup(float_key(dist), cid, d1, i1, d2, i2);
                 }
-                dist += __shfl_xor_sync(0xffffffffu, dist, 1);
-                dist += __shfl_xor_sync(0xffffffffu, dist, 2);
-                dist += __shfl_xor_sync(0xffffffffu, dist, 4);
-                if (part == 0 && cid >= 0) push_dedup(float_key(dist), cid, d1, i1, d2, i2);
+                __syncwarp();
             }
-            __syncwarp();
         }
     }
     #pragma unroll
