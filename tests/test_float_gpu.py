@@ -253,3 +253,33 @@ def test_lsh_on_general_floats(cuda_device):
     assert ms.lsh_gpu(qd, rd, ms.FLOAT_DEVICE, 400, 20000, m, 0.8, None, 2, 3, 0, 12) == ms.SIFT_OK
     mm = m.cpu().numpy().view(np.uint32)
     assert ((mm < 20000) | (mm == 0xFFFFFFFF)).all() and (mm < 20000).mean() > 0.5
+
+
+def test_lsh_on_general_floats_more_probes_never_lose_the_nearest(cuda_device):
+    """Multi-probe LSH on general float rows: the probe codes of P probes are a
+    prefix of those of more probes, so every added probe only adds candidates:
+    the candidate count never falls and the nearest distance never grows, up to
+    64 probes per table (more than a warp's 32 lanes)."""
+    import torch
+
+    from matching_sift_b200 import datagen
+
+    q, r = rand_unit(300, 21), rand_unit(20000, 22)
+    planes = torch.from_numpy(datagen.quantize_planes(datagen.make_hyperplanes(12, 2, seed=23), 32.0)).to(cuda_device)
+    qd, rd = torch.from_numpy(q).to(cuda_device), torch.from_numpy(r).to(cuda_device)
+    prev_d, prev_c = None, None
+    for probes in (1, 8, 33, 64):
+        o = ms.lsh_match(qd, rd, planes, threshold=0.0, probes=probes, candidates=True)
+        assert ms.stream_status() == ms.SIFT_OK
+        d1 = o["nn_dist"][:, 0].cpu().numpy().astype(np.float64)
+        c = o["candidates"].cpu().numpy().astype(np.int64)
+        if prev_d is not None:
+            assert (c >= prev_c).all()
+            assert (d1 <= prev_d).all()
+        prev_d, prev_c = d1, c
+    # every reported neighbour is a real row at its FP64 distance (within the float tolerance)
+    idx = o["nn_idx"][:, 0].cpu().numpy().astype(np.int64)
+    ok = idx >= 0
+    dd = ((q[ok].astype(np.float64) - r[idx[ok]].astype(np.float64)) ** 2).sum(1)
+    qn = (q.astype(np.float64) ** 2).sum(1)[ok]
+    assert (np.abs(prev_d[ok] - dd) <= TOL * 2 * qn + 1e-6).all()

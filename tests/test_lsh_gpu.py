@@ -213,7 +213,9 @@ def _probe_codes(codes, dots, k, probes):
     return out
 
 
-@pytest.mark.parametrize("L,k,probes", [(2, 16, 1), (2, 16, 4), (1, 12, 16), (3, 10, 8)])
+# (1, 14, 40) and (2, 12, 64): more probes per table than a warp has lanes
+# (the scan fetches a table's probes one per lane, two per lane past 32).
+@pytest.mark.parametrize("L,k,probes", [(2, 16, 1), (2, 16, 4), (1, 12, 16), (3, 10, 8), (1, 14, 40), (2, 12, 64)])
 def test_multiprobe_vs_oracle(cuda_device, L, k, probes):
     import torch
 
