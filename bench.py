@@ -381,7 +381,7 @@ def main():
         bf16x2 = 2.0 * peaks["bf16_tflops"]
         qps = world * q_n * args.steps / (step_ms * 1e-3)
         e2e_qps = world * q_n * args.steps / (e2e_ms * 1e-3) if e2e_ms == e2e_ms else None
-        traffic = _profile_value("exact2nn_u8_pair_10000x1M.md", "traffic_bytes_per_launch") if q_n == Q_N else None
+        traffic = _profile_value("exact2nn_u8fold_pair_10000x1M.md", "traffic_bytes_per_launch") if q_n == Q_N else None
         line = {
             "metric": METRIC,
             "value": round(qps, 1),
@@ -408,7 +408,7 @@ def main():
                     "h2d_note": "h2d_copy_ms: the step's input bytes copied alone from pinned memory on this box "
                                 "(the PCIe bound of the call); frac = that / the call's time"},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "tensor", "kernel": "exact2nn_u8_pair_kernel", "achieved": round(achieved, 1),
+            "roofline": {"bound": "tensor", "kernel": "exact2nn_u8fold_pair_kernel", "achieved": round(achieved, 1),
                          "peak": round(peak_int8, 1), "unit": "TFLOP/s", "frac": round(achieved / peak_int8, 4),
                          "traffic": traffic,
                          "ops_per_launch": ops, "kernel_ms": round(kernel_ms, 4),

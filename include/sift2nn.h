@@ -441,9 +441,11 @@ SIFT_API int sift_profile_collect(double* total_ms, int* launches);
 SIFT_API int sift_profile_collect_kernel(int kernel, double* total_ms, int* launches);
 
 /* Selects the exact-search kernel for subsequent calls in this process:
-   0 (default) the CTA-pair kernels (tcgen05 cta_group::2; half inputs go to
-   the FP16 kernel), 1 the single-CTA u8 kernel, 2 the CTA-pair u8 kernel for
-   every input type (half inputs packed to u8). All return identical results. */
+   0 (default) the CTA-pair kernels (tcgen05 cta_group::2): u8 rows on the
+   kernel that folds the base norms into a fifth MMA per tile, half inputs on
+   the FP16 kernel; 1 the single-CTA u8 kernel; 2 the CTA-pair u8 kernel
+   without folding for every input type (half inputs packed to u8); 3 as 0
+   but without folding. All return identical results. */
 SIFT_API int sift_set_kernel_variant(int variant);
 
 /* Fault injection for failure-detection tests (no counterpart in the

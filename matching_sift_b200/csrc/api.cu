@@ -148,6 +148,19 @@ int encode_u8_rows(CUtensorMap* m, const void* base, uint64_t rows, uint32_t box
     return r == CUDA_SUCCESS ? SIFT_OK : SIFT_ERR_CUDA;
 }
 
+// The folding digits of fold_records_kernel as a 2-D u8 tensor of 256-byte
+// rows (8 rows = one half tile, copied as is: no swizzle).
+int encode_fold_map(CUtensorMap* m, const void* base, uint64_t tiles) {
+    cuuint64_t dims[2] = {256, static_cast<cuuint64_t>(tiles) * 16};
+    cuuint64_t strides[1] = {256};
+    cuuint32_t box[2] = {256, 8};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? SIFT_OK : SIFT_ERR_CUDA;
+}
+
 int encode_bf16_2d(CUtensorMap* m, const void* base, uint64_t inner, uint64_t rows, uint32_t box_inner,
                    uint32_t box_rows) {
     cuuint64_t dims[2] = {static_cast<cuuint64_t>(inner), static_cast<cuuint64_t>(rows)};
@@ -580,7 +593,10 @@ int exact_match(const MatchArgs& a) {
     const int variant = g_variant.load();
     const bool use_pair = variant != 1;
     // Half inputs are searched as FP16 by the FP16 tensor-core kernel in place.
-    const bool use_f16 = variant == 0 && a.type == SIFT_HALF_DEVICE;
+    const bool use_f16 = (variant == 0 || variant == 3) && a.type == SIFT_HALF_DEVICE;
+    // The default for u8 rows: the pair kernel with the norms folded into the
+    // MMAs; variant 3 keeps the pair kernel without folding.
+    const bool use_fold = variant == 0 && a.type != SIFT_HALF_DEVICE;
     if (use_pair && a.type == SIFT_U8_HOST && r_n >= kChunkMinRows) return exact_match_chunked(a, c, st);
     const ExactPlan plan = use_pair ? make_exact_plan(q_n, r_n, c.num_sms / 2, 2) : make_exact_plan(q_n, r_n, c.num_sms, 1);
 
@@ -602,6 +618,7 @@ int exact_match(const MatchArgs& a) {
     const size_t o_s = (a.sorted && !s_dev) ? L.take(static_cast<size_t>(q_n) * 16) : 0;
     const size_t o_i = (a.nn_idx && !i_dev) ? L.take(static_cast<size_t>(q_n) * 8) : 0;
     const size_t o_d = (a.nn_dist && !d_dev) ? L.take(static_cast<size_t>(q_n) * 8) : 0;
+    const size_t o_fold = use_fold ? L.take(static_cast<size_t>(plan.base_tiles) * 2 * kFoldHalfBytes) : 0;
     SIFT_TRY(ensure_arena(c, L.off));
     char* A = c.arena;
 
@@ -633,7 +650,11 @@ int exact_match(const MatchArgs& a) {
         SIFT_CUDA(launch_row_norms_f16(a.r, r_n, plan.r_pad, mul, a.metric, nullptr, brec, nullptr, st));
         SIFT_CUDA(launch_row_norms_f16(a.q, q_n, plan.q_pad, mul, kMetricL2, qnorm, nullptr, thresh, st));
     } else {
-        SIFT_CUDA(launch_row_norms_u8(rd, r_n, plan.r_pad, a.metric, nullptr, brec, nullptr, st));
+        if (use_fold)
+            SIFT_CUDA(launch_fold_records_u8(rd, r_n, plan.r_pad, a.metric, brec,
+                                             reinterpret_cast<uint32_t*>(A + o_fold), st));
+        else
+            SIFT_CUDA(launch_row_norms_u8(rd, r_n, plan.r_pad, a.metric, nullptr, brec, nullptr, st));
         SIFT_CUDA(launch_row_norms_u8(qd, q_n, plan.q_pad, kMetricL2, qnorm, nullptr, thresh, st));
     }
     g_launches += (plan.r_pad > 0 ? 1 : 0) + 1;
@@ -654,7 +675,11 @@ int exact_match(const MatchArgs& a) {
         if (use_f16)
             SIFT_CUDA(launch_exact2nn_f16_pair(qmap, bmap, brec, plan, partial, thresh, c.d_status,
                                                ldexpf(1.0f, 2 * shift), st));
-        else if (use_pair)
+        else if (use_fold) {
+            CUtensorMap fmap;
+            SIFT_TRY(encode_fold_map(&fmap, A + o_fold, plan.base_tiles));
+            SIFT_CUDA(launch_exact2nn_u8fold_pair(qmap, bmap, fmap, brec, plan, partial, thresh, c.d_status, st));
+        } else if (use_pair)
             SIFT_CUDA(launch_exact2nn_u8_pair(qmap, bmap, brec, plan, partial, thresh, c.d_status, st));
         else
             SIFT_CUDA(launch_exact2nn_u8(qmap, bmap, brec, plan, partial, thresh, c.d_status, st));
@@ -993,7 +1018,7 @@ int profile_collect(int tag, double* total_ms, int* launches) {
 
 long long launch_count() { return g_launches.load(); }
 int set_variant(int v) {
-    if (v < 0 || v > 2) return SIFT_ERR_INVALID_ARG;
+    if (v < 0 || v > 3) return SIFT_ERR_INVALID_ARG;
     g_variant.store(v);
     return SIFT_OK;
 }

@@ -191,6 +191,14 @@ __device__ __forceinline__ uint32_t bound16(const uint32_t (&v)[16], const int32
     return bits;
 }
 
+// fold_bits16: the pass bits of a chunk's two 8-row subgroups in the fold
+// variant, whose accumulators hold q.b - c and whose keys are r - 2 acc with
+// residuals r >= -1: subgroup k may hold a key within thr only when its
+// largest accumulator reaches vt = -floor((thr + 1) / 2).
+__device__ __forceinline__ uint32_t fold_bits16(const uint32_t (&v)[16], int vt) {
+    return (max8(v) >= vt ? 1u : 0u) | (max8(v + 8) >= vt ? 2u : 0u);
+}
+
 // exact8: the exact keys of one 8-row subgroup [row0, row0 + 8) (v: its
 // accumulators, nrm: its 8 norms, 16-byte aligned); they update the running
 // top-2 only when their minimum is within the thread's current threshold (a

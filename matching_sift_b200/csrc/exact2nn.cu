@@ -130,6 +130,77 @@ __global__ void __launch_bounds__(256) row_norms_kernel(const T* __restrict__ x,
     }
 }
 
+// Norm folding (the fold variant of the u8 pair kernel). A fifth MMA per tile
+// product multiplies a constant query-side row a[32] (u8) with 32 signed
+// digits d[32] per base row (s8) so that the accumulator holds
+// q.b - c with c = min(ceil(|b|^2 / 2), kFoldMax) and a.d = -c:
+//   a = {1, 16, 255 x 30}, c = 255 h + l (0 <= l < 255),
+//   d[0] = -(l & 15), d[1] = -(l >> 4), d[2..31] = -h in parts of at most 128.
+// The key |b|^2 - 2 q.b = r - 2 acc with the residual r = |b|^2 - 2 c >= -1,
+// so every key of a row set is at least -1 - 2 max(acc): one max tree per
+// row set bounds its keys exactly up to that 1 (rows whose c was clamped
+// only make the bound looser). Records hold the residuals.
+//
+// fold[] layout: per base tile, per half of 64 rows, 2048 bytes in the
+// tensor cores' no-swizzle K-major layout (8-row groups of 256 bytes, two
+// 16-byte K chunks of 128 bytes each, 16 bytes per row), so one 2-D TMA box
+// of 8 x 256 bytes lands a half tile ready as an MMA operand.
+__global__ void __launch_bounds__(256) fold_records_kernel(const uint8_t* __restrict__ x, int n, int n_pad,
+                                                           int metric, int32_t* __restrict__ rec,
+                                                           uint32_t* __restrict__ fold) {
+    const int row = blockIdx.x * 32 + (threadIdx.x >> 3);
+    const int sub = threadIdx.x & 7;
+    uint32_t s = 0;
+    if (row < n) {
+        const uint4 w = load16_u8(x, row, sub, 1.0f);
+        s = __dp4a(w.x, w.x, 0u);
+        s = __dp4a(w.y, w.y, s);
+        s = __dp4a(w.z, w.z, s);
+        s = __dp4a(w.w, w.w, s);
+    }
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    s += __shfl_xor_sync(0xffffffffu, s, 4);
+    const int32_t norm = row < n ? (metric == kMetricL2 ? static_cast<int32_t>(s) : 0) : kKeyPad;
+    const int32_t c = row < n ? min((norm + 1) >> 1, kFoldMax) : 0;
+    const int32_t resid = norm - 2 * c;
+    // This thread's 4 digits k = 4 sub .. 4 sub + 3.
+    const int l = c % 255, h = c / 255;
+    uint32_t word = 0;
+    #pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        const int k = 4 * sub + b;
+        const int d = k == 0 ? -(l & 15) : (k == 1 ? -(l >> 4) : -min(128, max(0, h - 128 * (k - 2))));
+        word |= (static_cast<uint32_t>(d) & 0xFFu) << (8 * b);
+    }
+    const int t = row >> 7, w = row & 127;
+    const size_t off = (static_cast<size_t>(t) * 2 + (w >> 6)) * kFoldHalfBytes + ((w & 63) >> 3) * 256 +
+                       (sub >> 2) * 128 + (w & 7) * 16 + 4 * (sub & 3);
+    fold[off / 4] = word;
+
+    __shared__ int32_t res[32];
+    int32_t* r = rec + static_cast<size_t>(blockIdx.x / 4) * kRecInts;
+    const int part = blockIdx.x & 3;
+    if (sub == 0) {
+        res[threadIdx.x >> 3] = resid;
+        r[part * 32 + (threadIdx.x >> 3)] = resid;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        int m = res[8 * threadIdx.x];
+        #pragma unroll
+        for (int i = 1; i < 8; ++i) m = min(m, res[8 * threadIdx.x + i]);
+        r[128 + part * 4 + threadIdx.x] = m;
+    }
+    if (threadIdx.x >= 32 && threadIdx.x < 34) {
+        const int hh = threadIdx.x - 32;
+        int m = res[16 * hh];
+        #pragma unroll
+        for (int i = 1; i < 16; ++i) m = min(m, res[16 * hh + i]);
+        r[144 + part * 2 + hh] = m;
+    }
+}
+
 // 16 consecutive elements of a row, times mul, as floats.
 __device__ __forceinline__ void load16_f32(const float* x, int row, int sub, float mul, float (&f)[16]) {
     const float4* p = reinterpret_cast<const float4*>(x + static_cast<size_t>(row) * kDim) + 4 * sub;
@@ -659,6 +730,13 @@ cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, 
                                 int32_t* thresh, cudaStream_t stream) {
     if (n_pad <= 0) return cudaSuccess;
     row_norms_kernel<uint8_t><<<n_pad / 32, 256, 0, stream>>>(x, n, n_pad, 1.0f, metric, norm, rec, thresh);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fold_records_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* rec, uint32_t* fold,
+                                   cudaStream_t stream) {
+    if (n_pad <= 0) return cudaSuccess;
+    fold_records_kernel<<<n_pad / 32, 256, 0, stream>>>(x, n, n_pad, metric, rec, fold);
     return cudaGetLastError();
 }
 

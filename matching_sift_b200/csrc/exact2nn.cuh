@@ -16,6 +16,8 @@ constexpr int kEpiWarps = 4 * kQT;   // one epilogue warp per (query tile, TMEM 
 constexpr int kThreads = 64 + 32 * kEpiWarps;
 constexpr int kTmemCols = kQT * kBN; // one accumulator slot of kBN columns per query tile
 constexpr int32_t kKeyPad = 1 << 30; // ranking key of padding rows (never a real key)
+constexpr int32_t kFoldMax = 30 * 128 * 255 + 254;  // largest folded half-norm (norms up to ~1.96e6 fold exactly)
+constexpr int kFoldHalfBytes = 2048;                // folding digits of 64 base rows (32 s8 each)
 constexpr int kRecInts = 160;        // per-base-tile record: 128 norms, 16 8-row minima, pad
 
 // Distance definitions of the exact path.
@@ -139,6 +141,11 @@ cudaError_t launch_merge2nn_float(const int4* partial, const ExactPlan& plan, in
 //                                     pruning bound of the search kernel)
 cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* norm, int32_t* rec,
                                 int32_t* thresh, cudaStream_t stream);
+// Records of the fold variant: residuals |b|^2 - 2 c (c = the folded
+// half-norm) in place of the norms, their 8- and 16-row minima, and the
+// folding digits of every row, n_pad / kBN tiles x 2 x kFoldHalfBytes bytes.
+cudaError_t launch_fold_records_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* rec, uint32_t* fold,
+                                   cudaStream_t stream);
 // The same for FP16 rows whose values times mul (a power of two) are
 // integers in [0, 255].
 cudaError_t launch_row_norms_f16(const void* x, int n, int n_pad, float mul, int metric, int32_t* norm, int32_t* rec,
@@ -179,6 +186,12 @@ struct ChunkSet {
     int tiles[kMaxChunks];
 };
 // The pair kernel over one explicit work item (a chunk of the base).
+// The fold variant of launch_exact2nn_u8_pair: brec from launch_fold_records_u8
+// (residual records) and fmap a 2-D u8 tensor map of its folding digits
+// (rows of 256 bytes, box 256 x 8: one half tile).
+cudaError_t launch_exact2nn_u8fold_pair(const CUtensorMap& qmap, const CUtensorMap& bmap_half,
+                                        const CUtensorMap& fmap, const int32_t* brec, const ExactPlan& plan,
+                                        int4* partial, int32_t* thresh, int* err, cudaStream_t stream);
 cudaError_t launch_exact2nn_u8_pair_item(const CUtensorMap& qmap, const CUtensorMap& bmap_half, const int32_t* brec,
                                          const ExactPlan& plan, const WorkItem& item, int4* partial, int32_t* thresh,
                                          int* err, cudaStream_t stream);

@@ -96,6 +96,7 @@ enum PairMode : int {
     kModeU8 = 0,     // u8 rows, kind::i8, integer keys
     kModeF16Int = 1, // FP16 rows holding integers x 2^-s, kind::f16, integer keys
     kModeFloat = 2,  // split FP16 rows [hi | lo] (or plain FP16 rows), kind::f16, float keys
+    kModeU8Fold = 3, // u8 rows plus a fifth MMA that folds the norms in (fold_records_kernel)
 };
 
 // Shapes of one instantiation. A row of 128 elements is kKBlocks blocks of
@@ -104,9 +105,12 @@ enum PairMode : int {
 // consumes 32 bytes of K.
 template <int MODE, int QPT, int QB>
 struct PairCfg {
-    static constexpr bool F16 = MODE != kModeU8;
+    static constexpr bool F16 = MODE == kModeF16Int || MODE == kModeFloat;
+    static constexpr bool kFold = MODE == kModeU8Fold;
+    static constexpr int kFoldStage = kFold ? kFoldHalfBytes : 0;  // digits of the base half, per stage
+    static constexpr int kAConst = kFold ? kBM * 32 : 0;           // the constant fold row, 128 rows
     static constexpr int kElemBytes = F16 ? 2 : 1;
-    static constexpr int kKBlocks = MODE == kModeU8 ? 1 : (MODE == kModeFloat ? 4 : 2);
+    static constexpr int kKBlocks = !F16 ? 1 : (MODE == kModeFloat ? 4 : 2);
     static constexpr int kBoxElems = 128 / kElemBytes;       // TMA box width of one K block
     static constexpr int kQKBlock = kBM * 128;               // bytes of one K block of a query tile
     static constexpr int kBKBlock = kPHalf * 128;            // bytes of one K block of a base half
@@ -119,7 +123,8 @@ struct PairCfg {
     static constexpr int kThreads = 64 + 32 * kEpiWarps + 32;
     static constexpr int kTmemCols = kSlots * kBN;
     static constexpr int kStagesFit =
-        static_cast<int>((kPSmemBudget - 1024 - 512 - QB * kQBufBytes) / (kBHalfBytes + kPRecBytes));
+        static_cast<int>((kPSmemBudget - 1024 - 512 - QB * kQBufBytes - kAConst) /
+                         (kBHalfBytes + kFoldStage + kPRecBytes));
     // 16 stages when they fit (a power of two keeps the ring index cheap in
     // the issue loop), else as many as fit.
     static constexpr int kStages = kStagesFit >= 16 ? 16 : kStagesFit;
@@ -135,7 +140,8 @@ struct PairCfg {
         int no_abort;
     };
     static constexpr size_t kSmemBytes =
-        1024 + QB * kQBufBytes + kStages * kBHalfBytes + kStages * kPRecBytes + sizeof(Ctl);
+        1024 + QB * kQBufBytes + kStages * (kBHalfBytes + kFoldStage) + kAConst + kStages * kPRecBytes +
+        sizeof(Ctl);
     // M = 256 (the pair), N = kBN; s32 accumulators for u8 x u8, f32 for f16 x f16.
     static constexpr uint32_t kIdesc =
         F16 ? ptx::idesc_make(1 /*F32*/, 0 /*F16*/, 0 /*F16*/, 2 * kBM, kBN)
@@ -196,7 +202,7 @@ struct Cursor {
 // TWO_PASS: the two-pass epilogue (single searches) or the one-pass scan
 // (batches of small problems).
 template <int MODE, int QPT, int QB, bool TWO_PASS>
-__device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtensorMap& bmap,
+__device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtensorMap& bmap, const CUtensorMap& fmap,
                                           const int32_t* __restrict__ brec, const ExactPlan& plan,
                                           const WorkItem* __restrict__ items, int n_items, const WorkItem& single,
                                           int4* __restrict__ partial, int32_t* __restrict__ thresh,
@@ -215,11 +221,15 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
     uint8_t* smem = smem_raw + ((1024u - (raw_u32 & 1023u)) & 1023u);
     uint8_t* q_smem = smem;
     uint8_t* b_smem = smem + QB * Cfg::kQBufBytes;
-    int32_t* r_smem = reinterpret_cast<int32_t*>(b_smem + kPStages * kPBHalfBytes);
+    uint8_t* f_smem = b_smem + kPStages * kPBHalfBytes;        // fold digits per stage (fold only)
+    uint8_t* a_smem = f_smem + kPStages * Cfg::kFoldStage;     // the constant fold row tile (fold only)
+    int32_t* r_smem = reinterpret_cast<int32_t*>(a_smem + Cfg::kAConst);
     PairCtl* ctl = reinterpret_cast<PairCtl*>(r_smem + kPStages * kRecInts);
     const uint32_t q_s = ptx::smem_u32(q_smem);
     const uint32_t b_s = ptx::smem_u32(b_smem);
     const uint32_t r_s = ptx::smem_u32(r_smem);
+    const uint32_t f_s = ptx::smem_u32(f_smem);
+    const uint32_t a_s = ptx::smem_u32(a_smem);
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -262,6 +272,22 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
     if (warp == 1) {
         ptx::tmem_alloc_pair(ptx::smem_u32(&ctl->tmem_base), Cfg::kTmemCols);
         ptx::tmem_relinquish_pair();
+    }
+    if constexpr (Cfg::kFold) {
+        // The constant fold row a = {1, 16, 255 x 30} for all 128 query rows,
+        // in the no-swizzle K-major layout of fold_records_kernel's digits
+        // (8-row groups of 256 B, two 16-byte K chunks 128 B apart).
+        for (int i = threadIdx.x; i < Cfg::kAConst / 4; i += blockDim.x) {
+            const int kc = (i >> 5) & 1, b0 = (i & 3) * 4;  // 4 bytes: K = 16 kc + b0 .. + 3
+            uint32_t word = 0;
+            #pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int k = 16 * kc + b0 + b;
+                word |= static_cast<uint32_t>(k == 0 ? 1 : (k == 1 ? 16 : 255)) << (8 * b);
+            }
+            reinterpret_cast<uint32_t*>(a_smem)[i] = word;
+        }
+        ptx::fence_proxy_async();
     }
     ptx::tc_fence_before();
     __syncthreads();
@@ -306,13 +332,16 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                 const int s = n % kPStages;
                 if (!ptx::mbar_wait(bar_sfree + 8 * s, ((n / kPStages) & 1) ^ 1, abort_flag, err, kErrWaitProducer))
                     break;
-                if (leader) ptx::mbar_arrive_expect_tx(bar_full + 8 * s, 2 * kb_load * Cfg::kBKBlock);
+                if (leader) ptx::mbar_arrive_expect_tx(bar_full + 8 * s, 2 * (kb_load * Cfg::kBKBlock + Cfg::kFoldStage));
                 const int brow = cur.it.b_off + cur.j * kBN + static_cast<int>(rank) * kPHalf;
                 #pragma unroll
                 for (int kb = 0; kb < Cfg::kKBlocks; ++kb)
                     if (kb < kb_load)
                         ptx::tma_load_2d_pair(b_s + s * kPBHalfBytes + kb * Cfg::kBKBlock, &bmap, kb * Cfg::kBoxElems,
                                               brow, lead_full + 8 * s);
+                if constexpr (Cfg::kFold)
+                    ptx::tma_load_2d_pair(f_s + s * Cfg::kFoldStage, &fmap, 0,
+                                          ((cur.it.rec_off + cur.j) * 2 + static_cast<int>(rank)) * 8, lead_full + 8 * s);
                 ptx::mbar_arrive_expect_tx(bar_rfull + 8 * s, kPRecBytes);
                 ptx::bulk_load(r_s + s * kPRecBytes, brec + static_cast<size_t>(cur.it.rec_off + cur.j) * kRecInts,
                                kPRecBytes, bar_rfull + 8 * s);
@@ -393,6 +422,10 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                                     ptx::mma_i8_pair(d, a_desc + 2 * kk, b_kb + 2 * kk, idesc, acc);
                             }
                         }
+                        if constexpr (Cfg::kFold)
+                            ptx::mma_i8_pair(d, ptx::sdesc_kmajor_noswz(a_s, 128, 256),
+                                             ptx::sdesc_kmajor_noswz(f_s + s * Cfg::kFoldStage, 128, 256),
+                                             ptx::idesc_make(2 /*S32*/, 0 /*u8*/, 1 /*s8*/, 2 * kBM, kBN), 1u);
                         ptx::tc_commit_pair_mc(bar_tfull + 8 * (t * 2 + mt), kPairMask);
                     }
                     if (!ok) break;
@@ -477,21 +510,28 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
                         // handed back.
                         uint32_t va[16], vb[16];
                         const int thr0 = st.thr;
+                        const int vt = -((thr0 >> 1) + (thr0 & 1));  // fold variant: -floor((thr0 + 1) / 2)
+                        auto bits = [&](const uint32_t (&v)[16], int c) -> uint32_t {
+                            if constexpr (Cfg::kFold)
+                                return fold_bits16(v, vt);
+                            else
+                                return bound16<kKind>(v, rec + kBN + 2 * c, thr0, dscale);
+                        };
                         uint32_t pass = 0;  // bit 2 c + k: subgroup k of chunk c may hold a candidate
                         ptx::tmem_ld16(taddr, va);
                         ptx::tmem_ld_wait(va);
                         #pragma unroll
                         for (int c = 1; c < 8; c += 2) {
                             ptx::tmem_ld16(taddr + 16 * c, vb);
-                            pass |= bound16<kKind>(va, rec + kBN + 2 * (c - 1), thr0, dscale) << (2 * (c - 1));
+                            pass |= bits(va, c - 1) << (2 * (c - 1));
                             ptx::tmem_ld_wait(vb);
                             if (c + 1 < 8) {
                                 ptx::tmem_ld16(taddr + 16 * (c + 1), va);
-                                pass |= bound16<kKind>(vb, rec + kBN + 2 * c, thr0, dscale) << (2 * c);
+                                pass |= bits(vb, c) << (2 * c);
                                 ptx::tmem_ld_wait(va);
                             }
                         }
-                        pass |= bound16<kKind>(vb, rec + kBN + 14, thr0, dscale) << 14;
+                        pass |= bits(vb, 7) << 14;
                         // Subgroups in increasing order, so the top-2 still sees
                         // the rows in index order (ties keep the lower index).
                         uint32_t todo = __reduce_or_sync(0xffffffffu, pass);
@@ -564,6 +604,7 @@ __device__ __forceinline__ void pair_body(const CUtensorMap& qmap, const CUtenso
 
 using CfgU8 = PairCfg<kModeU8, 2, 1>;
 using CfgF16 = PairCfg<kModeF16Int, 2, 1>;
+using CfgFold = PairCfg<kModeU8Fold, 2, 1>;
 // Split float rows are 512 bytes: one query tile per CTA (groups of 256
 // queries) leaves room for 4 base stages.
 using CfgFloat = PairCfg<kModeFloat, 1, 1>;
@@ -572,7 +613,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CfgU8::kThreads, 1)
     exact2nn_u8_pair_kernel(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap bmap,
                             const int32_t* __restrict__ brec, const ExactPlan plan, const WorkItem single,
                             int4* __restrict__ partial, int32_t* __restrict__ thresh, int* __restrict__ err) {
-    pair_body<kModeU8, 2, 1, true>(qmap, bmap, brec, plan, nullptr, 1, single, partial, thresh, err, 1.0f);
+    pair_body<kModeU8, 2, 1, true>(qmap, bmap, qmap, brec, plan, nullptr, 1, single, partial, thresh, err, 1.0f);
+}
+
+// fmap: the folding digits (fold_records_kernel), a 2-D u8 tensor of
+// 256-byte rows, 8 rows per half tile.
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CfgFold::kThreads, 1)
+    exact2nn_u8fold_pair_kernel(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap bmap,
+                                const __grid_constant__ CUtensorMap fmap, const int32_t* __restrict__ brec,
+                                const ExactPlan plan, const WorkItem single, int4* __restrict__ partial,
+                                int32_t* __restrict__ thresh, int* __restrict__ err) {
+    pair_body<kModeU8Fold, 2, 1, true>(qmap, bmap, fmap, brec, plan, nullptr, 1, single, partial, thresh, err, 1.0f);
 }
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CfgF16::kThreads, 1)
@@ -580,7 +631,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CfgF16::kThreads, 1)
                              const int32_t* __restrict__ brec, const ExactPlan plan, const WorkItem single,
                              int4* __restrict__ partial, int32_t* __restrict__ thresh, int* __restrict__ err,
                              float dscale) {
-    pair_body<kModeF16Int, 2, 1, true>(qmap, bmap, brec, plan, nullptr, 1, single, partial, thresh, err, dscale);
+    pair_body<kModeF16Int, 2, 1, true>(qmap, bmap, qmap, brec, plan, nullptr, 1, single, partial, thresh, err,
+                                       dscale);
 }
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CfgFloat::kThreads, 1)
@@ -588,7 +640,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CfgFloat::kThreads, 
                                const int32_t* __restrict__ brec, const ExactPlan plan, const WorkItem single,
                                int4* __restrict__ partial, int32_t* __restrict__ thresh, int* __restrict__ err,
                                int has_lo) {
-    pair_body<kModeFloat, 1, 1, true>(qmap, bmap, brec, plan, nullptr, 1, single, partial, thresh, err, 1.0f,
+    pair_body<kModeFloat, 1, 1, true>(qmap, bmap, qmap, brec, plan, nullptr, 1, single, partial, thresh, err, 1.0f,
                                       has_lo != 0);
 }
 
@@ -598,7 +650,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PairCfg<kModeU8, QPT
                                   const int32_t* __restrict__ brec, const ExactPlan plan,
                                   const WorkItem* __restrict__ items, int n_items, int4* __restrict__ partial,
                                   int32_t* __restrict__ thresh, int* __restrict__ err) {
-    pair_body<kModeU8, QPT, QB, false>(qmap, bmap, brec, plan, items, n_items, WorkItem{}, partial, thresh, err,
+    pair_body<kModeU8, QPT, QB, false>(qmap, bmap, qmap, brec, plan, items, n_items, WorkItem{}, partial, thresh, err,
                                        1.0f);
 }
 
@@ -654,6 +706,18 @@ cudaError_t launch_exact2nn_u8_pair(const CUtensorMap& qmap, const CUtensorMap& 
     if (plan.grid <= 0) return cudaSuccess;
     exact2nn_u8_pair_kernel<<<2 * plan.grid, CfgU8::kThreads, CfgU8::kSmemBytes, stream>>>(
         qmap, bmap_half, brec, plan, single_item(plan), partial, thresh, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_exact2nn_u8fold_pair(const CUtensorMap& qmap, const CUtensorMap& bmap_half,
+                                        const CUtensorMap& fmap, const int32_t* brec, const ExactPlan& plan,
+                                        int4* partial, int32_t* thresh, int* err, cudaStream_t stream) {
+    static bool attr_set[64] = {};
+    cudaError_t e = set_smem_once(exact2nn_u8fold_pair_kernel, CfgFold::kSmemBytes, attr_set);
+    if (e != cudaSuccess) return e;
+    if (plan.grid <= 0) return cudaSuccess;
+    exact2nn_u8fold_pair_kernel<<<2 * plan.grid, CfgFold::kThreads, CfgFold::kSmemBytes, stream>>>(
+        qmap, bmap_half, fmap, brec, plan, single_item(plan), partial, thresh, err);
     return cudaGetLastError();
 }
 

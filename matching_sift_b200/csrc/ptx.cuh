@@ -157,6 +157,14 @@ __device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
            (static_cast<uint64_t>(2) << 61);
 }
 
+// Shared-memory matrix descriptor, K-major without swizzle: core matrices of
+// 8 rows x 16 bytes stored contiguously; lbo = bytes between core matrices
+// adjacent in K, sbo = bytes between adjacent 8-row groups (layout type 0).
+__device__ __forceinline__ uint64_t sdesc_kmajor_noswz(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return static_cast<uint64_t>((saddr & 0x3FFFFu) >> 4) | (static_cast<uint64_t>(lbo >> 4) << 16) |
+           (static_cast<uint64_t>(sbo >> 4) << 32) | (static_cast<uint64_t>(1) << 46);
+}
+
 // Instruction descriptor (kind::i8 / kind::f16): D format in [4,6)
 // (1 = F32, 2 = S32), A format [7,10), B format [10,13) (u8 = 0 / f16 = 0),
 // both operands K-major, N >> 3 in [17,23), M >> 4 in [24,29).

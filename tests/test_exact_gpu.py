@@ -19,12 +19,12 @@ GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 FLT_MAX = np.float32(np.finfo(np.float32).max)
 
 
-KERNELS = {"pair": 0, "single": 1}
+KERNELS = {"fold": 0, "single": 1, "pair": 3}
 
 
 @pytest.fixture(params=sorted(KERNELS))
 def kernel(request):
-    """Runs a test once per exact-search kernel (CTA-pair and single-CTA)."""
+    """Runs a test once per exact-search kernel (CTA-pair with folded norms, single-CTA, CTA-pair)."""
     ms.lib().sift_set_kernel_variant(KERNELS[request.param])
     yield request.param
     ms.lib().sift_set_kernel_variant(0)
