@@ -349,21 +349,55 @@ int stage_inputs(DeviceCtx& c, char* A, const InputPlan& ip, int type, const voi
 }
 
 // Host u8 inputs (U8_HOST) with a large base: the base is copied to the
-// device in kChunks chunks on the copy stream while the search kernel runs
-// on the chunks that have landed (records, then one persistent pair-kernel
-// launch per chunk); the per-query pruning bounds carry over from chunk to
-// chunk and one merge combines every chunk's partial lists. Same results as
-// the single-launch path. Caller holds c.mu.
+// device in chunks on the copy stream while the search kernel runs on the
+// chunks that have landed (records, then one persistent pair-kernel launch
+// per chunk); the per-query pruning bounds carry over from chunk to chunk
+// and one merge combines every chunk's partial lists. Same results as the
+// single-launch path. Caller holds c.mu.
 constexpr int kChunkMinRows = 1 << 16;
 constexpr int kChunks = 8;
+
+// Base tiles per chunk, in base order (returns the number of chunks).
+// The pinned copy moves a 128-byte row in ~2.3 ns (~55 GB/s of PCIe), and
+// the search kernel spends ~0.128 ps per query x row (10,000 x 1,000,000 in
+// ~1.28 ms), so with q_n queries a chunk's search takes beta = q_n x 5.5e-5
+// of its copy time. When beta is small the copy sets the pace and only the
+// last chunk's search (plus the merge) runs after the last byte lands: the
+// chunks then shrink geometrically toward the end of the base, each one
+// 1 / (1.25 beta) of the size of the chunk after it (between 1.25 and 4
+// times, the 1.25 covering the launches of a chunk), from a last chunk of 128
+// tiles (or 1/64 of the base), so that every chunk's search ends about when
+// the next chunk lands. Otherwise (the search sets the pace) the base goes in
+// kChunks equal chunks.
+int plan_chunk_tiles(int q_n, int tiles, int (&out)[kMaxChunks]) {
+    const double beta = 5.5e-5 * q_n, paced = 1.25 * beta;
+    if (paced > 1.0) {
+        const int per = (tiles + kChunks - 1) / kChunks;
+        int n = 0;
+        for (int t = 0; t < tiles; t += per) out[n++] = std::min(per, tiles - t);
+        return n;
+    }
+    const double grow = std::min(4.0, std::max(1.25, 1.0 / paced));
+    int rev[kMaxChunks];
+    int n = 0, left = tiles;
+    double size = std::max(128.0, tiles / 64.0);
+    while (left > 0) {
+        const int t = (n + 1 == kMaxChunks) ? left : std::min(left, static_cast<int>(size));
+        rev[n++] = t;
+        left -= t;
+        size *= grow;
+    }
+    for (int k = 0; k < n; ++k) out[k] = rev[n - 1 - k];
+    return n;
+}
 
 int exact_match_chunked(const MatchArgs& a, DeviceCtx& c, cudaStream_t st) {
     const int q_n = static_cast<int>(a.q_n), r_n = static_cast<int>(a.r_n);
     const int workers = c.num_sms / 2;
     const ExactPlan whole = make_exact_plan(q_n, r_n, workers, 2);
-    const int chunk_rows = ((r_n + kChunks - 1) / kChunks + kBN - 1) / kBN * kBN;
-    const int n_chunks = (r_n + chunk_rows - 1) / chunk_rows;
-    if (n_chunks > kMaxChunks) return SIFT_ERR_INVALID_ARG;
+    int chunk_tiles[kMaxChunks];
+    const int n_chunks = plan_chunk_tiles(q_n, whole.base_tiles, chunk_tiles);
+    int chunk_off[kMaxChunks];  // first base row of each chunk (a multiple of kBN)
     ChunkSet cs{};
     cs.n = n_chunks;
     cs.r_n = r_n;
@@ -371,8 +405,10 @@ int exact_match_chunked(const MatchArgs& a, DeviceCtx& c, cudaStream_t st) {
     cs.q_pad = whole.q_pad;
     ExactPlan plans[kMaxChunks];
     long long slots = 1;
-    for (int ch = 0; ch < n_chunks; ++ch) {
-        const int rows = std::min(chunk_rows, r_n - ch * chunk_rows);
+    for (int ch = 0, off = 0; ch < n_chunks; ++ch) {
+        chunk_off[ch] = off;
+        const int rows = std::min(chunk_tiles[ch] * kBN, r_n - off);
+        off += rows;
         plans[ch] = make_exact_plan(q_n, rows, workers, 2);
         cs.W[ch] = plans[ch].units;
         cs.G[ch] = plans[ch].grid;
@@ -413,7 +449,7 @@ int exact_match_chunked(const MatchArgs& a, DeviceCtx& c, cudaStream_t st) {
     SIFT_CUDA(cudaMemcpyAsync(qd, a.q, static_cast<size_t>(q_n) * kDim, cudaMemcpyHostToDevice, st));
     SIFT_CUDA(launch_row_norms_u8(qd, q_n, whole.q_pad, kMetricL2, qnorm, nullptr, thresh, st));
     for (int ch = 0; ch < n_chunks; ++ch) {
-        const size_t off = static_cast<size_t>(ch) * chunk_rows;
+        const size_t off = static_cast<size_t>(chunk_off[ch]);
         SIFT_CUDA(cudaMemcpyAsync(rd + off * kDim, rh + off * kDim, static_cast<size_t>(plans[ch].r_n) * kDim,
                                   cudaMemcpyHostToDevice, c.copy_stream));
         SIFT_CUDA(cudaEventRecord(c.chunk_ev[ch], c.copy_stream));
@@ -422,7 +458,7 @@ int exact_match_chunked(const MatchArgs& a, DeviceCtx& c, cudaStream_t st) {
     SIFT_TRY(encode_u8_rows(&qmap, qd, q_n, kBM));
     SIFT_TRY(encode_u8_rows(&bmap, rd, r_n, kBN / 2));
     for (int ch = 0; ch < n_chunks; ++ch) {
-        const int off = ch * chunk_rows;
+        const int off = chunk_off[ch];
         SIFT_CUDA(cudaStreamWaitEvent(st, c.chunk_ev[ch], 0));
         SIFT_CUDA(launch_row_norms_u8(rd + static_cast<size_t>(off) * kDim, plans[ch].r_n, plans[ch].r_pad, a.metric,
                                       nullptr, brec + static_cast<size_t>(off / kBN) * kRecInts, nullptr, st));

@@ -227,29 +227,30 @@ def test_against_reference_gpu_functions(cuda_device):
 
 
 @pytest.mark.parametrize("metric", [ms.METRIC_L2, ms.METRIC_DOT])
-def test_host_inputs_pipelined_over_base_chunks(cuda_device, metric):
+@pytest.mark.parametrize("q_n", [700, 16_000])
+def test_host_inputs_pipelined_over_base_chunks(cuda_device, metric, q_n):
     """U8_HOST with a large base: the base is copied in chunks that overlap the
-    search; results equal the device-input path bit for bit (ragged last
-    chunk), and a query subset equals the oracle."""
-    import torch
-
-    q, r = datagen.make_workload(700, 200_003, seed=41)
+    search (700 queries: chunks shrinking toward the end of the base, the copy
+    setting the pace; 16,000 queries: equal chunks, the search setting it);
+    results equal the device-input path bit for bit (ragged last chunk), and a
+    query subset equals the oracle."""
+    q, r = datagen.make_workload(q_n, 200_003, seed=41)
     dev = _run(q, r, cuda_device, metric=metric)
-    out = {"matches": np.zeros(700, np.uint32), "sorted": np.zeros((700, 4), np.float32),
-           "nn_idx": np.zeros((700, 2), np.int32), "nn_dist": np.zeros((700, 2), np.float32)}
-    rc = ms.lib().sift2nn_match(q.ctypes.data, r.ctypes.data, ms.U8_HOST, 700, r.shape[0], metric, 0.8,
+    out = {"matches": np.zeros(q_n, np.uint32), "sorted": np.zeros((q_n, 4), np.float32),
+           "nn_idx": np.zeros((q_n, 2), np.int32), "nn_dist": np.zeros((q_n, 2), np.float32)}
+    rc = ms.lib().sift2nn_match(q.ctypes.data, r.ctypes.data, ms.U8_HOST, q_n, r.shape[0], metric, 0.8,
                                 out["matches"].ctypes.data, out["sorted"].ctypes.data, out["nn_idx"].ctypes.data,
                                 out["nn_dist"].ctypes.data, None)
     assert rc == ms.SIFT_OK
     for k in out:
         np.testing.assert_array_equal(out[k].view(np.int32) if k == "matches" else out[k],
                                       dev[k].view(np.int32) if k == "matches" else dev[k], err_msg=k)
-    sel = np.arange(0, 700, 7)
+    sel = np.arange(0, q_n, q_n // 100)
     d, i = oracle.brute_2nn_u8(q[sel], r, metric=metric)
     np.testing.assert_array_equal(out["nn_idx"][sel].astype(np.int64), i)
     np.testing.assert_array_equal(out["nn_dist"][sel].astype(np.int64), d)
     # the reference-named call on host buffers takes the same path
-    m = np.zeros(700, np.uint32)
+    m = np.zeros(q_n, np.uint32)
     if metric == ms.METRIC_L2:
-        assert ms.cublas_2nn_sift(q, r, ms.U8_HOST, 700, r.shape[0], m, 0.8) == ms.SIFT_OK
+        assert ms.cublas_2nn_sift(q, r, ms.U8_HOST, q_n, r.shape[0], m, 0.8) == ms.SIFT_OK
         np.testing.assert_array_equal(m, out["matches"])
