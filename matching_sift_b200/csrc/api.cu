@@ -194,7 +194,8 @@ int map_cuda(cudaError_t e) {
 }
 
 
-// Reads and clears the device status words. Caller has synchronised `st`.
+// Reads and clears the device status words: one copy on `st` and one
+// synchronisation, which also waits for all the work enqueued on `st` before.
 int collect_device_status(DeviceCtx& c, cudaStream_t st) {
     SIFT_CUDA(cudaMemcpyAsync(c.h_status, c.d_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
     SIFT_CUDA(cudaStreamSynchronize(st));
@@ -391,7 +392,9 @@ int plan_chunk_tiles(int q_n, int tiles, int (&out)[kMaxChunks]) {
     return n;
 }
 
-int exact_match_chunked(const MatchArgs& a, DeviceCtx& c, cudaStream_t st) {
+// fold: the search kernel with the norms folded into the MMAs (the default
+// for u8 rows), else the pair kernel without folding.
+int exact_match_chunked(const MatchArgs& a, DeviceCtx& c, cudaStream_t st, bool fold) {
     const int q_n = static_cast<int>(a.q_n), r_n = static_cast<int>(a.r_n);
     const int workers = c.num_sms / 2;
     const ExactPlan whole = make_exact_plan(q_n, r_n, workers, 2);
@@ -428,6 +431,7 @@ int exact_match_chunked(const MatchArgs& a, DeviceCtx& c, cudaStream_t st) {
     const size_t o_qnorm = L.take(static_cast<size_t>(whole.q_pad) * 4);
     const size_t o_thr = L.take(static_cast<size_t>(whole.q_pad) * 4);
     const size_t o_part = L.take(static_cast<size_t>(n_chunks) * cs.slot_stride * sizeof(int4));
+    const size_t o_fold = fold ? L.take(static_cast<size_t>(whole.base_tiles) * 2 * kFoldHalfBytes) : 0;
     const size_t o_m = (a.matches && !m_dev) ? L.take(static_cast<size_t>(q_n) * 4) : 0;
     const size_t o_s = (a.sorted && !s_dev) ? L.take(static_cast<size_t>(q_n) * 16) : 0;
     const size_t o_i = (a.nn_idx && !i_dev) ? L.take(static_cast<size_t>(q_n) * 8) : 0;
@@ -440,6 +444,7 @@ int exact_match_chunked(const MatchArgs& a, DeviceCtx& c, cudaStream_t st) {
     int32_t* qnorm = reinterpret_cast<int32_t*>(A + o_qnorm);
     int32_t* thresh = reinterpret_cast<int32_t*>(A + o_thr);
     int4* partial = reinterpret_cast<int4*>(A + o_part);
+    uint32_t* fold_digits = reinterpret_cast<uint32_t*>(A + o_fold);
     const uint8_t* rh = static_cast<const uint8_t*>(a.r);
 
     // The base chunks on the copy stream once every earlier use of the arena
@@ -454,14 +459,21 @@ int exact_match_chunked(const MatchArgs& a, DeviceCtx& c, cudaStream_t st) {
                                   cudaMemcpyHostToDevice, c.copy_stream));
         SIFT_CUDA(cudaEventRecord(c.chunk_ev[ch], c.copy_stream));
     }
-    CUtensorMap qmap, bmap;
+    CUtensorMap qmap, bmap, fmap;
     SIFT_TRY(encode_u8_rows(&qmap, qd, q_n, kBM));
     SIFT_TRY(encode_u8_rows(&bmap, rd, r_n, kBN / 2));
+    if (fold) SIFT_TRY(encode_fold_map(&fmap, fold_digits, whole.base_tiles));
     for (int ch = 0; ch < n_chunks; ++ch) {
         const int off = chunk_off[ch];
+        const uint8_t* rows = rd + static_cast<size_t>(off) * kDim;
+        int32_t* rec = brec + static_cast<size_t>(off / kBN) * kRecInts;
         SIFT_CUDA(cudaStreamWaitEvent(st, c.chunk_ev[ch], 0));
-        SIFT_CUDA(launch_row_norms_u8(rd + static_cast<size_t>(off) * kDim, plans[ch].r_n, plans[ch].r_pad, a.metric,
-                                      nullptr, brec + static_cast<size_t>(off / kBN) * kRecInts, nullptr, st));
+        if (fold)
+            SIFT_CUDA(launch_fold_records_u8(rows, plans[ch].r_n, plans[ch].r_pad, a.metric, rec,
+                                             fold_digits + static_cast<size_t>(off / kBN) * 2 * kFoldHalfBytes / 4,
+                                             st));
+        else
+            SIFT_CUDA(launch_row_norms_u8(rows, plans[ch].r_n, plans[ch].r_pad, a.metric, nullptr, rec, nullptr, st));
         WorkItem it{};
         it.n_a = q_n;
         it.b_off = off;
@@ -470,8 +482,12 @@ int exact_match_chunked(const MatchArgs& a, DeviceCtx& c, cudaStream_t st) {
         it.tiles = plans[ch].base_tiles;
         it.rec_off = off / kBN;
         it.idx_base = off;
-        SIFT_CUDA(launch_exact2nn_u8_pair_item(qmap, bmap, brec, plans[ch], it, partial + ch * cs.slot_stride, thresh,
-                                               c.d_status, st));
+        if (fold)
+            SIFT_CUDA(launch_exact2nn_u8fold_pair_item(qmap, bmap, fmap, brec, plans[ch], it,
+                                                       partial + ch * cs.slot_stride, thresh, c.d_status, st));
+        else
+            SIFT_CUDA(launch_exact2nn_u8_pair_item(qmap, bmap, brec, plans[ch], it, partial + ch * cs.slot_stride,
+                                                   thresh, c.d_status, st));
     }
     g_launches += 1 + 2 * n_chunks + 1;
 
@@ -489,7 +505,6 @@ int exact_match_chunked(const MatchArgs& a, DeviceCtx& c, cudaStream_t st) {
         SIFT_CUDA(cudaMemcpyAsync(a.nn_idx, i_out, static_cast<size_t>(q_n) * 8, cudaMemcpyDeviceToHost, st));
     if (a.nn_dist && !d_dev)
         SIFT_CUDA(cudaMemcpyAsync(a.nn_dist, d_out, static_cast<size_t>(q_n) * 8, cudaMemcpyDeviceToHost, st));
-    SIFT_CUDA(cudaStreamSynchronize(st));
     return collect_device_status(c, st);
 }
 
@@ -604,7 +619,6 @@ int exact_match_float(const MatchArgs& a, DeviceCtx& c, cudaStream_t st) {
     if (a.nn_dist && !d_dev)
         SIFT_CUDA(cudaMemcpyAsync(a.nn_dist, d_out, static_cast<size_t>(q_n) * 8, cudaMemcpyDeviceToHost, st));
     if (a.sync || host_out || host_in) {
-        SIFT_CUDA(cudaStreamSynchronize(st));
         return collect_device_status(c, st);
     }
     return SIFT_OK;
@@ -633,7 +647,7 @@ int exact_match(const MatchArgs& a) {
     // The default for u8 rows: the pair kernel with the norms folded into the
     // MMAs; variant 3 keeps the pair kernel without folding.
     const bool use_fold = variant == 0 && a.type != SIFT_HALF_DEVICE;
-    if (use_pair && a.type == SIFT_U8_HOST && r_n >= kChunkMinRows) return exact_match_chunked(a, c, st);
+    if (use_pair && a.type == SIFT_U8_HOST && r_n >= kChunkMinRows) return exact_match_chunked(a, c, st, use_fold);
     const ExactPlan plan = use_pair ? make_exact_plan(q_n, r_n, c.num_sms / 2, 2) : make_exact_plan(q_n, r_n, c.num_sms, 1);
 
     // Output placement: direct when the device can write the pointer, else staged.
@@ -742,7 +756,6 @@ int exact_match(const MatchArgs& a) {
 
     const bool host_in = a.type == SIFT_U8_HOST || a.type == SIFT_FLOAT_HOST;
     if (a.sync || host_out || host_in) {
-        SIFT_CUDA(cudaStreamSynchronize(st));
         return collect_device_status(c, st);
     }
     return SIFT_OK;
@@ -840,7 +853,6 @@ int lsh_match_float(const LshArgs& a, DeviceCtx& c, cudaStream_t st) {
     if (a.nn_dist && !d_dev)
         SIFT_CUDA(cudaMemcpyAsync(a.nn_dist, d_out, static_cast<size_t>(q_n) * 8, cudaMemcpyDeviceToHost, st));
     if (a.sync || host_out || host_in) {
-        SIFT_CUDA(cudaStreamSynchronize(st));
         return collect_device_status(c, st);
     }
     return SIFT_OK;
@@ -950,7 +962,6 @@ int lsh_match(const LshArgs& a) {
         SIFT_CUDA(cudaMemcpyAsync(a.nn_dist, d_out, static_cast<size_t>(q_n) * 8, cudaMemcpyDeviceToHost, st));
     const bool host_in = a.type == SIFT_U8_HOST || a.type == SIFT_FLOAT_HOST || !planes_dev;
     if (a.sync || host_out || host_in) {
-        SIFT_CUDA(cudaStreamSynchronize(st));
         return collect_device_status(c, st);
     }
     return SIFT_OK;

@@ -630,15 +630,22 @@ __global__ void __launch_bounds__(256) merge2nn_kernel(const int4* __restrict__ 
     }
 }
 
-// Merge of a search split over base chunks (indices already global).
+// Merge of a search split over base chunks (indices already global). A
+// query row has a partial list per (chunk, CTA pair of its group, buffer),
+// ~90 for 10,000 x 1,000,000 in 9 chunks: kMergeLanes threads per row read
+// every kMergeLanes-th list (independent loads instead of one dependent
+// chain), and their top-2s are merged by shuffles. Every row of the base is
+// in exactly one list and (key, index) is a total order, so the top-2 does
+// not depend on the order of the merges.
+constexpr int kMergeLanes = 8;
 __global__ void __launch_bounds__(256) merge2nn_chunks_kernel(const int4* __restrict__ partial, const ChunkSet cs,
                                                               int q_n, const int32_t* __restrict__ qnorm, int metric,
                                                               float thr, float dscale, uint32_t* __restrict__ matches,
                                                               float4* __restrict__ sorted,
                                                               int32_t* __restrict__ nn_idx,
                                                               float* __restrict__ nn_dist) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= q_n) return;
+    const long long tid = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int q = static_cast<int>(tid / kMergeLanes), sub = static_cast<int>(tid % kMergeLanes);
     int a1 = INT_MAX, j1 = -1, a2 = INT_MAX, j2 = -1;
     auto push = [&](int k, int i) {
         if (i < 0) return;
@@ -649,19 +656,33 @@ __global__ void __launch_bounds__(256) merge2nn_chunks_kernel(const int4* __rest
             a2 = k; j2 = i;
         }
     };
-    const int g = q / (kQT * kBM);
-    for (int c = 0; c < cs.n; ++c) {
-        if (cs.W[c] <= 0 || cs.tiles[c] <= 0) continue;
-        const long long first = static_cast<long long>(g) * cs.tiles[c];
-        const int c0 = plan_cta_of(first, cs.W[c], cs.G[c]);
-        const int c1 = plan_cta_of(first + cs.tiles[c] - 1, cs.W[c], cs.G[c]);
-        const int4* pc = partial + c * cs.slot_stride;
-        for (int s = 0; s < (c1 - c0 + 1) * cs.parts; ++s) {
-            const int4 p = pc[static_cast<size_t>(s) * cs.q_pad + q];
-            push(p.x, p.y);
-            push(p.z, p.w);
+    if (q < q_n) {
+        const int g = q / (kQT * kBM);
+        int done = 0;  // lists of the earlier chunks
+        for (int c = 0; c < cs.n; ++c) {
+            if (cs.W[c] <= 0 || cs.tiles[c] <= 0) continue;
+            const long long first = static_cast<long long>(g) * cs.tiles[c];
+            const int c0 = plan_cta_of(first, cs.W[c], cs.G[c]);
+            const int c1 = plan_cta_of(first + cs.tiles[c] - 1, cs.W[c], cs.G[c]);
+            const int4* pc = partial + c * cs.slot_stride;
+            const int n_lists = (c1 - c0 + 1) * cs.parts;
+            for (int s = (sub - done % kMergeLanes + kMergeLanes) % kMergeLanes; s < n_lists; s += kMergeLanes) {
+                const int4 p = pc[static_cast<size_t>(s) * cs.q_pad + q];
+                push(p.x, p.y);
+                push(p.z, p.w);
+            }
+            done += n_lists;
         }
     }
+    // The kMergeLanes threads of a row are consecutive lanes of one warp.
+    #pragma unroll
+    for (int off = 1; off < kMergeLanes; off <<= 1) {
+        const int b1 = __shfl_xor_sync(0xffffffffu, a1, off), i1 = __shfl_xor_sync(0xffffffffu, j1, off);
+        const int b2 = __shfl_xor_sync(0xffffffffu, a2, off), i2 = __shfl_xor_sync(0xffffffffu, j2, off);
+        push(b1, i1);
+        push(b2, i2);
+    }
+    if (q >= q_n || sub != 0) return;
     const bool v1 = j1 >= 0 && j1 < cs.r_n && a1 < kKeyPad;
     const bool v2 = j2 >= 0 && j2 < cs.r_n && a2 < kKeyPad;
     const int qn = metric == kMetricL2 ? qnorm[q] : 0;
@@ -694,8 +715,9 @@ cudaError_t launch_merge2nn_chunks(const int4* partial, const ChunkSet& cs, int 
                                    float threshold, float dist_scale, uint32_t* matches, float4* sorted,
                                    int32_t* nn_idx, float* nn_dist, cudaStream_t stream) {
     if (q_n <= 0) return cudaSuccess;
-    merge2nn_chunks_kernel<<<(q_n + 255) / 256, 256, 0, stream>>>(partial, cs, q_n, qnorm, metric, threshold,
-                                                                  dist_scale, matches, sorted, nn_idx, nn_dist);
+    const long long threads = static_cast<long long>(q_n) * kMergeLanes;
+    merge2nn_chunks_kernel<<<static_cast<unsigned>((threads + 255) / 256), 256, 0, stream>>>(
+        partial, cs, q_n, qnorm, metric, threshold, dist_scale, matches, sorted, nn_idx, nn_dist);
     return cudaGetLastError();
 }
 

@@ -185,13 +185,19 @@ struct ChunkSet {
     int G[kMaxChunks];
     int tiles[kMaxChunks];
 };
-// The pair kernel over one explicit work item (a chunk of the base).
 // The fold variant of launch_exact2nn_u8_pair: brec from launch_fold_records_u8
 // (residual records) and fmap a 2-D u8 tensor map of its folding digits
 // (rows of 256 bytes, box 256 x 8: one half tile).
 cudaError_t launch_exact2nn_u8fold_pair(const CUtensorMap& qmap, const CUtensorMap& bmap_half,
                                         const CUtensorMap& fmap, const int32_t* brec, const ExactPlan& plan,
                                         int4* partial, int32_t* thresh, int* err, cudaStream_t stream);
+// The fold variant over one explicit work item (the item's rec_off indexes
+// both the residual records and the folding digits).
+cudaError_t launch_exact2nn_u8fold_pair_item(const CUtensorMap& qmap, const CUtensorMap& bmap_half,
+                                             const CUtensorMap& fmap, const int32_t* brec, const ExactPlan& plan,
+                                             const WorkItem& item, int4* partial, int32_t* thresh, int* err,
+                                             cudaStream_t stream);
+// The pair kernel over one explicit work item (a chunk of the base).
 cudaError_t launch_exact2nn_u8_pair_item(const CUtensorMap& qmap, const CUtensorMap& bmap_half, const int32_t* brec,
                                          const ExactPlan& plan, const WorkItem& item, int4* partial, int32_t* thresh,
                                          int* err, cudaStream_t stream);

@@ -721,6 +721,19 @@ cudaError_t launch_exact2nn_u8fold_pair(const CUtensorMap& qmap, const CUtensorM
     return cudaGetLastError();
 }
 
+cudaError_t launch_exact2nn_u8fold_pair_item(const CUtensorMap& qmap, const CUtensorMap& bmap_half,
+                                             const CUtensorMap& fmap, const int32_t* brec, const ExactPlan& plan,
+                                             const WorkItem& item, int4* partial, int32_t* thresh, int* err,
+                                             cudaStream_t stream) {
+    static bool attr_set[64] = {};
+    cudaError_t e = set_smem_once(exact2nn_u8fold_pair_kernel, CfgFold::kSmemBytes, attr_set);
+    if (e != cudaSuccess) return e;
+    if (plan.grid <= 0) return cudaSuccess;
+    exact2nn_u8fold_pair_kernel<<<2 * plan.grid, CfgFold::kThreads, CfgFold::kSmemBytes, stream>>>(
+        qmap, bmap_half, fmap, brec, plan, item, partial, thresh, err);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_exact2nn_u8_pair_item(const CUtensorMap& qmap, const CUtensorMap& bmap_half, const int32_t* brec,
                                          const ExactPlan& plan, const WorkItem& item, int4* partial, int32_t* thresh,
                                          int* err, cudaStream_t stream) {

@@ -228,12 +228,14 @@ def test_against_reference_gpu_functions(cuda_device):
 
 @pytest.mark.parametrize("metric", [ms.METRIC_L2, ms.METRIC_DOT])
 @pytest.mark.parametrize("q_n", [700, 16_000])
-def test_host_inputs_pipelined_over_base_chunks(cuda_device, metric, q_n):
+def test_host_inputs_pipelined_over_base_chunks(cuda_device, kernel, metric, q_n):
     """U8_HOST with a large base: the base is copied in chunks that overlap the
     search (700 queries: chunks shrinking toward the end of the base, the copy
     setting the pace; 16,000 queries: equal chunks, the search setting it);
     results equal the device-input path bit for bit (ragged last chunk), and a
-    query subset equals the oracle."""
+    query subset equals the oracle. The CTA-pair kernels (with and without
+    folded norms) search the chunks; the single-CTA kernel takes the
+    unchunked path."""
     q, r = datagen.make_workload(q_n, 200_003, seed=41)
     dev = _run(q, r, cuda_device, metric=metric)
     out = {"matches": np.zeros(q_n, np.uint32), "sorted": np.zeros((q_n, 4), np.float32),
