@@ -145,59 +145,67 @@ __global__ void __launch_bounds__(256) row_norms_kernel(const T* __restrict__ x,
 // tensor cores' no-swizzle K-major layout (8-row groups of 256 bytes, two
 // 16-byte K chunks of 128 bytes each, 16 bytes per row), so one 2-D TMA box
 // of 8 x 256 bytes lands a half tile ready as an MMA operand.
+//
+// One block per base tile: 8 threads per row, the 4 rows of a thread's
+// 32-row parts loaded up front (64 bytes in flight per thread), then per row
+// the norm, the folded half-norm c, its digits and the residual.
 __global__ void __launch_bounds__(256) fold_records_kernel(const uint8_t* __restrict__ x, int n, int n_pad,
                                                            int metric, int32_t* __restrict__ rec,
                                                            uint32_t* __restrict__ fold) {
-    const int row = blockIdx.x * 32 + (threadIdx.x >> 3);
+    const int t = blockIdx.x;
     const int sub = threadIdx.x & 7;
-    uint32_t s = 0;
-    if (row < n) {
-        const uint4 w = load16_u8(x, row, sub, 1.0f);
-        s = __dp4a(w.x, w.x, 0u);
-        s = __dp4a(w.y, w.y, s);
-        s = __dp4a(w.z, w.z, s);
-        s = __dp4a(w.w, w.w, s);
-    }
-    s += __shfl_xor_sync(0xffffffffu, s, 1);
-    s += __shfl_xor_sync(0xffffffffu, s, 2);
-    s += __shfl_xor_sync(0xffffffffu, s, 4);
-    const int32_t norm = row < n ? (metric == kMetricL2 ? static_cast<int32_t>(s) : 0) : kKeyPad;
-    const int32_t c = row < n ? min((norm + 1) >> 1, kFoldMax) : 0;
-    const int32_t resid = norm - 2 * c;
-    // This thread's 4 digits k = 4 sub .. 4 sub + 3.
-    const int l = c % 255, h = c / 255;
-    uint32_t word = 0;
+    const int lrow = threadIdx.x >> 3;
+    uint4 w[4];
     #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-        const int k = 4 * sub + b;
-        const int d = k == 0 ? -(l & 15) : (k == 1 ? -(l >> 4) : -min(128, max(0, h - 128 * (k - 2))));
-        word |= (static_cast<uint32_t>(d) & 0xFFu) << (8 * b);
+    for (int part = 0; part < 4; ++part) {
+        const int row = t * kBN + part * 32 + lrow;
+        w[part] = row < n ? load16_u8(x, row, sub, 1.0f) : make_uint4(0u, 0u, 0u, 0u);
     }
-    const int t = row >> 7, w = row & 127;
-    const size_t off = (static_cast<size_t>(t) * 2 + (w >> 6)) * kFoldHalfBytes + ((w & 63) >> 3) * 256 +
-                       (sub >> 2) * 128 + (w & 7) * 16 + 4 * (sub & 3);
-    fold[off / 4] = word;
-
-    __shared__ int32_t res[32];
-    int32_t* r = rec + static_cast<size_t>(blockIdx.x / 4) * kRecInts;
-    const int part = blockIdx.x & 3;
-    if (sub == 0) {
-        res[threadIdx.x >> 3] = resid;
-        r[part * 32 + (threadIdx.x >> 3)] = resid;
+    __shared__ int32_t res[kBN];
+    int32_t* r = rec + static_cast<size_t>(t) * kRecInts;
+    #pragma unroll
+    for (int part = 0; part < 4; ++part) {
+        const int wr = part * 32 + lrow;  // row within the tile
+        const bool live = t * kBN + wr < n;
+        uint32_t s = __dp4a(w[part].x, w[part].x, 0u);
+        s = __dp4a(w[part].y, w[part].y, s);
+        s = __dp4a(w[part].z, w[part].z, s);
+        s = __dp4a(w[part].w, w[part].w, s);
+        s += __shfl_xor_sync(0xffffffffu, s, 1);
+        s += __shfl_xor_sync(0xffffffffu, s, 2);
+        s += __shfl_xor_sync(0xffffffffu, s, 4);
+        const int32_t norm = live ? (metric == kMetricL2 ? static_cast<int32_t>(s) : 0) : kKeyPad;
+        const int32_t c = live ? min((norm + 1) >> 1, kFoldMax) : 0;
+        const int32_t resid = norm - 2 * c;
+        // This thread's 4 digits k = 4 sub .. 4 sub + 3.
+        const int l = c % 255, h = c / 255;
+        uint32_t word = 0;
+        #pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int k = 4 * sub + b;
+            const int d = k == 0 ? -(l & 15) : (k == 1 ? -(l >> 4) : -min(128, max(0, h - 128 * (k - 2))));
+            word |= (static_cast<uint32_t>(d) & 0xFFu) << (8 * b);
+        }
+        const size_t off = (static_cast<size_t>(t) * 2 + (wr >> 6)) * kFoldHalfBytes + ((wr & 63) >> 3) * 256 +
+                           (sub >> 2) * 128 + (wr & 7) * 16 + 4 * (sub & 3);
+        fold[off / 4] = word;
+        if (sub == 0) {
+            res[wr] = resid;
+            r[wr] = resid;
+        }
     }
     __syncthreads();
-    if (threadIdx.x < 4) {
+    if (threadIdx.x < 16) {
         int m = res[8 * threadIdx.x];
         #pragma unroll
         for (int i = 1; i < 8; ++i) m = min(m, res[8 * threadIdx.x + i]);
-        r[128 + part * 4 + threadIdx.x] = m;
-    }
-    if (threadIdx.x >= 32 && threadIdx.x < 34) {
-        const int hh = threadIdx.x - 32;
+        r[128 + threadIdx.x] = m;
+    } else if (threadIdx.x < 24) {
+        const int hh = threadIdx.x - 16;
         int m = res[16 * hh];
         #pragma unroll
         for (int i = 1; i < 16; ++i) m = min(m, res[16 * hh + i]);
-        r[144 + part * 2 + hh] = m;
+        r[144 + hh] = m;
     }
 }
 
@@ -758,7 +766,7 @@ cudaError_t launch_row_norms_u8(const uint8_t* x, int n, int n_pad, int metric, 
 cudaError_t launch_fold_records_u8(const uint8_t* x, int n, int n_pad, int metric, int32_t* rec, uint32_t* fold,
                                    cudaStream_t stream) {
     if (n_pad <= 0) return cudaSuccess;
-    fold_records_kernel<<<n_pad / 32, 256, 0, stream>>>(x, n, n_pad, metric, rec, fold);
+    fold_records_kernel<<<n_pad / kBN, 256, 0, stream>>>(x, n, n_pad, metric, rec, fold);
     return cudaGetLastError();
 }
 
